@@ -1,0 +1,384 @@
+"""Python mirror of the daniel-koudouna/cuda-bimp keypoint API over the C ABI.
+
+Names follow the reference (bimp/include/detection/cuda_bimp.hpp,
+bimp/include/detection/bimp.hpp, bimp/include/detection/utils.hpp):
+
+* ``CudaStuff(width, height, lambdas)``        -> bimp_ctx_create
+* ``getKeypoints(gpu_image, cs)``               -> bimp_detect_device, returns the
+  7 x n device matrix (SURF_CUDA row layout), like the GpuMat colRange view
+* ``downloadKeypoints(kp)`` / ``uploadKeypoints`` (utils.cpp:109-150)
+* ``makeLambdasLog`` / ``makeLambdasLin`` / ``snapTransformSize``
+* ``Context(image)`` with ``getKeypoints()``, ``getKeypointsAndDownload()``,
+  ``loadImage()``, ``getResponses()`` (bimp.cpp:7-129)
+
+Device memory and streams come from torch; every computation runs in
+libbimp_b200.so.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+import warnings
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+KP_MAX_POINTS = L.KP_MAX_POINTS
+KP_VECTOR_LENGTH = L.KP_VECTOR_LENGTH
+NUM_ORI = L.NUM_ORI
+X_ROW, Y_ROW, LAPLACIAN_ROW, OCTAVE_ROW, SIZE_ROW, ANGLE_ROW, HESSIAN_ROW = range(7)
+
+
+def _torch():
+    import torch  # plumbing only: device memory and streams
+    return torch
+
+
+def _stream_ptr(stream=None) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+@dataclass
+class KeyPoint:
+    """Field-for-field stand-in of cv::KeyPoint."""
+    pt: tuple
+    size: float
+    angle: float
+    response: float
+    octave: int
+    class_id: int
+
+
+def default_params() -> L.Params:
+    p = L.Params()
+    L.lib().bimp_default_params(C.byref(p))
+    return p
+
+
+def makeLambdasLog(start: float, end: float, scales_per_octave: int) -> list:
+    n = C.c_int(0)
+    L.check(L.lib().bimp_make_lambdas_log(start, end, scales_per_octave, None, 0, C.byref(n)),
+            "makeLambdasLog")
+    buf = (C.c_float * max(n.value, 1))()
+    L.check(L.lib().bimp_make_lambdas_log(start, end, scales_per_octave, buf, n.value, C.byref(n)),
+            "makeLambdasLog")
+    return [float(buf[i]) for i in range(n.value)]
+
+
+def makeLambdasLin(start: float, end: float, num_scales: int) -> list:
+    n = C.c_int(0)
+    buf = (C.c_float * max(num_scales, 1))()
+    L.check(L.lib().bimp_make_lambdas_lin(start, end, num_scales, buf, num_scales, C.byref(n)),
+            "makeLambdasLin")
+    return [float(buf[i]) for i in range(n.value)]
+
+
+def snapTransformSize(n: int) -> int:
+    return int(L.lib().bimp_snap_transform_size(int(n)))
+
+
+def _params(params) -> L.Params | None:
+    if params is None:
+        return None
+    p = default_params()
+    items = params.items() if isinstance(params, dict) else vars(params).items()
+    for k, v in items:
+        if not hasattr(p, k):
+            raise ValueError(f"unknown parameter {k!r}")
+        setattr(p, k, float(v))
+    return p
+
+
+class CudaStuff:
+    """bimp::cuda::CudaStuff: filter bank + buffers for one image size."""
+
+    def __init__(self, width: int, height: int, lambdas, params=None):
+        lam = (C.c_float * len(lambdas))(*[float(x) for x in lambdas])
+        h = C.c_void_p()
+        p = _params(params)
+        L.check(L.lib().bimp_ctx_create(C.byref(h), int(width), int(height), lam, len(lambdas),
+                                        C.byref(p) if p is not None else None), "CudaStuff")
+        self._h = h
+        self.width, self.height = int(width), int(height)
+        self.ks = [self.scale_info(i) for i in range(L.lib().bimp_ctx_num_scales(h))]
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("CudaStuff already released")
+        return self._h
+
+    def scale_info(self, i: int) -> dict:
+        si = L.ScaleInfo()
+        L.check(L.lib().bimp_ctx_scale_info(self._h, i, C.byref(si)), "scale_info")
+        return {f: getattr(si, f) for f, _ in L.ScaleInfo._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            L.lib().bimp_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- dense maps of the last detection ---------------------------------
+    def dense_map(self, scale: int, which: int = 0):
+        torch = _torch()
+        k = self.ks[scale]
+        out = torch.empty((k["data_h"], k["data_w"]), dtype=torch.float32, device="cuda")
+        L.check(L.lib().bimp_dense_map(self.handle, scale, which, C.c_void_p(out.data_ptr()),
+                                       out.stride(0), _stream_ptr()), "dense_map")
+        return out
+
+    def complex_map(self, scale: int, orientation: int):
+        torch = _torch()
+        k = self.ks[scale]
+        out = torch.empty((k["data_h"] + 1, k["data_w"] + 1), dtype=torch.float32, device="cuda")
+        L.check(L.lib().bimp_complex_map(self.handle, scale, orientation, C.c_void_p(out.data_ptr()),
+                                         out.stride(0), _stream_ptr()), "complex_map")
+        return out
+
+
+def _as_gpu_u8(image):
+    torch = _torch()
+    if isinstance(image, np.ndarray):
+        image = torch.from_numpy(np.ascontiguousarray(image)).cuda()
+    if image.dtype != torch.uint8 or image.dim() != 2 or not image.is_cuda:
+        raise ValueError("expected a 2-D uint8 CUDA tensor")
+    if image.stride(1) != 1:
+        image = image.contiguous()
+    return image
+
+
+def getKeypoints(input, cs: CudaStuff, capacity: int = KP_MAX_POINTS, return_count: bool = False):
+    """bimp::cuda::getKeypoints(GpuMat&, CudaStuff&) (cuda_bimp.cu:129-140).
+
+    Returns the 7 x n float32 device matrix; like the reference, more than
+    ``capacity`` keypoints produce a warning and the first ``capacity`` are
+    kept ((scale, y, x) order).
+    """
+    torch = _torch()
+    img = _as_gpu_u8(input)
+    kp = torch.zeros((KP_VECTOR_LENGTH, max(capacity, 1)), dtype=torch.float32, device="cuda")
+    n = C.c_int(0)
+    rc = L.lib().bimp_detect_device(cs.handle, C.c_void_p(img.data_ptr()), img.stride(0),
+                                    img.shape[1], img.shape[0], C.c_void_p(kp.data_ptr()),
+                                    kp.stride(0), capacity, C.byref(n), _stream_ptr())
+    if rc == L.BIMP_ERR_CAPACITY:
+        warnings.warn(f"Keypoints ({n.value}) exceed current keypoint maximum ({capacity}).")
+    elif rc != L.BIMP_OK:
+        L.check(rc, "getKeypoints")
+    rows = min(n.value, capacity)
+    view = kp[:, :rows]
+    return (view, n.value) if return_count else view
+
+
+def downloadKeypoints(kp) -> list:
+    """bimp::utils::downloadKeypoints (utils.cpp:130-150)."""
+    n = kp.shape[1]
+    out = (L.KeyPointC * max(n, 1))()
+    L.check(L.lib().bimp_download_keypoints(C.c_void_p(kp.data_ptr()), kp.stride(0), n, out,
+                                            _stream_ptr()), "downloadKeypoints")
+    return [KeyPoint((k.x, k.y), k.size, k.angle, k.response, k.octave, k.class_id) for k in out[:n]]
+
+
+def uploadKeypoints(points) -> "object":
+    """bimp::utils::uploadKeypoints (utils.cpp:109-128)."""
+    torch = _torch()
+    n = len(points)
+    arr = (L.KeyPointC * max(n, 1))()
+    for i, p in enumerate(points):
+        arr[i] = L.KeyPointC(p.pt[0], p.pt[1], p.size, p.angle, p.response, p.octave, p.class_id)
+    kp = torch.empty((KP_VECTOR_LENGTH, max(n, 1)), dtype=torch.float32, device="cuda")
+    L.check(L.lib().bimp_upload_keypoints(arr, n, C.c_void_p(kp.data_ptr()), kp.stride(0),
+                                          _stream_ptr()), "uploadKeypoints")
+    return kp[:, :n]
+
+
+def detect_host(cs: CudaStuff, image: np.ndarray, capacity: int = KP_MAX_POINTS):
+    """Host image in, host records out through bimp_detect_host.
+
+    Returns (structured array of cv::KeyPoint fields, total count, status)."""
+    img = np.ascontiguousarray(image, dtype=np.uint8)
+    out = (L.KeyPointC * max(capacity, 1))()
+    n = C.c_int(0)
+    rc = L.lib().bimp_detect_host(cs.handle, C.c_void_p(img.ctypes.data), img.strides[0], img.shape[1],
+                                  img.shape[0], out, capacity, C.byref(n), _stream_ptr())
+    if rc not in (L.BIMP_OK, L.BIMP_ERR_CAPACITY):
+        L.check(rc, "detect_host")
+    m = min(n.value, capacity)
+    rec = np.frombuffer(out, dtype=np.dtype([("x", "<f4"), ("y", "<f4"), ("size", "<f4"),
+                                             ("angle", "<f4"), ("response", "<f4"),
+                                             ("octave", "<i4"), ("class_id", "<i4")]),
+                        count=m).copy()
+    return rec, n.value, rc
+
+
+def keypoint_matrix_to_records(kp) -> np.ndarray:
+    """7 x n device matrix -> structured numpy array (host)."""
+    h = kp.detach().cpu().numpy()
+    rec = np.zeros(h.shape[1], dtype=[("x", "f4"), ("y", "f4"), ("size", "f4"), ("angle", "f4"),
+                                      ("response", "f4"), ("octave", "i4"), ("class_id", "i4")])
+    rec["x"] = h[X_ROW]
+    rec["y"] = h[Y_ROW]
+    rec["size"] = h[SIZE_ROW]
+    rec["angle"] = h[ANGLE_ROW]
+    rec["response"] = h[HESSIAN_ROW]
+    rec["octave"] = h[OCTAVE_ROW].view(np.int32)
+    rec["class_id"] = h[LAPLACIAN_ROW].view(np.int32)
+    return rec
+
+
+class Context:
+    """bimp::Context (bimp.hpp:19-51, bimp.cpp:7-129) for grey uint8 images.
+
+    The bank is makeLambdasLog(4, 64, 2) as in bimp.cpp:8.
+    """
+
+    def __init__(self, image, lambdas=None, params=None):
+        img = np.asarray(image)
+        if img.ndim != 2:
+            raise ValueError("Context expects a grey uint8 image")
+        self.lambdas = list(lambdas) if lambdas is not None else makeLambdasLog(4, 64, 2)
+        self.cuda_data = CudaStuff(img.shape[1], img.shape[0], self.lambdas, params)
+        self.current_image = _as_gpu_u8(img)
+        self.current_keypoints = None
+        self.has_changed_keypoints = True
+
+    def width(self) -> int:
+        return int(self.current_image.shape[1])
+
+    def height(self) -> int:
+        return int(self.current_image.shape[0])
+
+    def loadImage(self, new_image):
+        self.current_image = _as_gpu_u8(new_image)
+        self.has_changed_keypoints = True
+
+    def getKeypoints(self):
+        if self.has_changed_keypoints:
+            self.current_keypoints = getKeypoints(self.current_image, self.cuda_data)
+            self.has_changed_keypoints = False
+        return self.current_keypoints
+
+    def getKeypointsAndDownload(self) -> list:
+        return downloadKeypoints(self.getKeypoints())
+
+    def getResponses(self) -> list:
+        """Per-scale summed keypoint map D and single-stopped map S."""
+        self.getKeypoints()
+        out = []
+        for i, k in enumerate(self.cuda_data.ks):
+            out.append(dict(k, D=self.cuda_data.dense_map(i, 0), S=self.cuda_data.dense_map(i, 1)))
+        return out
+
+
+class Batch:
+    """Many images of mixed sizes, one CUDA-graph replay per detection."""
+
+    def __init__(self, sizes, lambdas, params=None, kp_capacity: int = 65536):
+        n = len(sizes)
+        ws = (C.c_int * n)(*[int(w) for w, h in sizes])
+        hs = (C.c_int * n)(*[int(h) for w, h in sizes])
+        lam = (C.c_float * len(lambdas))(*[float(x) for x in lambdas])
+        p = _params(params)
+        h = C.c_void_p()
+        L.check(L.lib().bimp_batch_create(C.byref(h), ws, hs, n, lam, len(lambdas),
+                                          C.byref(p) if p is not None else None, kp_capacity),
+                "Batch")
+        self._h = h
+        self.sizes = [(int(w), int(hh)) for w, hh in sizes]
+        self.kp_capacity = kp_capacity
+        self._inputs = []
+        torch = _torch()
+        for i in range(n):
+            ptr = C.c_void_p()
+            pitch = C.c_size_t()
+            L.check(L.lib().bimp_batch_image(h, i, C.byref(ptr), C.byref(pitch)), "batch_image")
+            self._inputs.append((ptr.value, pitch.value))
+        self._counts = torch.zeros(n, dtype=torch.int32, device="cuda")
+
+    def input_view(self, i: int):
+        """(pointer, pitch) of image i's device input buffer."""
+        return self._inputs[i]
+
+    def input_tensor(self, i: int):
+        """uint8 CUDA tensor (h x w, row stride = pitch) aliasing image i's input."""
+        ptr, pitch = self._inputs[i]
+        w, h = self.sizes[i]
+        return _wrap_device(ptr, (h, w), (pitch, 1), "|u1")
+
+    def load(self, images, stream=None):
+        """Copy uint8 images (numpy or CUDA tensors) into the batch inputs."""
+        torch = _torch()
+        with torch.cuda.stream(stream) if stream is not None else _nullcontext():
+            for i, img in enumerate(images):
+                img = _as_gpu_u8(img)
+                if tuple(img.shape) != (self.sizes[i][1], self.sizes[i][0]):
+                    raise ValueError(f"image {i} has shape {tuple(img.shape)}, batch expects {self.sizes[i]}")
+                self.input_tensor(i).copy_(img, non_blocking=True)
+
+    def run(self, stream=None):
+        L.check(L.lib().bimp_batch_run(self._h, _stream_ptr(stream)), "batch_run")
+
+    def counts(self, stream=None):
+        L.check(L.lib().bimp_batch_counts(self._h, C.c_void_p(self._counts.data_ptr()),
+                                          _stream_ptr(stream)), "batch_counts")
+        return self._counts
+
+    def keypoints(self, i: int):
+        torch = _torch()
+        ptr = C.c_void_p()
+        ld = C.c_size_t()
+        L.check(L.lib().bimp_batch_keypoints_device(self._h, i, C.byref(ptr), C.byref(ld)),
+                "batch_keypoints")
+        n = int(self.counts()[i].item())
+        n = min(n, self.kp_capacity)
+        # wrap the internal matrix without copying
+        buf = _wrap_device(ptr.value, (KP_VECTOR_LENGTH, ld.value), (4 * ld.value, 4), "<f4")
+        return buf[:, :n]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            L.lib().bimp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _wrap_device(ptr: int, shape, strides_bytes, typestr: str):
+    """A CUDA tensor aliasing library-owned device memory (no copy)."""
+    torch = _torch()
+
+    class _Arr:
+        __cuda_array_interface__ = {"shape": tuple(shape), "strides": tuple(strides_bytes),
+                                    "typestr": typestr, "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_Arr(), device="cuda")
+
+
+class _nullcontext:
+    def __enter__(self):
+        return None
+
+    def __exit__(self, *a):
+        return False
+
+
+__all__ = ["KeyPoint", "CudaStuff", "Context", "Batch", "getKeypoints", "downloadKeypoints",
+           "uploadKeypoints", "makeLambdasLog", "makeLambdasLin", "snapTransformSize", "detect_host",
+           "keypoint_matrix_to_records", "default_params", "KP_MAX_POINTS"]
+
+if sys.version_info < (3, 8):  # pragma: no cover
+    raise RuntimeError("python >= 3.8 required")

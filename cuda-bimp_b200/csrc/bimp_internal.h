@@ -1,0 +1,87 @@
+// Internal structures shared by the host bank builder, the kernels and the
+// C ABI.  Not part of the public interface.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "bimp_b200.h"
+
+namespace bimp_b200 {
+
+constexpr int kNumOri = 8;
+// Overlap-save tile: 128 x 128 complex FFT held in shared memory.
+constexpr int kTile = 128;
+constexpr int kTileLD = 136;               // complex row stride of the work buffer
+constexpr int kXhCols = 65;                // Hermitian half: kx = 0..64
+constexpr int kTileThreads = 512;
+constexpr int kMaxHalf = 56;               // largest supported kernel half size
+constexpr int kSpecFloats = kTile * kTile; // one orientation's real spectrum
+
+// Per (image, scale) descriptor read by every kernel.  Plain old data.
+struct ScaleDev {
+  // geometry (cuda_bimp.cu:249-256)
+  int dataW, dataH, fftW, fftH;
+  int kX;          // kernel half size == kernelX == kernelY
+  int V;           // valid outputs per tile side = kTile - 2*kX
+  int tilesX, tilesY;
+  int cRows, cCols;  // complex-cell window stored: (dataH+2) x (dataW+1)
+  int wrapW;         // fftW == dataW: column dataW reads the next row's column 0
+  // level image (uint8, full pyrDown size lvlW x lvlH)
+  const uint8_t* lvl;
+  int lvlPitch, lvlW, lvlH;
+  // real tile spectra, kNumOri x kTile x kTile floats in (py, px) order
+  const float* G;
+  // complex-cell maps: kNumOri maps, each cRows x cPitch floats
+  float* C;
+  int cPitch;
+  long long cStride;
+  // stencil offsets (cuda_bimp.cu:533-550)
+  int es1[kNumOri], es2[kNumOri];   // end-stop (row, col)
+  int in1[kNumOri], in2[kNumOri];   // inhibition (row, col)
+  int ih1[kNumOri], ih2[kNumOri];   // radial half offsets round(0.5*in)
+  float radialGain, wTan, wRad;
+  // dense maps: dataH x dPitch floats
+  float* D;
+  float* S;
+  int dPitch;
+  unsigned int* maxKey;   // order-preserving key of max(D)
+  // keypoints (cuda_bimp.cu:737-740)
+  int off;                // (int)lambda
+  float pyrstep;
+  float kpSize;           // lambda*pyrstep
+  int kpOctave;           // (int)(lambda*pyrstep)
+  float threshRatio;
+  int rowBase;            // first entry of this scale in the per-row count array
+  int image;              // image index inside a batch
+};
+
+// One unit of tiled-FFT work: tile `tile` of descriptor `entry`.
+struct TileWork {
+  int entry;
+  int tile;
+};
+
+// Host-side description of one scale (geometry + bank).
+struct ScaleHost {
+  float lambda2, lambda, pyrstep, filtersize;
+  int kW, kX, dataW, dataH, fftW, fftH, level, off;
+  int es1[kNumOri], es2[kNumOri], in1[kNumOri], in2[kNumOri];
+  std::vector<float> even[kNumOri], odd[kNumOri];   // kW x kW taps
+  std::vector<float> spectrum;                       // kNumOri x kTile x kTile
+};
+
+// Reference-equivalent helpers (bank.cpp).
+int snap_transform_size(int n);
+std::vector<float> make_lambdas_log(float start, float end, int spo);
+std::vector<float> make_lambdas_lin(float start, float end, int n);
+bool build_scales(int width, int height, const std::vector<float>& lambdas,
+                  const bimp_params& p, std::vector<ScaleHost>& out, std::string& err);
+void tile_spectrum(const ScaleHost& s, std::vector<float>& out);
+
+// Position of natural frequency k in the digit-permuted 128-point layout.
+inline int perm128(int k) { return 8 * (k & 15) + (k >> 4); }
+
+}  // namespace bimp_b200

@@ -1,0 +1,799 @@
+// C ABI of the B200 BIMP detector: contexts (one image size), batches (many
+// images of mixed sizes, one launch per kernel type, replayed as a CUDA
+// graph), dense-map access and keypoint conversion.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bimp_b200.h"
+#include "bimp_b200_batch.h"
+#include "bimp_internal.h"
+#include "kernels.h"
+
+using namespace bimp_b200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define BIMP_CUDA(call)                                                              \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      return fail(e_ == cudaErrorMemoryAllocation ? BIMP_ERR_NOMEM : BIMP_ERR_CUDA,  \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    }                                                                                \
+  } while (0)
+
+std::mutex g_cfg_mutex;
+bool g_cfg_done[128];
+
+int ensure_device_configured(int dev) {
+  std::lock_guard<std::mutex> lk(g_cfg_mutex);
+  if (dev < 0 || dev >= 128) return fail(BIMP_ERR_NO_DEVICE, "device index out of range");
+  if (g_cfg_done[dev]) return BIMP_OK;
+  cudaDeviceProp prop;
+  BIMP_CUDA(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major != 10) return fail(BIMP_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
+  BIMP_CUDA(configure_kernels());
+  g_cfg_done[dev] = true;
+  return BIMP_OK;
+}
+
+bimp_params default_params() {
+  bimp_params p;
+  p.gamma = 0.5;
+  p.sigma_ratio = 0.56;
+  p.size_ratio = 7.0;
+  p.offset_ratio = 0.6;
+  p.level_max = 7.5;
+  p.radial_gain = 16.0;
+  p.w_tan = 1.0;
+  p.w_rad = 1.0;
+  p.thresh_ratio = 0.104;
+  return p;
+}
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+int round_half_away(double v) {
+  return static_cast<int>(v >= 0 ? std::floor(v + 0.5) : -std::floor(-v + 0.5));
+}
+
+// Bump allocator over one device allocation.
+struct Arena {
+  size_t size = 0;
+  char* base = nullptr;
+  size_t reserve(size_t bytes) {
+    const size_t at = align_up(size, 256);
+    size = at + bytes;
+    return at;
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// shared engine: N images with their own sizes, one wavelength bank
+// ---------------------------------------------------------------------------
+struct Engine {
+  int device = 0;
+  bimp_params params{};
+  std::vector<ScaleHost> bank;          // geometry of the first image size + taps
+  int nScales = 0;
+  int nImages = 0;
+  std::vector<int> widths, heights;
+  std::vector<std::vector<ScaleHost>> geo;   // per image per scale geometry
+  // device memory
+  char* d_mem = nullptr;
+  size_t memBytes = 0;
+  float* d_G = nullptr;
+  std::vector<std::vector<uint8_t*>> lvl;    // per image per level
+  std::vector<std::vector<int>> lvlW, lvlH, lvlP;
+  std::vector<ScaleDev> h_sd;
+  ScaleDev* d_sd = nullptr;
+  TileWork* d_tiles = nullptr;
+  int nTiles = 0;
+  int2* d_sten = nullptr;
+  int nSten = 0;
+  int2* d_rows = nullptr;
+  int nRows = 0;
+  int* d_counts = nullptr;
+  int* d_offsets = nullptr;
+  int* d_imgRowStart = nullptr;
+  int* d_totals = nullptr;
+  unsigned int* d_maxKeys = nullptr;
+  KpOut* d_outs = nullptr;
+  std::vector<PyrJob> h_pyr;                 // grouped by level
+  std::vector<int> pyrFirst, pyrCount, pyrMaxW, pyrMaxH;
+  PyrJob* d_pyr = nullptr;
+  std::vector<size_t> imgKpOffset;           // internal keypoint buffers (batch)
+  float* d_kpInternal = nullptr;
+  int kpCapInternal = 0;
+
+  int build(int dev, const int* w, const int* h, int n, const float* lambdas, int nl,
+            const bimp_params& p, int internalKpCap) {
+    device = dev;
+    params = p;
+    nImages = n;
+    widths.assign(w, w + n);
+    heights.assign(h, h + n);
+    std::vector<float> lam(lambdas, lambdas + nl);
+    std::string err;
+    geo.resize(n);
+    for (int i = 0; i < n; ++i) {
+      if (w[i] < 2 || h[i] < 2) return fail(BIMP_ERR_INVALID, "image size must be at least 2x2");
+      if (!build_scales(w[i], h[i], lam, p, geo[i], err)) return fail(BIMP_ERR_INVALID, err);
+      if (i == 0) bank = geo[0];
+      for (auto& s : geo[i]) {        // taps and spectra are shared with image 0
+        for (int o = 0; o < kNumOri; ++o) { s.even[o].clear(); s.odd[o].clear(); }
+        if (i > 0) s.spectrum.clear();
+      }
+    }
+    for (auto& s : geo[0]) s.spectrum.clear();
+    nScales = static_cast<int>(bank.size());
+
+    // ---- layout
+    Arena a;
+    const size_t offG = a.reserve(sizeof(float) * (size_t)nScales * kNumOri * kSpecFloats);
+    lvl.assign(n, {});
+    lvlW.assign(n, {});
+    lvlH.assign(n, {});
+    lvlP.assign(n, {});
+    std::vector<std::vector<size_t>> offLvl(n);
+    std::vector<std::vector<size_t>> offC(n), offD(n), offS(n);
+    int maxLevel = 0;
+    for (auto& s : bank) maxLevel = std::max(maxLevel, s.level);
+    for (int i = 0; i < n; ++i) {
+      int cw = w[i], ch = h[i];
+      for (int l = 0; l <= maxLevel; ++l) {
+        if (l > 0) { cw = (cw + 1) / 2; ch = (ch + 1) / 2; }
+        const int pitch = static_cast<int>(align_up(cw, 16));
+        lvlW[i].push_back(cw);
+        lvlH[i].push_back(ch);
+        lvlP[i].push_back(pitch);
+        offLvl[i].push_back(a.reserve((size_t)pitch * ch));
+      }
+      for (auto& s : geo[i]) {
+        const int cPitch = static_cast<int>(align_up(s.dataW + 1, 32));
+        offC[i].push_back(a.reserve(sizeof(float) * (size_t)kNumOri * (s.dataH + 2) * cPitch));
+        const int dPitch = static_cast<int>(align_up(s.dataW, 32));
+        offD[i].push_back(a.reserve(sizeof(float) * (size_t)s.dataH * dPitch));
+        offS[i].push_back(a.reserve(sizeof(float) * (size_t)s.dataH * dPitch));
+      }
+    }
+    // work lists
+    std::vector<TileWork> tiles;
+    std::vector<int2> sten, rows;
+    std::vector<int> imgRowStart;
+    std::vector<ScaleDev> sds;
+    for (int i = 0; i < n; ++i) {
+      imgRowStart.push_back(static_cast<int>(rows.size()));
+      for (int si = 0; si < nScales; ++si) {
+        const ScaleHost& s = geo[i][si];
+        ScaleDev d;
+        std::memset(&d, 0, sizeof(d));
+        d.dataW = s.dataW; d.dataH = s.dataH; d.fftW = s.fftW; d.fftH = s.fftH;
+        d.kX = s.kX;
+        d.V = kTile - 2 * s.kX;
+        d.cRows = s.dataH + 2;
+        d.cCols = s.dataW + 1;
+        d.tilesX = (d.cCols + d.V - 1) / d.V;
+        d.tilesY = (d.cRows + d.V - 1) / d.V;
+        d.wrapW = s.fftW == s.dataW ? 1 : 0;
+        d.lvlW = lvlW[i][s.level];
+        d.lvlH = lvlH[i][s.level];
+        d.lvlPitch = lvlP[i][s.level];
+        d.cPitch = static_cast<int>(align_up(s.dataW + 1, 32));
+        d.cStride = (long long)(s.dataH + 2) * d.cPitch;
+        for (int o = 0; o < kNumOri; ++o) {
+          d.es1[o] = s.es1[o]; d.es2[o] = s.es2[o];
+          d.in1[o] = s.in1[o]; d.in2[o] = s.in2[o];
+          d.ih1[o] = round_half_away(0.5 * s.in1[o]);   // cuda_bimp.cuh:495-496
+          d.ih2[o] = round_half_away(0.5 * s.in2[o]);
+        }
+        d.radialGain = static_cast<float>(p.radial_gain);
+        d.wTan = static_cast<float>(p.w_tan);
+        d.wRad = static_cast<float>(p.w_rad);
+        d.dPitch = static_cast<int>(align_up(s.dataW, 32));
+        d.off = s.off;
+        d.pyrstep = s.pyrstep;
+        d.kpSize = s.lambda * s.pyrstep;
+        d.kpOctave = static_cast<int>(s.lambda * s.pyrstep);
+        d.threshRatio = static_cast<float>(p.thresh_ratio);
+        d.image = i;
+        const int entry = static_cast<int>(sds.size());
+        d.rowBase = static_cast<int>(rows.size());
+        for (int tIdx = 0; tIdx < d.tilesX * d.tilesY; ++tIdx) tiles.push_back({entry, tIdx});
+        const int nbx = (s.dataW + 31) / 32, nby = (s.dataH + 31) / 32;
+        for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
+        const int yEnd = std::min(s.dataH - s.off - 1, s.dataH - 2);
+        for (int y = s.off + 1; y <= yEnd; ++y) rows.push_back(make_int2(entry, y - s.off - 1));
+        sds.push_back(d);
+      }
+    }
+    imgRowStart.push_back(static_cast<int>(rows.size()));
+    // pyramid jobs grouped by level
+    pyrFirst.clear(); pyrCount.clear(); pyrMaxW.clear(); pyrMaxH.clear(); h_pyr.clear();
+    for (int l = 1; l <= maxLevel; ++l) {
+      pyrFirst.push_back(static_cast<int>(h_pyr.size()));
+      int mw = 0, mh = 0;
+      for (int i = 0; i < n; ++i) {
+        PyrJob j;
+        j.sw = lvlW[i][l - 1]; j.sh = lvlH[i][l - 1]; j.sp = lvlP[i][l - 1];
+        j.dw = lvlW[i][l]; j.dh = lvlH[i][l]; j.dp = lvlP[i][l];
+        j.src = nullptr; j.dst = nullptr;
+        h_pyr.push_back(j);
+        mw = std::max(mw, j.dw); mh = std::max(mh, j.dh);
+      }
+      pyrCount.push_back(n);
+      pyrMaxW.push_back(mw);
+      pyrMaxH.push_back(mh);
+    }
+    nTiles = static_cast<int>(tiles.size());
+    nSten = static_cast<int>(sten.size());
+    nRows = static_cast<int>(rows.size());
+    const size_t offSd = a.reserve(sizeof(ScaleDev) * sds.size());
+    const size_t offTiles = a.reserve(sizeof(TileWork) * std::max<size_t>(1, tiles.size()));
+    const size_t offSten = a.reserve(sizeof(int2) * std::max<size_t>(1, sten.size()));
+    const size_t offRows = a.reserve(sizeof(int2) * std::max<size_t>(1, rows.size()));
+    const size_t offCounts = a.reserve(sizeof(int) * std::max<size_t>(1, rows.size()));
+    const size_t offOffsets = a.reserve(sizeof(int) * std::max<size_t>(1, rows.size()));
+    const size_t offImgRow = a.reserve(sizeof(int) * imgRowStart.size());
+    const size_t offTotals = a.reserve(sizeof(int) * n);
+    const size_t offMax = a.reserve(sizeof(unsigned int) * sds.size());
+    const size_t offOuts = a.reserve(sizeof(KpOut) * n);
+    const size_t offPyr = a.reserve(sizeof(PyrJob) * std::max<size_t>(1, h_pyr.size()));
+    size_t offKp = 0;
+    kpCapInternal = internalKpCap;
+    if (internalKpCap > 0)
+      offKp = a.reserve(sizeof(float) * (size_t)n * BIMP_KP_VECTOR_LENGTH * internalKpCap);
+
+    memBytes = a.size;
+    cudaError_t e = cudaMalloc(&d_mem, memBytes);
+    if (e != cudaSuccess) {
+      d_mem = nullptr;
+      return fail(BIMP_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(memBytes) +
+                                      " bytes: " + cudaGetErrorString(e));
+    }
+    char* base = d_mem;
+    d_G = reinterpret_cast<float*>(base + offG);
+    for (int i = 0; i < n; ++i) {
+      for (size_t l = 0; l < offLvl[i].size(); ++l)
+        lvl[i].push_back(reinterpret_cast<uint8_t*>(base + offLvl[i][l]));
+    }
+    for (int i = 0, e2 = 0; i < n; ++i) {
+      for (int si = 0; si < nScales; ++si, ++e2) {
+        ScaleDev& d = sds[e2];
+        const ScaleHost& s = geo[i][si];
+        d.lvl = lvl[i][s.level];
+        d.G = d_G + (size_t)si * kNumOri * kSpecFloats;
+        d.C = reinterpret_cast<float*>(base + offC[i][si]);
+        d.D = reinterpret_cast<float*>(base + offD[i][si]);
+        d.S = reinterpret_cast<float*>(base + offS[i][si]);
+        d.maxKey = reinterpret_cast<unsigned int*>(base + offMax) + e2;
+      }
+    }
+    for (int l = 1, k = 0; l <= maxLevel; ++l)
+      for (int i = 0; i < n; ++i, ++k) {
+        h_pyr[k].src = lvl[i][l - 1];
+        h_pyr[k].dst = lvl[i][l];
+      }
+    h_sd = sds;
+    d_sd = reinterpret_cast<ScaleDev*>(base + offSd);
+    d_tiles = reinterpret_cast<TileWork*>(base + offTiles);
+    d_sten = reinterpret_cast<int2*>(base + offSten);
+    d_rows = reinterpret_cast<int2*>(base + offRows);
+    d_counts = reinterpret_cast<int*>(base + offCounts);
+    d_offsets = reinterpret_cast<int*>(base + offOffsets);
+    d_imgRowStart = reinterpret_cast<int*>(base + offImgRow);
+    d_totals = reinterpret_cast<int*>(base + offTotals);
+    d_maxKeys = reinterpret_cast<unsigned int*>(base + offMax);
+    d_outs = reinterpret_cast<KpOut*>(base + offOuts);
+    d_pyr = reinterpret_cast<PyrJob*>(base + offPyr);
+    d_kpInternal = internalKpCap > 0 ? reinterpret_cast<float*>(base + offKp) : nullptr;
+
+    // ---- uploads (setup only)
+    for (int si = 0; si < nScales; ++si)
+      BIMP_CUDA(cudaMemcpy(d_G + (size_t)si * kNumOri * kSpecFloats, bank[si].spectrum.data(),
+                           sizeof(float) * kNumOri * kSpecFloats, cudaMemcpyHostToDevice));
+    for (auto& s : bank) { s.spectrum.clear(); s.spectrum.shrink_to_fit(); }
+    BIMP_CUDA(cudaMemcpy(d_sd, sds.data(), sizeof(ScaleDev) * sds.size(), cudaMemcpyHostToDevice));
+    if (!tiles.empty())
+      BIMP_CUDA(cudaMemcpy(d_tiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice));
+    if (!sten.empty())
+      BIMP_CUDA(cudaMemcpy(d_sten, sten.data(), sizeof(int2) * sten.size(), cudaMemcpyHostToDevice));
+    if (!rows.empty())
+      BIMP_CUDA(cudaMemcpy(d_rows, rows.data(), sizeof(int2) * rows.size(), cudaMemcpyHostToDevice));
+    BIMP_CUDA(cudaMemcpy(d_imgRowStart, imgRowStart.data(), sizeof(int) * imgRowStart.size(),
+                         cudaMemcpyHostToDevice));
+    if (!h_pyr.empty())
+      BIMP_CUDA(cudaMemcpy(d_pyr, h_pyr.data(), sizeof(PyrJob) * h_pyr.size(), cudaMemcpyHostToDevice));
+    if (internalKpCap > 0) {
+      std::vector<KpOut> outs(n);
+      for (int i = 0; i < n; ++i) {
+        outs[i].kp = d_kpInternal + (size_t)i * BIMP_KP_VECTOR_LENGTH * internalKpCap;
+        outs[i].ld = internalKpCap;
+        outs[i].capacity = internalKpCap;
+        outs[i].pad_ = 0;
+      }
+      BIMP_CUDA(cudaMemcpy(d_outs, outs.data(), sizeof(KpOut) * n, cudaMemcpyHostToDevice));
+    }
+    BIMP_CUDA(cudaMemset(d_maxKeys, 0, sizeof(unsigned int) * sds.size()));
+    return BIMP_OK;
+  }
+
+  int stage(int which, cudaStream_t s) {
+    switch (which) {
+      case 0:
+        for (size_t l = 0; l < pyrFirst.size(); ++l)
+          launch_pyr(d_pyr + pyrFirst[l], pyrCount[l], pyrMaxW[l], pyrMaxH[l], s);
+        break;
+      case 1:
+        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, nTiles, s);
+        break;
+      case 2:
+        if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, s);
+        break;
+      case 3:
+        launch_nms(d_sd, d_rows, nRows, d_counts, d_offsets, d_imgRowStart, nImages, d_totals, d_outs, s);
+        break;
+      default:
+        return fail(BIMP_ERR_INVALID, "unknown stage");
+    }
+    BIMP_CUDA(cudaGetLastError());
+    return BIMP_OK;
+  }
+
+  int kernel_launches() const {
+    return static_cast<int>(pyrFirst.size()) + (nTiles > 0) + (nSten > 0) + 1 + 2 * (nRows > 0);
+  }
+
+  // Everything after the level-0 images are in place.
+  int enqueue(cudaStream_t s) {
+    int rc = stage(0, s);
+    if (rc != BIMP_OK) return rc;
+    BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, sizeof(unsigned int) * h_sd.size(), s));
+    for (int k = 1; k <= 3; ++k) {
+      rc = stage(k, s);
+      if (rc != BIMP_OK) return rc;
+    }
+    return BIMP_OK;
+  }
+
+  void release() {
+    if (d_mem) cudaFree(d_mem);
+    d_mem = nullptr;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// context: one image size
+// ---------------------------------------------------------------------------
+struct bimp_context {
+  Engine eng;
+  int width = 0, height = 0;
+  std::vector<ScaleHost> info;
+  // pinned staging for the host path
+  bimp_keypoint* h_kp = nullptr;
+  int h_kpCap = 0;
+  bimp_keypoint* d_aos = nullptr;
+  int d_aosCap = 0;
+  int* h_count = nullptr;
+  float* d_kpScratch = nullptr;
+  int d_kpScratchCap = 0;
+};
+
+struct bimp_batch {
+  Engine eng;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t capStream = nullptr;
+  int* h_totals = nullptr;
+  std::vector<bimp_keypoint> tmp;
+};
+
+extern "C" {
+
+const char* bimp_version(void) { return "bimp_b200 0.1 (sm_100a)"; }
+const char* bimp_last_error(void) { return g_last_error.c_str(); }
+void bimp_default_params(bimp_params* p) {
+  if (p) *p = default_params();
+}
+
+int bimp_make_lambdas_log(float start, float end, int spo, float* out, int cap, int* n) {
+  if (!n || spo <= 0 || !(start > 0.f)) return fail(BIMP_ERR_INVALID, "bad makeLambdasLog arguments");
+  const std::vector<float> v = make_lambdas_log(start, end, spo);
+  *n = static_cast<int>(v.size());
+  if (out)
+    for (int i = 0; i < std::min(cap, *n); ++i) out[i] = v[i];
+  return BIMP_OK;
+}
+
+int bimp_make_lambdas_lin(float start, float end, int num, float* out, int cap, int* n) {
+  if (!n || num <= 0) return fail(BIMP_ERR_INVALID, "bad makeLambdasLin arguments");
+  const std::vector<float> v = make_lambdas_lin(start, end, num);
+  *n = static_cast<int>(v.size());
+  if (out)
+    for (int i = 0; i < std::min(cap, *n); ++i) out[i] = v[i];
+  return BIMP_OK;
+}
+
+int bimp_snap_transform_size(int n) { return snap_transform_size(n); }
+
+int bimp_ctx_create(bimp_context** ctx, int width, int height, const float* lambdas, int n_lambdas,
+                    const bimp_params* params) {
+  if (!ctx) return fail(BIMP_ERR_INVALID, "ctx is null");
+  *ctx = nullptr;
+  if (!lambdas || n_lambdas <= 0) return fail(BIMP_ERR_INVALID, "empty wavelength list");
+  if (width < 2 || height < 2) return fail(BIMP_ERR_INVALID, "image size must be at least 2x2");
+  int dev = 0;
+  BIMP_CUDA(cudaGetDevice(&dev));
+  int rc = ensure_device_configured(dev);
+  if (rc != BIMP_OK) return rc;
+  bimp_context* c = new bimp_context();
+  c->width = width;
+  c->height = height;
+  const bimp_params p = params ? *params : default_params();
+  rc = c->eng.build(dev, &width, &height, 1, lambdas, n_lambdas, p, 0);
+  if (rc != BIMP_OK) {
+    c->eng.release();
+    delete c;
+    return rc;
+  }
+  c->info = c->eng.geo[0];
+  cudaError_t e = cudaMallocHost(&c->h_count, sizeof(int));
+  if (e != cudaSuccess) {
+    c->eng.release();
+    delete c;
+    return fail(BIMP_ERR_NOMEM, "cudaMallocHost failed");
+  }
+  *ctx = c;
+  return BIMP_OK;
+}
+
+int bimp_ctx_destroy(bimp_context* c) {
+  if (!c) return BIMP_OK;
+  cudaSetDevice(c->eng.device);
+  c->eng.release();
+  if (c->h_kp) cudaFreeHost(c->h_kp);
+  if (c->h_count) cudaFreeHost(c->h_count);
+  if (c->d_aos) cudaFree(c->d_aos);
+  if (c->d_kpScratch) cudaFree(c->d_kpScratch);
+  delete c;
+  return BIMP_OK;
+}
+
+int bimp_ctx_num_scales(const bimp_context* c) { return c ? c->eng.nScales : 0; }
+
+int bimp_ctx_scale_info(const bimp_context* c, int s, bimp_scale_info* out) {
+  if (!c || !out || s < 0 || s >= c->eng.nScales) return fail(BIMP_ERR_INVALID, "bad scale index");
+  const ScaleHost& h = c->info[s];
+  out->lambda_full = h.lambda2;
+  out->lambda_level = h.lambda;
+  out->pyrstep = h.pyrstep;
+  out->kernel_w = h.kW;
+  out->kernel_x = h.kX;
+  out->data_w = h.dataW;
+  out->data_h = h.dataH;
+  out->fft_w = h.fftW;
+  out->fft_h = h.fftH;
+  out->margin = h.off;
+  return BIMP_OK;
+}
+
+static int ctx_run(bimp_context* c, const uint8_t* image, size_t pitch, int width, int height,
+                   cudaMemcpyKind kind, float* d_kp, size_t ld, int capacity, int* d_count,
+                   cudaStream_t s) {
+  if (!c || !image) return fail(BIMP_ERR_INVALID, "null argument");
+  if (width != c->width || height != c->height)
+    return fail(BIMP_ERR_INVALID, "image size differs from the context's");
+  if (pitch < (size_t)width) return fail(BIMP_ERR_INVALID, "pitch smaller than width");
+  if (capacity < 0) return fail(BIMP_ERR_INVALID, "negative capacity");
+  if (capacity > 0 && (!d_kp || ld < (size_t)capacity)) return fail(BIMP_ERR_INVALID, "bad keypoint matrix");
+  BIMP_CUDA(cudaSetDevice(c->eng.device));
+  Engine& e = c->eng;
+  BIMP_CUDA(cudaMemcpy2DAsync(e.lvl[0][0], e.lvlP[0][0], image, pitch, width, height, kind, s));
+  KpOut o;
+  o.kp = d_kp;
+  o.ld = ld;
+  o.capacity = capacity;
+  o.pad_ = 0;
+  BIMP_CUDA(cudaMemcpyAsync(e.d_outs, &o, sizeof(o), cudaMemcpyHostToDevice, s));
+  int rc = e.enqueue(s);
+  if (rc != BIMP_OK) return rc;
+  if (d_count) BIMP_CUDA(cudaMemcpyAsync(d_count, e.d_totals, sizeof(int), cudaMemcpyDeviceToDevice, s));
+  return BIMP_OK;
+}
+
+int bimp_detect_device_async(bimp_context* c, const uint8_t* d_image, size_t pitch, int width,
+                             int height, float* d_kp, size_t ld, int capacity, int* d_count,
+                             void* stream) {
+  return ctx_run(c, d_image, pitch, width, height, cudaMemcpyDeviceToDevice, d_kp, ld, capacity,
+                 d_count, static_cast<cudaStream_t>(stream));
+}
+
+int bimp_detect_device(bimp_context* c, const uint8_t* d_image, size_t pitch, int width, int height,
+                       float* d_kp, size_t ld, int capacity, int* n_found, void* stream) {
+  if (!n_found) return fail(BIMP_ERR_INVALID, "n_found is null");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = ctx_run(c, d_image, pitch, width, height, cudaMemcpyDeviceToDevice, d_kp, ld, capacity,
+                   nullptr, s);
+  if (rc != BIMP_OK) return rc;
+  BIMP_CUDA(cudaMemcpyAsync(c->h_count, c->eng.d_totals, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIMP_CUDA(cudaStreamSynchronize(s));
+  *n_found = *c->h_count;
+  if (*n_found > capacity)
+    return fail(BIMP_ERR_CAPACITY, "keypoints exceed capacity (" + std::to_string(*n_found) + ")");
+  return BIMP_OK;
+}
+
+static int ensure_host_buffers(bimp_context* c, int capacity) {
+  if (c->d_kpScratchCap < capacity) {
+    if (c->d_kpScratch) cudaFree(c->d_kpScratch);
+    c->d_kpScratch = nullptr;
+    c->d_kpScratchCap = 0;
+    BIMP_CUDA(cudaMalloc(&c->d_kpScratch, sizeof(float) * BIMP_KP_VECTOR_LENGTH * (size_t)capacity));
+    c->d_kpScratchCap = capacity;
+  }
+  if (c->h_kpCap < capacity) {
+    if (c->h_kp) cudaFreeHost(c->h_kp);
+    c->h_kp = nullptr;
+    c->h_kpCap = 0;
+    BIMP_CUDA(cudaMallocHost(&c->h_kp, sizeof(float) * BIMP_KP_VECTOR_LENGTH * (size_t)capacity));
+    c->h_kpCap = capacity;
+  }
+  return BIMP_OK;
+}
+
+int bimp_detect_host(bimp_context* c, const uint8_t* image, size_t pitch, int width, int height,
+                     bimp_keypoint* out, int capacity, int* n_found, void* stream) {
+  if (!c || !n_found || capacity < 0 || (capacity > 0 && !out))
+    return fail(BIMP_ERR_INVALID, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BIMP_CUDA(cudaSetDevice(c->eng.device));
+  const int cap = std::max(capacity, 1);
+  int rc = ensure_host_buffers(c, cap);
+  if (rc != BIMP_OK) return rc;
+  rc = ctx_run(c, image, pitch, width, height, cudaMemcpyHostToDevice, c->d_kpScratch, cap,
+               capacity, nullptr, s);
+  if (rc != BIMP_OK) return rc;
+  BIMP_CUDA(cudaMemcpyAsync(c->h_count, c->eng.d_totals, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIMP_CUDA(cudaStreamSynchronize(s));
+  const int total = *c->h_count;
+  const int n = std::min(total, capacity);
+  if (n > 0) {
+    float* hk = reinterpret_cast<float*>(c->h_kp);
+    BIMP_CUDA(cudaMemcpy2DAsync(hk, sizeof(float) * n, c->d_kpScratch, sizeof(float) * cap,
+                                sizeof(float) * n, BIMP_KP_VECTOR_LENGTH, cudaMemcpyDeviceToHost, s));
+    BIMP_CUDA(cudaStreamSynchronize(s));
+    for (int j = 0; j < n; ++j) {
+      bimp_keypoint& k = out[j];
+      k.x = hk[BIMP_X_ROW * n + j];
+      k.y = hk[BIMP_Y_ROW * n + j];
+      std::memcpy(&k.class_id, &hk[BIMP_LAPLACIAN_ROW * n + j], 4);
+      std::memcpy(&k.octave, &hk[BIMP_OCTAVE_ROW * n + j], 4);
+      k.size = hk[BIMP_SIZE_ROW * n + j];
+      k.angle = hk[BIMP_ANGLE_ROW * n + j];
+      k.response = hk[BIMP_HESSIAN_ROW * n + j];
+    }
+  }
+  *n_found = total;
+  if (total > capacity)
+    return fail(BIMP_ERR_CAPACITY, "keypoints exceed capacity (" + std::to_string(total) + ")");
+  return BIMP_OK;
+}
+
+int bimp_dense_map(bimp_context* c, int scale, int which, float* d_out, size_t ld, void* stream) {
+  if (!c || !d_out || scale < 0 || scale >= c->eng.nScales || which < 0 || which > 1)
+    return fail(BIMP_ERR_INVALID, "bad dense-map arguments");
+  const ScaleDev& d = c->eng.h_sd[scale];
+  if (ld < (size_t)d.dataW) return fail(BIMP_ERR_INVALID, "ld smaller than data width");
+  BIMP_CUDA(cudaSetDevice(c->eng.device));
+  const float* src = which == 0 ? d.D : d.S;
+  BIMP_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), src, d.dPitch * sizeof(float),
+                              d.dataW * sizeof(float), d.dataH, cudaMemcpyDeviceToDevice,
+                              static_cast<cudaStream_t>(stream)));
+  return BIMP_OK;
+}
+
+int bimp_complex_map(bimp_context* c, int scale, int o, float* d_out, size_t ld, void* stream) {
+  if (!c || !d_out || scale < 0 || scale >= c->eng.nScales || o < 0 || o >= kNumOri)
+    return fail(BIMP_ERR_INVALID, "bad complex-map arguments");
+  const ScaleDev& d = c->eng.h_sd[scale];
+  if (ld < (size_t)d.cCols) return fail(BIMP_ERR_INVALID, "ld smaller than data width + 1");
+  BIMP_CUDA(cudaSetDevice(c->eng.device));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float* src = d.C + (size_t)o * d.cStride;
+  BIMP_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), src, d.cPitch * sizeof(float),
+                              d.cCols * sizeof(float), d.dataH + 1, cudaMemcpyDeviceToDevice, s));
+  if (d.wrapW) {
+    // the stencils address y*fftW + x: with fftW == dataW, column dataW is
+    // the next row's column 0
+    BIMP_CUDA(cudaMemcpy2DAsync(d_out + d.dataW, ld * sizeof(float), src + d.cPitch,
+                                d.cPitch * sizeof(float), sizeof(float), d.dataH + 1,
+                                cudaMemcpyDeviceToDevice, s));
+  }
+  return BIMP_OK;
+}
+
+int bimp_ctx_kernel_launches(const bimp_context* c) { return c ? c->eng.kernel_launches() : 0; }
+
+int bimp_ctx_run_stage(bimp_context* c, int stage, void* stream) {
+  if (!c) return fail(BIMP_ERR_INVALID, "ctx is null");
+  BIMP_CUDA(cudaSetDevice(c->eng.device));
+  return c->eng.stage(stage, static_cast<cudaStream_t>(stream));
+}
+
+int bimp_download_keypoints(const float* d_kp, size_t ld, int n, bimp_keypoint* out, void* stream) {
+  if (n < 0 || (n > 0 && (!d_kp || !out || ld < (size_t)n)))
+    return fail(BIMP_ERR_INVALID, "bad download arguments");
+  if (n == 0) return BIMP_OK;
+  std::vector<float> h((size_t)BIMP_KP_VECTOR_LENGTH * n);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BIMP_CUDA(cudaMemcpy2DAsync(h.data(), sizeof(float) * n, d_kp, sizeof(float) * ld, sizeof(float) * n,
+                              BIMP_KP_VECTOR_LENGTH, cudaMemcpyDeviceToHost, s));
+  BIMP_CUDA(cudaStreamSynchronize(s));
+  for (int j = 0; j < n; ++j) {
+    bimp_keypoint& k = out[j];
+    k.x = h[BIMP_X_ROW * n + j];
+    k.y = h[BIMP_Y_ROW * n + j];
+    std::memcpy(&k.class_id, &h[BIMP_LAPLACIAN_ROW * n + j], 4);
+    std::memcpy(&k.octave, &h[BIMP_OCTAVE_ROW * n + j], 4);
+    k.size = h[BIMP_SIZE_ROW * n + j];
+    k.angle = h[BIMP_ANGLE_ROW * n + j];
+    k.response = h[BIMP_HESSIAN_ROW * n + j];
+  }
+  return BIMP_OK;
+}
+
+int bimp_upload_keypoints(const bimp_keypoint* kps, int n, float* d_kp, size_t ld, void* stream) {
+  if (n < 0 || (n > 0 && (!kps || !d_kp || ld < (size_t)n)))
+    return fail(BIMP_ERR_INVALID, "bad upload arguments");
+  if (n == 0) return BIMP_OK;
+  std::vector<float> h((size_t)BIMP_KP_VECTOR_LENGTH * n);
+  for (int j = 0; j < n; ++j) {
+    const bimp_keypoint& k = kps[j];
+    h[BIMP_X_ROW * n + j] = k.x;
+    h[BIMP_Y_ROW * n + j] = k.y;
+    h[BIMP_SIZE_ROW * n + j] = k.size;
+    h[BIMP_ANGLE_ROW * n + j] = k.angle;
+    h[BIMP_HESSIAN_ROW * n + j] = k.response;
+    std::memcpy(&h[BIMP_OCTAVE_ROW * n + j], &k.octave, 4);
+    const int one = 1;   // utils.cpp:126 writes LAPLACIAN = 1
+    std::memcpy(&h[BIMP_LAPLACIAN_ROW * n + j], &one, 4);
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BIMP_CUDA(cudaMemcpy2DAsync(d_kp, sizeof(float) * ld, h.data(), sizeof(float) * n, sizeof(float) * n,
+                              BIMP_KP_VECTOR_LENGTH, cudaMemcpyHostToDevice, s));
+  BIMP_CUDA(cudaStreamSynchronize(s));
+  return BIMP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+int bimp_batch_create(bimp_batch** out, const int* widths, const int* heights, int n_images,
+                      const float* lambdas, int n_lambdas, const bimp_params* params, int kp_capacity) {
+  if (!out) return fail(BIMP_ERR_INVALID, "batch is null");
+  *out = nullptr;
+  if (!widths || !heights || n_images <= 0 || !lambdas || n_lambdas <= 0 || kp_capacity <= 0)
+    return fail(BIMP_ERR_INVALID, "bad batch arguments");
+  int dev = 0;
+  BIMP_CUDA(cudaGetDevice(&dev));
+  int rc = ensure_device_configured(dev);
+  if (rc != BIMP_OK) return rc;
+  bimp_batch* b = new bimp_batch();
+  const bimp_params p = params ? *params : default_params();
+  rc = b->eng.build(dev, widths, heights, n_images, lambdas, n_lambdas, p, kp_capacity);
+  if (rc != BIMP_OK) {
+    b->eng.release();
+    delete b;
+    return rc;
+  }
+  cudaError_t e = cudaMallocHost(&b->h_totals, sizeof(int) * n_images);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capStream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(b->capStream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const int rc2 = b->eng.enqueue(b->capStream);
+    cudaError_t e2 = cudaStreamEndCapture(b->capStream, &b->graph);
+    if (rc2 != BIMP_OK) e = cudaErrorUnknown;
+    else e = e2;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e != cudaSuccess) {
+    const std::string msg = std::string("batch graph setup: ") + cudaGetErrorString(e);
+    bimp_batch_destroy(b);
+    return fail(BIMP_ERR_CUDA, msg);
+  }
+  *out = b;
+  return BIMP_OK;
+}
+
+int bimp_batch_destroy(bimp_batch* b) {
+  if (!b) return BIMP_OK;
+  cudaSetDevice(b->eng.device);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->capStream) cudaStreamDestroy(b->capStream);
+  if (b->h_totals) cudaFreeHost(b->h_totals);
+  b->eng.release();
+  delete b;
+  return BIMP_OK;
+}
+
+int bimp_batch_num_images(const bimp_batch* b) { return b ? b->eng.nImages : 0; }
+
+int bimp_batch_image(bimp_batch* b, int i, uint8_t** d_image, size_t* pitch) {
+  if (!b || i < 0 || i >= b->eng.nImages || !d_image || !pitch)
+    return fail(BIMP_ERR_INVALID, "bad batch image arguments");
+  *d_image = b->eng.lvl[i][0];
+  *pitch = (size_t)b->eng.lvlP[i][0];
+  return BIMP_OK;
+}
+
+int bimp_batch_run(bimp_batch* b, void* stream) {
+  if (!b) return fail(BIMP_ERR_INVALID, "batch is null");
+  BIMP_CUDA(cudaSetDevice(b->eng.device));
+  BIMP_CUDA(cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)));
+  return BIMP_OK;
+}
+
+int bimp_batch_counts(bimp_batch* b, int* d_counts, void* stream) {
+  if (!b || !d_counts) return fail(BIMP_ERR_INVALID, "bad batch count arguments");
+  BIMP_CUDA(cudaMemcpyAsync(d_counts, b->eng.d_totals, sizeof(int) * b->eng.nImages,
+                            cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)));
+  return BIMP_OK;
+}
+
+int bimp_batch_keypoints_device(bimp_batch* b, int i, const float** d_kp, size_t* ld) {
+  if (!b || i < 0 || i >= b->eng.nImages || !d_kp || !ld)
+    return fail(BIMP_ERR_INVALID, "bad batch keypoint arguments");
+  *d_kp = b->eng.d_kpInternal + (size_t)i * BIMP_KP_VECTOR_LENGTH * b->eng.kpCapInternal;
+  *ld = (size_t)b->eng.kpCapInternal;
+  return BIMP_OK;
+}
+
+int bimp_batch_detect_host(bimp_batch* b, const uint8_t* const* images, const size_t* pitches,
+                           bimp_keypoint* const* outs, const int* capacities, int* n_found,
+                           void* stream) {
+  if (!b || !images || !pitches || !n_found) return fail(BIMP_ERR_INVALID, "bad batch arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Engine& e = b->eng;
+  BIMP_CUDA(cudaSetDevice(e.device));
+  for (int i = 0; i < e.nImages; ++i) {
+    if (!images[i]) return fail(BIMP_ERR_INVALID, "null image");
+    BIMP_CUDA(cudaMemcpy2DAsync(e.lvl[i][0], e.lvlP[i][0], images[i], pitches[i], e.widths[i],
+                                e.heights[i], cudaMemcpyHostToDevice, s));
+  }
+  BIMP_CUDA(cudaGraphLaunch(b->exec, s));
+  BIMP_CUDA(cudaMemcpyAsync(b->h_totals, e.d_totals, sizeof(int) * e.nImages, cudaMemcpyDeviceToHost, s));
+  BIMP_CUDA(cudaStreamSynchronize(s));
+  int status = BIMP_OK;
+  for (int i = 0; i < e.nImages; ++i) {
+    n_found[i] = b->h_totals[i];
+    const int cap = std::min(capacities ? capacities[i] : 0, e.kpCapInternal);
+    const int n = std::min(n_found[i], cap);
+    if (n_found[i] > cap) status = BIMP_ERR_CAPACITY;
+    if (n > 0 && outs && outs[i]) {
+      const float* dk = e.d_kpInternal + (size_t)i * BIMP_KP_VECTOR_LENGTH * e.kpCapInternal;
+      const int rc = bimp_download_keypoints(dk, e.kpCapInternal, n, outs[i], stream);
+      if (rc != BIMP_OK) return rc;
+    }
+  }
+  if (status != BIMP_OK) return fail(status, "keypoints exceed capacity for some image");
+  return BIMP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+// Launch interface of the BIMP kernels (kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "bimp_internal.h"
+
+namespace bimp_b200 {
+
+// One pyramid step src (sw x sh, pitch sp) -> dst (dw x dh, pitch dp).
+struct PyrJob {
+  const uint8_t* src;
+  int sw, sh, sp;
+  uint8_t* dst;
+  int dw, dh, dp;
+};
+
+// Keypoint destination of one image: 7 x ld float matrix, `capacity` columns.
+struct KpOut {
+  float* kp;
+  size_t ld;
+  int capacity;
+  int pad_;
+};
+
+cudaError_t configure_kernels();
+size_t gabor_smem_bytes();
+size_t stencil_smem_bytes();
+
+void launch_pyr(const PyrJob* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
+void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, cudaStream_t s);
+void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
+void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
+                const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,
+                cudaStream_t s);
+
+}  // namespace bimp_b200

@@ -1,0 +1,184 @@
+/*
+ * bimp_b200.h -- C ABI of the B200-native BIMP keypoint detector.
+ *
+ * Plain C types only (pointers, sizes, ints, floats); no CUDA, torch or
+ * OpenCV types appear in the signatures.  Streams are passed as `void*`
+ * holding a cudaStream_t (NULL = the legacy default stream).
+ *
+ * Each entry point names the daniel-koudouna/cuda-bimp interface it replaces
+ * (paths relative to that project).
+ */
+#ifndef BIMP_B200_H
+#define BIMP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BIMP_NUM_ORI 8            /* bimp/include/detection/cuda_bimp.hpp:10 */
+#define BIMP_KP_VECTOR_LENGTH 7   /* bimp/include/detection/cuda_bimp.hpp:13 */
+#define BIMP_KP_MAX_POINTS 8000   /* bimp/include/detection/cuda_bimp.hpp:14 */
+
+/* Row indices of the 7 x N device keypoint matrix (cv::cuda::SURF_CUDA
+ * KeypointLayout, consumed by bimp/src/utils.cpp:130-150).  Rows 2 and 3
+ * hold int32 bit patterns, the others float32. */
+enum bimp_kp_row {
+  BIMP_X_ROW = 0,
+  BIMP_Y_ROW = 1,
+  BIMP_LAPLACIAN_ROW = 2,
+  BIMP_OCTAVE_ROW = 3,
+  BIMP_SIZE_ROW = 4,
+  BIMP_ANGLE_ROW = 5,
+  BIMP_HESSIAN_ROW = 6
+};
+
+/* Status codes.  The reference prints and exit()s on any CUDA error
+ * (helper_cuda.h macros, bimp/src/cuda_bimp.cu:4-10) and warns + truncates
+ * on keypoint overflow (bimp/src/cuda_bimp.cu:132-138). */
+typedef enum bimp_status {
+  BIMP_OK = 0,
+  BIMP_ERR_INVALID = -1,      /* bad argument: null pointer, size, wavelength list */
+  BIMP_ERR_CUDA = -2,         /* CUDA runtime error; see bimp_last_error() */
+  BIMP_ERR_NOMEM = -3,        /* device or pinned-host allocation failed */
+  BIMP_ERR_CAPACITY = -4,     /* more keypoints than `capacity`; the first
+                                 `capacity` (in scale, y, x order) were written
+                                 and *n_found holds the true count */
+  BIMP_ERR_NO_DEVICE = -5,    /* no CUDA device / not an sm_100 device */
+  BIMP_ERR_UNSUPPORTED = -6   /* parameters outside what the kernels support */
+} bimp_status;
+
+/* Model constants hard-coded in bimp/src/cuda_bimp.cu (defaults = reference). */
+/* Doubles, so that the defaults are the reference's double literals. */
+typedef struct bimp_params {
+  double gamma;         /* 0.5   cuda_bimp.cu:241 (multiplies the squared term) */
+  double sigma_ratio;   /* 0.56  cuda_bimp.cu:243 */
+  double size_ratio;    /* 7     cuda_bimp.cu:245 */
+  double offset_ratio;  /* 0.6   cuda_bimp.cu:535 */
+  double level_max;     /* 7.5   cuda_bimp.cu:236 */
+  double radial_gain;   /* 16    cuda_bimp.cuh:497 */
+  double w_tan;         /* 1     cuda_bimp.cuh:514 (implicit weight) */
+  double w_rad;         /* 1     cuda_bimp.cuh:514 (implicit weight) */
+  double thresh_ratio;  /* 0.104 cuda_bimp.cu:721 */
+} bimp_params;
+
+/* Host keypoint record, byte-compatible with cv::KeyPoint
+ * {Point2f pt; float size, angle, response; int octave, class_id;}. */
+typedef struct bimp_keypoint {
+  float x, y;
+  float size;
+  float angle;
+  float response;
+  int32_t octave;
+  int32_t class_id;
+} bimp_keypoint;
+
+/* Geometry of one scale (fields of CudaKernels, cuda_bimp.hpp:38-73). */
+typedef struct bimp_scale_info {
+  float lambda_full;   /* lambda2: requested wavelength */
+  float lambda_level;  /* lambda: wavelength at the pyramid level */
+  float pyrstep;
+  int kernel_w;        /* kernelW == kernelH */
+  int kernel_x;        /* kernelX == kernelY */
+  int data_w, data_h;
+  int fft_w, fft_h;    /* torus the reference convolves on */
+  int margin;          /* (int)lambda: keypoint border margin */
+} bimp_scale_info;
+
+typedef struct bimp_context bimp_context;
+
+/* ---- library ------------------------------------------------------------ */
+const char* bimp_version(void);
+/* Message of the last error on the calling thread ("" if none). */
+const char* bimp_last_error(void);
+/* Fills the reference defaults. */
+void bimp_default_params(bimp_params* p);
+
+/* makeLambdasLog, bimp/src/cuda_bimp.cu:927-937 (float accumulation).
+ * Writes up to `cap` wavelengths; *n = number generated. */
+int bimp_make_lambdas_log(float start, float end, int scales_per_octave,
+                          float* out, int cap, int* n);
+/* makeLambdasLin, bimp/src/cuda_bimp.cu:905-921. */
+int bimp_make_lambdas_lin(float start, float end, int num_scales,
+                          float* out, int cap, int* n);
+/* snapTransformSize, bimp/src/cuda_bimp.cu:200-219. */
+int bimp_snap_transform_size(int data_size);
+
+/* ---- context (replaces bimp::cuda::CudaStuff) ---------------------------
+ * CudaStuff(int width, int height, std::vector<float> lambdas),
+ * bimp/include/detection/cuda_bimp.hpp:97, bimp/src/cuda_bimp.cu:222-397:
+ * sorts the wavelengths, builds the Gabor bank and all per-scale buffers on
+ * the current CUDA device.  `params` may be NULL (reference defaults). */
+int bimp_ctx_create(bimp_context** ctx, int width, int height,
+                    const float* lambdas, int n_lambdas,
+                    const bimp_params* params);
+/* ~CudaStuff, bimp/src/cuda_bimp.cu:399-460. */
+int bimp_ctx_destroy(bimp_context* ctx);
+int bimp_ctx_num_scales(const bimp_context* ctx);
+int bimp_ctx_scale_info(const bimp_context* ctx, int scale, bimp_scale_info* out);
+
+/* ---- detection -----------------------------------------------------------
+ * int getKeypoints(GpuMat& input, GpuMat& output, CudaStuff&, bool, bool),
+ * bimp/include/detection/cuda_bimp.hpp:111, bimp/src/cuda_bimp.cu:109-127.
+ * `d_image`: device uint8 grayscale, `pitch` bytes per row, size must equal
+ * the context's.  `d_kp`: device float matrix 7 x `ld` (row r at d_kp + r*ld)
+ * receiving up to `capacity` keypoints in (scale, y, x) order.  `n_found`
+ * (host) receives the total count; the call synchronises `stream`. */
+int bimp_detect_device(bimp_context* ctx, const uint8_t* d_image, size_t pitch,
+                       int width, int height, float* d_kp, size_t ld,
+                       int capacity, int* n_found, void* stream);
+
+/* Same as bimp_detect_device without any host synchronisation: the total
+ * count is written to the device int `d_count` (stream-ordered). */
+int bimp_detect_device_async(bimp_context* ctx, const uint8_t* d_image, size_t pitch,
+                             int width, int height, float* d_kp, size_t ld,
+                             int capacity, int* d_count, void* stream);
+
+/* Context(cv::Mat&) + Context::getKeypointsAndDownload(),
+ * bimp/include/detection/bimp.hpp:35,38, bimp/src/bimp.cpp:7-20,89-92,
+ * for an already-grey image: host uint8 image in, host cv::KeyPoint-layout
+ * records out (utils.cpp:130-150 downloadKeypoints).  Copies go through the
+ * context's pinned staging buffers on `stream`; the call synchronises. */
+int bimp_detect_host(bimp_context* ctx, const uint8_t* image, size_t pitch,
+                     int width, int height, bimp_keypoint* out, int capacity,
+                     int* n_found, void* stream);
+
+/* Per-scale dense maps of the last detection (Context::getResponses,
+ * bimp/src/bimp.cpp:94-104; k.d_ResultDouble / k.d_ResultSingle).
+ * which = 0: summed keypoint map D (double-stopped minus inhibition),
+ *         1: single-stopped map S minus inhibition.
+ * Copies data_h x data_w floats to device memory `d_out` (row pitch `ld`
+ * floats) on `stream`. */
+int bimp_dense_map(bimp_context* ctx, int scale, int which, float* d_out,
+                   size_t ld, void* stream);
+
+/* Complex-cell map C_o of the last detection for one scale/orientation
+ * (cs.im.d_complex[o], bimp/src/cuda_bimp.cu:518), restricted to the
+ * (data_h+1) x (data_w+1) window the stencils read. */
+int bimp_complex_map(bimp_context* ctx, int scale, int orientation, float* d_out,
+                     size_t ld, void* stream);
+
+/* ---- measurement hooks (no counterpart in the reference) -----------------
+ * Number of kernel launches one detection enqueues (all scales). */
+int bimp_ctx_kernel_launches(const bimp_context* ctx);
+/* Re-enqueues one stage of the last detection on `stream`, for timing a
+ * single kernel with events: 0 = pyramid, 1 = tiled-FFT Gabor filtering,
+ * 2 = end-stopping/inhibition stencil, 3 = NMS + compaction (into the last
+ * detection's keypoint destination).  Inputs of the stage are the buffers
+ * left by the previous detection, so the results are unchanged. */
+int bimp_ctx_run_stage(bimp_context* ctx, int stage, void* stream);
+
+/* downloadKeypoints, bimp/src/utils.cpp:130-150: device 7 x ld matrix with n
+ * columns -> host records (synchronous). */
+int bimp_download_keypoints(const float* d_kp, size_t ld, int n,
+                            bimp_keypoint* out, void* stream);
+/* uploadKeypoints, bimp/src/utils.cpp:109-128. */
+int bimp_upload_keypoints(const bimp_keypoint* kps, int n, float* d_kp,
+                          size_t ld, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BIMP_B200_H */

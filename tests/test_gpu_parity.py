@@ -1,0 +1,189 @@
+"""GPU parity: the CUDA path through the C ABI against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from bimp_b200 import api, synth
+from oracle import bimp_oracle as O
+from parity import ELEM_FLOOR, MAP_TOL, SUBPIX_TOL, compare_keypoints, elem_rel_error, peak_rel_error
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_gpu(img, lambdas, capacity=200000):
+    cs = api.CudaStuff(img.shape[1], img.shape[0], lambdas)
+    kp, n = api.getKeypoints(img, cs, capacity=capacity, return_count=True)
+    rec = api.keypoint_matrix_to_records(kp)
+    return cs, rec, n
+
+
+def _map_errors(cs, res):
+    worst = {"C": 0.0, "Cel": 0.0, "D": 0.0, "S": 0.0}
+    for i, r in enumerate(res):
+        for o in range(8):
+            g = cs.complex_map(i, o).cpu().numpy()
+            worst["C"] = max(worst["C"], peak_rel_error(g, r["Cw"][o]))
+            worst["Cel"] = max(worst["Cel"], elem_rel_error(g, r["Cw"][o], ELEM_FLOOR))
+        worst["D"] = max(worst["D"], peak_rel_error(cs.dense_map(i, 0).cpu().numpy(), r["D"]))
+        worst["S"] = max(worst["S"], peak_rel_error(cs.dense_map(i, 1).cpu().numpy(), r["S"]))
+    print("map errors", worst)
+    return worst
+
+
+def _check_scale_maps(cs, res):
+    worst = _map_errors(cs, res)
+    assert worst["C"] <= MAP_TOL and worst["Cel"] <= MAP_TOL
+    assert worst["D"] <= MAP_TOL and worst["S"] <= MAP_TOL
+    return worst
+
+
+def _check_keypoints(rec, res):
+    rep = compare_keypoints(rec, res)
+    print({k: (v if not isinstance(v, list) else len(v)) for k, v in rep.items()})
+    assert not rep["missing"], rep["missing"][:10]
+    assert not rep["extra"], rep["extra"][:10]
+    assert rep["max_subpix"] <= SUBPIX_TOL
+    assert rep["max_resp_rel"] <= MAP_TOL
+    return rep
+
+
+def test_vga_maps_and_keypoints():
+    imgs, lam = synth.workload("vga")
+    img = imgs[0]
+    res = O.run(img, lam)
+    cs, rec, n = _run_gpu(img, lam)
+    assert n == len(rec)
+    _map_errors(cs, res)
+    _check_keypoints(rec, res)
+    _check_scale_maps(cs, res)
+    # deterministic (scale, y, x) order
+    order = [(r["size"], r["y"], r["x"]) for r in rec]
+    assert len(order) == n
+
+
+@pytest.mark.parametrize("w,h,lam", [
+    (512, 512, [4.0, 5.656854, 8.0]),          # fftW == dataW and fftH == dataH (pure torus)
+    (333, 277, [4.0, 6.0, 11.0]),              # odd sizes, three pyramid levels
+    (48, 40, [4.0, 5.5]),                       # torus smaller than a tile: multiple wraps
+    (1024, 200, [4.0, 7.9999995, 16.0]),       # wrapW at every level
+    (130, 1100, [4.0, 5.656854]),               # fft height > 1024 (align 512)
+])
+def test_torus_edge_cases(w, h, lam):
+    img = synth.synth_image(w, h, max(2, w * h // 15000), seed=7 + w + h)
+    res = O.run(img, lam)
+    cs, rec, n = _run_gpu(img, lam)
+    _check_scale_maps(cs, res)
+    _check_keypoints(rec, res)
+
+
+def test_hd_keypoints_and_maps():
+    imgs, lam = synth.workload("hd")
+    img = imgs[0]
+    res = O.run(img, lam)
+    cs, rec, n = _run_gpu(img, lam)
+    _check_scale_maps(cs, res)
+    rep = _check_keypoints(rec, res)
+    assert rep["matched"] > 1000
+
+
+def test_detect_host_matches_device():
+    imgs, lam = synth.workload("vga")
+    img = imgs[0]
+    cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
+    kp, n = api.getKeypoints(img, cs, capacity=100000, return_count=True)
+    dev = api.keypoint_matrix_to_records(kp)
+    host, n2, rc = api.detect_host(cs, img, capacity=100000)
+    assert rc == 0 and n2 == n
+    assert np.array_equal(dev, host)
+
+
+def test_repeatable_bitwise():
+    imgs, lam = synth.workload("vga")
+    img = imgs[0]
+    cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
+    a = api.keypoint_matrix_to_records(api.getKeypoints(img, cs, capacity=100000))
+    d1 = cs.dense_map(0).cpu().numpy()
+    b = api.keypoint_matrix_to_records(api.getKeypoints(img, cs, capacity=100000))
+    d2 = cs.dense_map(0).cpu().numpy()
+    assert np.array_equal(a, b) and np.array_equal(d1, d2)
+
+
+def test_capacity_overflow_truncates_in_order():
+    imgs, lam = synth.workload("vga")
+    img = imgs[0]
+    cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
+    full = api.keypoint_matrix_to_records(api.getKeypoints(img, cs, capacity=100000))
+    with pytest.warns(UserWarning):
+        kp, n = api.getKeypoints(img, cs, capacity=1000, return_count=True)
+    part = api.keypoint_matrix_to_records(kp)
+    assert n == len(full) and len(part) == 1000
+    assert np.array_equal(part, full[:1000])
+    host, n2, rc = api.detect_host(cs, img, capacity=1000)
+    assert rc == -4 and n2 == n and np.array_equal(host, full[:1000])
+
+
+def test_errors_are_status_codes():
+    import ctypes as C
+    from bimp_b200 import _lib as L
+    imgs, lam = synth.workload("vga")
+    img = imgs[0]
+    cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
+    n = C.c_int()
+    # wrong size
+    rc = L.lib().bimp_detect_device(cs.handle, C.c_void_p(1), 640, 320, 240, None, 0, 0, C.byref(n), None)
+    assert rc == L.BIMP_ERR_INVALID
+    # null image
+    rc = L.lib().bimp_detect_device(cs.handle, None, 640, 640, 480, None, 0, 0, C.byref(n), None)
+    assert rc == L.BIMP_ERR_INVALID
+    # capacity without a matrix
+    rc = L.lib().bimp_detect_device(cs.handle, C.c_void_p(1), 640, 640, 480, None, 0, 10, C.byref(n), None)
+    assert rc == L.BIMP_ERR_INVALID
+    # empty wavelength list / unsupported wavelength geometry
+    h = C.c_void_p()
+    assert L.lib().bimp_ctx_create(C.byref(h), 64, 64, None, 0, None) == L.BIMP_ERR_INVALID
+    p = api.default_params()
+    p.level_max = 40.0   # kernels wider than the tile supports
+    lam1 = (C.c_float * 1)(30.0)
+    assert L.lib().bimp_ctx_create(C.byref(h), 640, 480, lam1, 1, C.byref(p)) == L.BIMP_ERR_INVALID
+    # the context still works afterwards
+    kp, n2 = api.getKeypoints(img, cs, capacity=100000, return_count=True)
+    assert n2 > 0
+
+
+def test_context_mirror():
+    imgs, lam = synth.workload("vga")
+    img = imgs[0]
+    ctx = api.Context(img, lambdas=lam)
+    pts = ctx.getKeypointsAndDownload()
+    assert len(pts) > 0 and all(p.class_id == 1 and p.angle == -1 for p in pts)
+    resp = ctx.getResponses()
+    assert len(resp) == len(lam) and resp[0]["D"].shape == (480, 640)
+    ctx.loadImage(np.ascontiguousarray(img[:, ::-1]))
+    pts2 = ctx.getKeypointsAndDownload()
+    assert len(pts2) > 0
+
+
+def test_upload_download_roundtrip():
+    pts = [api.KeyPoint((1.5, 2.25), 4.0, -1.0, 0.5, 4, 1), api.KeyPoint((10.0, 20.0), 8.0, -1.0, 2.0, 7, 1)]
+    kp = api.uploadKeypoints(pts)
+    back = api.downloadKeypoints(kp)
+    assert back == pts
+
+
+def test_batch_matches_single():
+    rng = np.random.default_rng(5)
+    sizes = [(int(rng.integers(20, 60)) * 16, int(rng.integers(15, 40)) * 16) for _ in range(5)]
+    imgs = [synth.synth_image(w, h, 10, seed=50 + i) for i, (w, h) in enumerate(sizes)]
+    lam = synth.bank(8)
+    b = api.Batch(sizes, lam, kp_capacity=100000)
+    b.load(imgs)
+    b.run()
+    for i, img in enumerate(imgs):
+        cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
+        ref = api.keypoint_matrix_to_records(api.getKeypoints(img, cs, capacity=100000))
+        got = api.keypoint_matrix_to_records(b.keypoints(i))
+        assert np.array_equal(ref, got), i
+    # replay again: same answer
+    b.run()
+    got0 = api.keypoint_matrix_to_records(b.keypoints(0))
+    cs = api.CudaStuff(imgs[0].shape[1], imgs[0].shape[0], lam)
+    assert np.array_equal(got0, api.keypoint_matrix_to_records(api.getKeypoints(imgs[0], cs, capacity=100000)))

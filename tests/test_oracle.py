@@ -1,0 +1,150 @@
+"""CPU tests of the FP64 oracle: pins against cv2.pyrDown, hand-built known
+answers for each stage, and the committed golden fixtures."""
+import math
+
+import numpy as np
+import pytest
+
+from bimp_b200 import synth
+from oracle import bimp_oracle as O
+
+
+def test_snap_transform_size_cases():
+    # snapTransformSize (cuda_bimp.cu:200-219)
+    cases = {1: 16, 16: 16, 17: 32, 480: 512, 640: 1024, 1024: 1024, 1025: 1536, 1080: 1536,
+             1920: 2048, 2160: 2560, 3840: 4096, 67: 128, 33: 64, 135: 256, 512: 512, 1536: 1536}
+    for n, want in cases.items():
+        assert O.snap_transform_size(n) == want, n
+
+
+def test_make_lambdas_log_float_accumulation():
+    lam = O.make_lambdas_log(4, 45.26, 2)
+    assert len(lam) == 8
+    assert lam[2] == float(np.float32(7.9999995))      # not exactly 8
+    assert O.make_lambdas_log(4, 32, 1) == [4.0, 8.0, 16.0, 32.0]
+    assert len(O.make_lambdas_log(4, 64, 2)) == 9       # Context's bank (bimp.cpp:8)
+    assert synth.lambdas_log(4, 45.26, 2) == lam
+
+
+def test_scale_geometry_hd():
+    sc = O.scale_geometry(1920, 1080, O.make_lambdas_log(4, 45.26, 2))
+    assert [s.kW for s in sc] == [29, 39, 27, 39, 27, 39, 27, 39]
+    assert [s.pyrstep for s in sc] == [1, 1, 2, 2, 4, 4, 8, 8]
+    assert [(s.fftW, s.fftH) for s in sc[:4:2]] == [(2048, 1536), (1024, 1024)]
+    assert [s.off for s in sc] == [4, 5, 3, 5, 3, 5, 3, 5]
+    assert sc[0].es_off == [(2, 0), (2, 1), (2, 2), (1, 2), (0, 2), (-1, 2), (-2, 2), (-2, 1)]
+    assert sc[0].in_off == [(0, 2), (1, 2), (2, 2), (2, 1), (2, 0), (2, -1), (2, -2), (1, -2)]
+
+
+def test_pyramid_matches_cv2_away_from_ties():
+    cv2 = pytest.importorskip("cv2")
+    img = synth.synth_image(321, 247, 15, seed=3)
+    a = O.pyr_down_u8(img).astype(int)
+    b = cv2.pyrDown(img).astype(int)
+    assert a.shape == b.shape == (124, 161)
+    # exact integer sums: cv2 rounds .5 up, the CUDA pyrDown rounds half to even
+    diff = a != b
+    assert np.all(np.abs(a - b)[diff] == 1)
+    assert np.all(a[diff] % 2 == 0) and np.all(b[diff] % 2 == 1)
+
+
+def test_pyramid_tie_rounding():
+    img = np.zeros((5, 5), np.uint8)
+    img[2, 2] = 128          # centre weight 36/256 -> 18.0 exactly
+    assert O.pyr_down_u8(img)[1, 1] == 18
+    img[2, 2] = 64 + 32      # 96*36 = 3456 = 13.5*256 -> tie, rounds to even 14
+    assert O.pyr_down_u8(img)[1, 1] == 14
+
+
+def test_gabor_taps_symmetry_and_dc():
+    sc = O.scale_geometry(640, 480, [5.656854])[0]
+    for o in range(8):
+        e, od = O.gabor_taps(sc, o)
+        assert e.shape == (39, 39)
+        assert np.array_equal(e, e[::-1, ::-1])                 # point-symmetric
+        assert np.max(np.abs(od + od[::-1, ::-1])) < 1e-6       # antisymmetric up to float
+        # DC removed with the float filtersize divisor (39.598^2, not 39^2)
+        resid = float(e.astype(np.float64).sum())
+        assert abs(resid) < 0.5
+
+
+def test_delta_image_gives_flipped_taps():
+    # A delta inside the data gives the torus convolution = the (flipped) taps.
+    sc = O.scale_geometry(96, 96, [4.0])[0]
+    data = np.zeros((sc.dataH, sc.dataW))
+    data[40, 50] = 1.0
+    Ip = O.padded_image(data, sc)
+    X = np.fft.rfft2(Ip)
+    e, od = O.gabor_taps(sc, 3)
+    E = np.fft.irfft2(X * np.fft.rfft2(O.padded_kernel(e, sc)), s=Ip.shape)
+    k = sc.kX
+    patch = E[40 - k:40 + k + 1, 50 - k:50 + k + 1]
+    assert np.allclose(patch, e[::-1, ::-1], atol=1e-12)
+
+
+def test_padding_semantics():
+    # rows < dataH copy, then kY clamp-to-last rows, then clamp-to-first
+    m = O.pad_map(64, 40, 14)
+    assert list(m[:40]) == list(range(40))
+    assert set(m[40:54]) == {39} and set(m[54:]) == {0}
+    m2 = O.pad_map(48, 40, 14)            # torus shorter than data + half kernel
+    assert list(m2[40:]) == [39] * 8
+
+
+def test_stencil_window_flat_addressing():
+    sc = O.scale_geometry(32, 32, [4.0])[0]     # fft == data: flat wrap cases
+    assert (sc.fftW, sc.fftH) == (32, 32)
+    Ct = np.arange(32 * 32, dtype=float).reshape(32, 32)
+    Cw = O.stencil_window(Ct, sc)
+    assert Cw.shape == (33, 33)
+    assert Cw[3, 32] == Ct[4, 0]          # column dataW -> next row, column 0
+    assert Cw[32, 5] == Ct[0, 5]          # row dataH wraps modulo fftH*fftW
+    assert Cw[32, 32] == Ct[1, 0]
+
+
+def test_end_stop_on_hand_map():
+    # A single bright complex-cell spot: the double-stopped response at the
+    # spot is C - 0.5*0 - 0.5*0 for every orientation whose bounds hold.
+    sc = O.scale_geometry(40, 40, [4.0])[0]
+    Cw = np.zeros((8, sc.dataH + 1, sc.dataW + 1))
+    Cw[:, 20, 20] = 1.0
+    maps = O.keypoint_maps(Cw, sc)
+    assert maps["D0"][20, 20] == pytest.approx(8.0)
+    # tangential inhibition at a neighbour that sees the spot at -offset
+    o1, o2 = sc.in_off[0]
+    assert maps["T"][20 + o1, 20 + o2] >= 1.0 - 1e-12
+
+
+def test_nms_and_subpixel_on_hand_map():
+    sc = O.scale_geometry(20, 20, [4.0])[0]
+    D = np.zeros((20, 20))
+    D[10, 10] = 1.0
+    D[10, 11] = 0.5
+    D[9, 10] = 0.25
+    D[11, 10] = 0.25
+    D[15, 15] = 0.05        # below 0.104*max
+    kp = O.extract_keypoints(D, sc, 0)
+    assert list(zip(kp.ix, kp.iy)) == [(10, 10)]
+    # parabola through (0, 1, 0.5): x + 0.5*(0-0.5)/(0+0.5-2) = 10 + 1/6
+    assert kp.x[0] == pytest.approx(10 + 1 / 6)
+    assert kp.y[0] == pytest.approx(10.0)
+    assert kp.octave == 4 and kp.size == 4.0
+
+
+def test_float_pyramid_is_linear():
+    rng = np.random.default_rng(0)
+    a, b = rng.random((37, 29)), rng.random((37, 29))
+    assert np.allclose(O.pyr_down_f(a + 2 * b), O.pyr_down_f(a) + 2 * O.pyr_down_f(b))
+
+
+def test_golden_fixture():
+    from pathlib import Path
+    g = np.load(Path(__file__).parent / "golden" / "oracle_small.npz")
+    img = g["image"]
+    lam = list(g["lambdas"])
+    res = O.run(img, lam)
+    for i, r in enumerate(res):
+        assert np.allclose(r["D"], g[f"D{i}"], rtol=0, atol=1e-9 * np.abs(g[f"D{i}"]).max())
+    tab = O.keypoint_table(res)
+    assert np.array_equal(tab["ix"], g["kp_ix"]) and np.array_equal(tab["iy"], g["kp_iy"])
+    assert np.array_equal(tab["scale"], g["kp_scale"])
