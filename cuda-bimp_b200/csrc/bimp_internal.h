@@ -14,7 +14,6 @@ namespace bimp_b200 {
 constexpr int kNumOri = 8;
 // Overlap-save tile: 128 x 128 complex FFT held in shared memory.
 constexpr int kTile = 128;
-constexpr int kTileLD = 136;               // complex row stride of the work buffer
 constexpr int kXhCols = 65;                // Hermitian half: kx = 0..64
 constexpr int kTileThreads = 512;
 constexpr int kMaxHalf = 56;               // largest supported kernel half size
@@ -56,7 +55,24 @@ struct ScaleDev {
   float threshRatio;
   int rowBase;            // first entry of this scale in the per-row count array
   int image;              // image index inside a batch
+  int pattern;            // stencil offsets: 0 = runtime, k > 0 = kOffsetSets[k-1]
 };
+
+// Stencil offset sets of the two level wavelengths the default bank uses
+// (lambda ~ 4 and ~ 5.657 at every pyramid level); scales whose offsets equal
+// one of them run a kernel specialised with compile-time offsets.
+// Layout per set: es1[8], es2[8], in1[8], in2[8], ih1[8], ih2[8].
+constexpr int kNumOffsetSets = 2;
+#define BIMP_OFFSET_SETS                                   \
+  {                                                        \
+    {{2, 2, 2, 1, 0, -1, -2, -2}, {0, 1, 2, 2, 2, 2, 2, 1}, \
+     {0, 1, 2, 2, 2, 2, 2, 1}, {2, 2, 2, 1, 0, -1, -2, -2}, \
+     {0, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 0, -1, -1, -1}},\
+    {{3, 3, 2, 1, 0, -1, -2, -3}, {0, 1, 2, 3, 3, 3, 2, 1}, \
+     {0, 1, 2, 3, 3, 3, 2, 1}, {3, 3, 2, 1, 0, -1, -2, -3}, \
+     {0, 1, 1, 2, 2, 2, 1, 1}, {2, 2, 1, 1, 0, -1, -1, -2}} \
+  }
+constexpr int kOffsetSets[kNumOffsetSets][6][8] = BIMP_OFFSET_SETS;
 
 // One unit of tiled-FFT work: tile `tile` of descriptor `entry`.
 struct TileWork {

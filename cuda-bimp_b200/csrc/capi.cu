@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -114,6 +115,7 @@ struct Engine {
   int* d_imgRowStart = nullptr;
   int* d_totals = nullptr;
   unsigned int* d_maxKeys = nullptr;
+  unsigned int* d_fault = nullptr;      // set by the tile kernel if a bounded wait expired
   KpOut* d_outs = nullptr;
   std::vector<PyrJob> h_pyr;                 // grouped by level
   std::vector<int> pyrFirst, pyrCount, pyrMaxW, pyrMaxH;
@@ -121,6 +123,7 @@ struct Engine {
   std::vector<size_t> imgKpOffset;           // internal keypoint buffers (batch)
   float* d_kpInternal = nullptr;
   int kpCapInternal = 0;
+  int tileGrid = 0;    // CTAs of the tile kernel (each loops over tiles)
 
   int build(int dev, const int* w, const int* h, int n, const float* lambdas, int nl,
             const bimp_params& p, int internalKpCap) {
@@ -134,6 +137,8 @@ struct Engine {
     geo.resize(n);
     for (int i = 0; i < n; ++i) {
       if (w[i] < 2 || h[i] < 2) return fail(BIMP_ERR_INVALID, "image size must be at least 2x2");
+      if (w[i] > 32767 || h[i] > 32767)   // tile index maps are int16
+        return fail(BIMP_ERR_UNSUPPORTED, "image sides above 32767 pixels are not supported");
       if (!build_scales(w[i], h[i], lam, p, geo[i], err)) return fail(BIMP_ERR_INVALID, err);
       if (i == 0) bank = geo[0];
       for (auto& s : geo[i]) {        // taps and spectra are shared with image 0
@@ -203,6 +208,16 @@ struct Engine {
           d.ih1[o] = round_half_away(0.5 * s.in1[o]);   // cuda_bimp.cuh:495-496
           d.ih2[o] = round_half_away(0.5 * s.in2[o]);
         }
+        d.pattern = 0;
+        for (int set = 0; set < kNumOffsetSets && d.pattern == 0; ++set) {
+          bool same = true;
+          for (int o = 0; o < kNumOri; ++o) {
+            same = same && d.es1[o] == kOffsetSets[set][0][o] && d.es2[o] == kOffsetSets[set][1][o] &&
+                   d.in1[o] == kOffsetSets[set][2][o] && d.in2[o] == kOffsetSets[set][3][o] &&
+                   d.ih1[o] == kOffsetSets[set][4][o] && d.ih2[o] == kOffsetSets[set][5][o];
+          }
+          if (same) d.pattern = set + 1;
+        }
         d.radialGain = static_cast<float>(p.radial_gain);
         d.wTan = static_cast<float>(p.w_tan);
         d.wRad = static_cast<float>(p.w_rad);
@@ -242,6 +257,13 @@ struct Engine {
       pyrMaxH.push_back(mh);
     }
     nTiles = static_cast<int>(tiles.size());
+    // One CTA per tile by default.  BIMP_TILE_GRID caps the grid so that each
+    // CTA walks several tiles (used by the tests of the persistent loop).
+    tileGrid = nTiles;
+    if (const char* g = std::getenv("BIMP_TILE_GRID")) {
+      const int cap = std::atoi(g);
+      if (cap > 0) tileGrid = std::min(tileGrid, cap);
+    }
     nSten = static_cast<int>(sten.size());
     nRows = static_cast<int>(rows.size());
     const size_t offSd = a.reserve(sizeof(ScaleDev) * sds.size());
@@ -252,7 +274,7 @@ struct Engine {
     const size_t offOffsets = a.reserve(sizeof(int) * std::max<size_t>(1, rows.size()));
     const size_t offImgRow = a.reserve(sizeof(int) * imgRowStart.size());
     const size_t offTotals = a.reserve(sizeof(int) * n);
-    const size_t offMax = a.reserve(sizeof(unsigned int) * sds.size());
+    const size_t offMax = a.reserve(sizeof(unsigned int) * (sds.size() + 1));
     const size_t offOuts = a.reserve(sizeof(KpOut) * n);
     const size_t offPyr = a.reserve(sizeof(PyrJob) * std::max<size_t>(1, h_pyr.size()));
     size_t offKp = 0;
@@ -300,6 +322,7 @@ struct Engine {
     d_imgRowStart = reinterpret_cast<int*>(base + offImgRow);
     d_totals = reinterpret_cast<int*>(base + offTotals);
     d_maxKeys = reinterpret_cast<unsigned int*>(base + offMax);
+    d_fault = d_maxKeys + sds.size();
     d_outs = reinterpret_cast<KpOut*>(base + offOuts);
     d_pyr = reinterpret_cast<PyrJob*>(base + offPyr);
     d_kpInternal = internalKpCap > 0 ? reinterpret_cast<float*>(base + offKp) : nullptr;
@@ -330,7 +353,7 @@ struct Engine {
       }
       BIMP_CUDA(cudaMemcpy(d_outs, outs.data(), sizeof(KpOut) * n, cudaMemcpyHostToDevice));
     }
-    BIMP_CUDA(cudaMemset(d_maxKeys, 0, sizeof(unsigned int) * sds.size()));
+    BIMP_CUDA(cudaMemset(d_maxKeys, 0, sizeof(unsigned int) * (sds.size() + 1)));
     return BIMP_OK;
   }
 
@@ -341,7 +364,7 @@ struct Engine {
           launch_pyr(d_pyr + pyrFirst[l], pyrCount[l], pyrMaxW[l], pyrMaxH[l], s);
         break;
       case 1:
-        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, nTiles, s);
+        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s);
         break;
       case 2:
         if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, s);
@@ -364,7 +387,7 @@ struct Engine {
   int enqueue(cudaStream_t s) {
     int rc = stage(0, s);
     if (rc != BIMP_OK) return rc;
-    BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, sizeof(unsigned int) * h_sd.size(), s));
+    BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, sizeof(unsigned int) * (h_sd.size() + 1), s));
     for (int k = 1; k <= 3; ++k) {
       rc = stage(k, s);
       if (rc != BIMP_OK) return rc;
@@ -390,7 +413,7 @@ struct bimp_context {
   int h_kpCap = 0;
   bimp_keypoint* d_aos = nullptr;
   int d_aosCap = 0;
-  int* h_count = nullptr;
+  int* h_count = nullptr;   // pinned: [0] keypoint total, [1] device fault word
   float* d_kpScratch = nullptr;
   int d_kpScratchCap = 0;
 };
@@ -400,7 +423,7 @@ struct bimp_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t capStream = nullptr;
-  int* h_totals = nullptr;
+  int* h_totals = nullptr;   // pinned: n_images totals, then the device fault word
   std::vector<bimp_keypoint> tmp;
 };
 
@@ -453,7 +476,7 @@ int bimp_ctx_create(bimp_context** ctx, int width, int height, const float* lamb
     return rc;
   }
   c->info = c->eng.geo[0];
-  cudaError_t e = cudaMallocHost(&c->h_count, sizeof(int));
+  cudaError_t e = cudaMallocHost(&c->h_count, 2 * sizeof(int));
   if (e != cudaSuccess) {
     c->eng.release();
     delete c;
@@ -532,8 +555,10 @@ int bimp_detect_device(bimp_context* c, const uint8_t* d_image, size_t pitch, in
                    nullptr, s);
   if (rc != BIMP_OK) return rc;
   BIMP_CUDA(cudaMemcpyAsync(c->h_count, c->eng.d_totals, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIMP_CUDA(cudaMemcpyAsync(c->h_count + 1, c->eng.d_fault, sizeof(int), cudaMemcpyDeviceToHost, s));
   BIMP_CUDA(cudaStreamSynchronize(s));
   *n_found = *c->h_count;
+  if (c->h_count[1]) return fail(BIMP_ERR_CUDA, "a bounded device wait expired in the tile kernel");
   if (*n_found > capacity)
     return fail(BIMP_ERR_CAPACITY, "keypoints exceed capacity (" + std::to_string(*n_found) + ")");
   return BIMP_OK;
@@ -570,8 +595,10 @@ int bimp_detect_host(bimp_context* c, const uint8_t* image, size_t pitch, int wi
                capacity, nullptr, s);
   if (rc != BIMP_OK) return rc;
   BIMP_CUDA(cudaMemcpyAsync(c->h_count, c->eng.d_totals, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIMP_CUDA(cudaMemcpyAsync(c->h_count + 1, c->eng.d_fault, sizeof(int), cudaMemcpyDeviceToHost, s));
   BIMP_CUDA(cudaStreamSynchronize(s));
   const int total = *c->h_count;
+  if (c->h_count[1]) return fail(BIMP_ERR_CUDA, "a bounded device wait expired in the tile kernel");
   const int n = std::min(total, capacity);
   if (n > 0) {
     float* hk = reinterpret_cast<float*>(c->h_kp);
@@ -702,7 +729,7 @@ int bimp_batch_create(bimp_batch** out, const int* widths, const int* heights, i
     delete b;
     return rc;
   }
-  cudaError_t e = cudaMallocHost(&b->h_totals, sizeof(int) * n_images);
+  cudaError_t e = cudaMallocHost(&b->h_totals, sizeof(int) * (n_images + 1));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capStream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamBeginCapture(b->capStream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
@@ -779,7 +806,9 @@ int bimp_batch_detect_host(bimp_batch* b, const uint8_t* const* images, const si
   }
   BIMP_CUDA(cudaGraphLaunch(b->exec, s));
   BIMP_CUDA(cudaMemcpyAsync(b->h_totals, e.d_totals, sizeof(int) * e.nImages, cudaMemcpyDeviceToHost, s));
+  BIMP_CUDA(cudaMemcpyAsync(b->h_totals + e.nImages, e.d_fault, sizeof(int), cudaMemcpyDeviceToHost, s));
   BIMP_CUDA(cudaStreamSynchronize(s));
+  if (b->h_totals[e.nImages]) return fail(BIMP_ERR_CUDA, "a bounded device wait expired in the tile kernel");
   int status = BIMP_OK;
   for (int i = 0; i < e.nImages; ++i) {
     n_found[i] = b->h_totals[i];

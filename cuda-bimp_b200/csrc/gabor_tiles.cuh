@@ -1,0 +1,280 @@
+// k_gabor_tiles: overlap-save 128x128 tile FFT Gabor filtering (included by
+// kernels.cu).
+//
+// One CTA (512 threads, 16 warps) per tile.  The tile's real input window is
+// read from the uint8 pyramid level through the reference's padded-torus index
+// map, transformed once (forward 2D FFT, Hermitian half kept in shared
+// memory), and then for each of the 8 orientations the spectrum is multiplied
+// by that orientation's real Gabor spectrum G_o, inverse transformed as one
+// complex FFT (e + i o) and reduced to |e + i o| on the valid outputs.
+//
+// G_o (64 KB per orientation, L2-resident) is streamed into a double buffer of
+// 16 KB chunks with TMA bulk copies (cp.async.bulk + mbarrier): chunk c + 2 is
+// issued as soon as every thread has finished with chunk c, so the next
+// orientation's first chunks load during the current orientation's last three
+// passes.  Every mbarrier wait is bounded; on expiry the kernel records a
+// fault in *fault, waits once more (bounded) for its copies and carries on,
+// and the host reports the fault.
+//
+// Included inside namespace bimp_b200 by kernels.cu, after the helpers it uses
+// (pad_src, pmod, spectrum_at, c_w128).
+#pragma once
+
+constexpr int kGChunkRows = 32;                          // rows of G per chunk
+constexpr int kGChunkFloats = kGChunkRows * kTile;       // 4096 floats = 16 KB
+constexpr int kSmemW = kTile * kTile * 8;                // work buffer 128 x 128 complex
+constexpr int kSmemXh = kTile * kXhCols * 8;             // Hermitian half spectrum
+constexpr int kSmemG = 2 * kGChunkFloats * 4;            // G double buffer
+constexpr int kSmemTw = 8 * 17 * 8;                      // twiddles w128^(n1*k2)
+constexpr int kSmemMaps = 2 * kTile * 2;                 // int16 row / column maps
+constexpr int kSmemBars = 2 * 8;                         // two mbarriers
+constexpr int kGaborSmem = kSmemW + kSmemXh + kSmemG + kSmemTw + kSmemMaps + kSmemBars;
+static_assert(kGaborSmem <= 232448, "tile kernel exceeds the 227 KB shared-memory limit");
+
+// Work-buffer index of row y, position p: the rotate-by-(p>>4) swizzle inside
+// each group of 8 keeps the stride-8 and contiguous-8 passes conflict-free,
+// and odd rows swap the two halves of every 16-group so that two rows served
+// by one wavefront use disjoint banks.
+__device__ __forceinline__ int widx(int y, int p) { return y * kTile + (phys(p) ^ ((y & 1) << 3)); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// 1-D TMA bulk copy global -> shared, completion counted on `bar`.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// Bounded wait for phase `parity` of `bar`; false if it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kTileThreads, 1)
+k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ work, int nwork,
+              unsigned int* __restrict__ fault_word) {
+  extern __shared__ float4 smem4[];
+  char* base = reinterpret_cast<char*>(smem4);
+  float2* W = reinterpret_cast<float2*>(base);
+  float2* Xh = reinterpret_cast<float2*>(base + kSmemW);
+  float* Gbuf = reinterpret_cast<float*>(base + kSmemW + kSmemXh);
+  float2* tw = reinterpret_cast<float2*>(base + kSmemW + kSmemXh + kSmemG);
+  short* rmap = reinterpret_cast<short*>(base + kSmemW + kSmemXh + kSmemG + kSmemTw);
+  short* cmap = rmap + kTile;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kSmemW + kSmemXh + kSmemG + kSmemTw + kSmemMaps);
+  const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+  const uint32_t gdst0 = smem_u32(Gbuf), gdst1 = smem_u32(Gbuf + kGChunkFloats);
+  const int t = threadIdx.x;
+
+  if (t < 8 * 17) {
+    const int n1 = t / 17, k2 = t % 17;
+    tw[t] = k2 < 16 ? c_w128[(n1 * k2) & 127] : make_float2(0.f, 0.f);
+  }
+  if (t == 0) {
+    mbar_init(bar0);
+    mbar_init(bar1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  uint32_t gc = 0;       // G chunks consumed by this CTA (identical in every thread)
+  bool fault = false;
+
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const TileWork item = work[w];
+    const ScaleDev* sd = sds + item.entry;
+    const int kX = sd->kX, V = sd->V;
+    const int ty = item.tile / sd->tilesX, tx = item.tile - ty * sd->tilesX;
+    const int R0 = ty * V, C0 = tx * V;
+    const uint8_t* __restrict__ lvl = sd->lvl;
+    const int lp = sd->lvlPitch;
+    const float* __restrict__ G0 = sd->G;
+
+    __syncthreads();   // previous tile finished with every buffer
+    if (t == 0) {      // first two chunks of this tile's orientation 0
+      fence_proxy_async();
+      bulk_load((gc & 1) ? gdst1 : gdst0, G0, kGChunkFloats * 4, (gc & 1) ? bar1 : bar0);
+      bulk_load(((gc + 1) & 1) ? gdst1 : gdst0, G0 + kGChunkFloats, kGChunkFloats * 4,
+                ((gc + 1) & 1) ? bar1 : bar0);
+    }
+    if (t < kTile) {
+      rmap[t] = (short)pad_src(pmod(R0 - kX + t, sd->fftH), sd->dataH, kX);
+    } else if (t < 2 * kTile) {
+      const int i = t - kTile;
+      cmap[i] = (short)pad_src(pmod(C0 - kX + i, sd->fftW), sd->dataW, kX);
+    }
+    __syncthreads();
+
+    // F1: x-dim pass A on packed rows z[r] = in[r] + i in[r+64], r < 64.
+    // Pixel value 255*u8/65536 (convertTo, cuda_bimp.cu:481) enters as
+    // (255*u8 - 32768)/65536 = value - 0.5, exactly; the 0.5 offset is put
+    // back into the DC bin below.  Removing the mean keeps the butterflies'
+    // intermediate magnitudes, and so their float rounding, small.
+    {
+      const int r = t >> 3, n1 = t & 7;
+      const uint8_t* rowA = lvl + (size_t)rmap[r] * lp;
+      const uint8_t* rowB = lvl + (size_t)rmap[r + 64] * lp;
+      const float s = 1.0f / 65536.0f;
+      float2 v[16];
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        const int c = cmap[n1 + 8 * m];
+        v[m] = make_float2(s * (float)(255 * (int)rowA[c] - 32768), s * (float)(255 * (int)rowB[c] - 32768));
+      }
+      dft16<false>(v);
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) W[widx(r, n1 + 8 * k2)] = c_mul(v[k2], tw[n1 * 17 + k2]);
+    }
+    __syncthreads();
+    // F2: x-dim pass B
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int j = t + it * kTileThreads;
+      const int r = j >> 4, k2 = j & 15;
+      float2 v[8];
+#pragma unroll
+      for (int n1 = 0; n1 < 8; ++n1) v[n1] = W[widx(r, 8 * k2 + n1)];
+      dft8<false>(v);
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) W[widx(r, 8 * k2 + k1)] = v[k1];
+    }
+    __syncthreads();
+    // separation of the packed rows into the Hermitian half (kx = 0..64)
+    for (int j = t; j < 64 * kXhCols; j += kTileThreads) {
+      const int r = j / kXhCols, s = j - r * kXhCols;
+      const int kx = s < 64 ? (s >> 2) + 16 * (s & 3) : 64;
+      const int nk = (128 - kx) & 127;
+      const float2 Z = W[widx(r, 8 * (kx & 15) + (kx >> 4))];
+      const float2 Zn = W[widx(r, 8 * (nk & 15) + (nk >> 4))];
+      Xh[r * kXhCols + s] = make_float2(0.5f * (Z.x + Zn.x), 0.5f * (Z.y - Zn.y));
+      Xh[(r + 64) * kXhCols + s] = make_float2(0.5f * (Z.y + Zn.y), 0.5f * (Zn.x - Z.x));
+    }
+    __syncthreads();
+    // F3: y-dim pass A on the 65 half columns
+    for (int j = t; j < 8 * kXhCols; j += kTileThreads) {
+      const int n1 = j / kXhCols, s = j - n1 * kXhCols;
+      float2 v[16];
+#pragma unroll
+      for (int m = 0; m < 16; ++m) v[m] = Xh[(n1 + 8 * m) * kXhCols + s];
+      dft16<false>(v);
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) Xh[(n1 + 8 * k2) * kXhCols + s] = c_mul(v[k2], tw[n1 * 17 + k2]);
+    }
+    __syncthreads();
+    // F4: y-dim pass B -> Xh rows in permuted ky order
+    for (int j = t; j < 16 * kXhCols; j += kTileThreads) {
+      const int k2 = j / kXhCols, s = j - k2 * kXhCols;
+      float2 v[8];
+#pragma unroll
+      for (int n1 = 0; n1 < 8; ++n1) v[n1] = Xh[(8 * k2 + n1) * kXhCols + s];
+      dft8<false>(v);
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) Xh[(8 * k2 + k1) * kXhCols + s] = v[k1];
+    }
+    __syncthreads();
+    if (t == 0) Xh[0].x += 0.5f * (float)(kTile * kTile);   // DC of the removed 0.5 offset
+    __syncthreads();
+
+    const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
+    float* __restrict__ C0p = sd->C;
+    const long long cStride = sd->cStride;
+    for (int o = 0; o < kNumOri; ++o) {
+      float* __restrict__ Cout = C0p + (size_t)o * cStride;
+      // I1: y-dim pass B' with the spectrum product Z = X * G, one 16 KB
+      // chunk of G (rows py in [32q, 32q+32)) per quarter q
+#pragma unroll 1
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t buf = gc & 1;
+        if (!mbar_wait(buf ? bar1 : bar0, (gc >> 1) & 1)) fault = true;
+        const float* Gq = Gbuf + buf * kGChunkFloats;
+        const int p = t & 127, k2 = (t >> 7) + 4 * q;
+        float2 v[8];
+#pragma unroll
+        for (int k1 = 0; k1 < 8; ++k1) {
+          const int py = 8 * k2 + k1;
+          v[k1] = c_scale(spectrum_at(Xh, py, p), Gq[(py - kGChunkRows * q) * kTile + p]);
+        }
+        dft8<true>(v);
+#pragma unroll
+        for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, p)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
+        __syncthreads();   // chunk buffer free, and (q == 3) the pass is complete
+        const int next = 4 * o + q + 2;
+        if (t == 0 && next < 4 * kNumOri) {
+          fence_proxy_async();
+          bulk_load(buf ? gdst1 : gdst0, G0 + (size_t)next * kGChunkFloats, kGChunkFloats * 4, buf ? bar1 : bar0);
+        }
+        ++gc;
+      }
+      // I2: y-dim pass A' -> natural y
+#pragma unroll
+      for (int it = 0; it < 2; ++it) {
+        const int j = t + it * kTileThreads;
+        const int p = j & 127, n1 = j >> 7;
+        float2 v[16];
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(8 * k2 + n1, p)];
+        dft16<true>(v);
+#pragma unroll
+        for (int n2 = 0; n2 < 16; ++n2) W[widx(n1 + 8 * n2, p)] = v[n2];
+      }
+      __syncthreads();
+      // I3: x-dim pass B' on the rows holding valid outputs
+      for (int j = t; j < V * 16; j += kTileThreads) {
+        const int y = kX + (j >> 4), k2 = j & 15;
+        float2 v[8];
+#pragma unroll
+        for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
+        dft8<true>(v);
+#pragma unroll
+        for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
+      }
+      __syncthreads();
+      // I4: x-dim pass A' -> natural x; complex magnitude of valid outputs
+      for (int j = t; j < V * 8; j += kTileThreads) {
+        const int y = kX + (j >> 3), n1 = j & 7;
+        float2 v[16];
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(y, 8 * k2 + n1)];
+        dft16<true>(v);
+        const int gy = R0 + y - kX;
+        if (gy < cRows) {
+          float* dst = Cout + (size_t)gy * cPitch;
+#pragma unroll
+          for (int n2 = 0; n2 < 16; ++n2) {
+            const int x = n1 + 8 * n2;
+            const int gx = C0 + x - kX;
+            if (x >= kX && x < kX + V && gx < cCols) dst[gx] = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (fault) {
+    // a wait expired: record it, then give the copies still in flight a
+    // second bounded chance to land before the CTA releases its memory
+    if (t == 0) atomicOr(fault_word, 1u);
+    mbar_wait(bar0, ((gc + 1) >> 1) & 1);
+    mbar_wait(bar1, (gc >> 1) & 1);
+  }
+}

@@ -83,183 +83,7 @@ __device__ __forceinline__ float2 spectrum_at(const float2* __restrict__ Xh, int
   return make_float2(v.x, -v.y);
 }
 
-__global__ void __launch_bounds__(kTileThreads, 1)
-k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ work, int nwork) {
-  extern __shared__ float4 smem4[];
-  float2* W = reinterpret_cast<float2*>(smem4);      // kTile x kTileLD
-  float2* Xh = W + kTile * kTileLD;                    // kTile x kXhCols
-  float2* tw = Xh + kTile * kXhCols;                   // 8 x 17: w128^(n1*k2)
-  int* rmap = reinterpret_cast<int*>(tw + 8 * 17);     // window row -> level row
-  int* cmap = rmap + kTile;                            // window col -> level col
-  const int t = threadIdx.x;
-
-  if (t < 8 * 17) {
-    const int n1 = t / 17, k2 = t % 17;
-    tw[t] = k2 < 16 ? c_w128[(n1 * k2) & 127] : make_float2(0.f, 0.f);
-  }
-
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const TileWork item = work[w];
-    const ScaleDev* sd = sds + item.entry;
-    const int kX = sd->kX, V = sd->V;
-    const int ty = item.tile / sd->tilesX, tx = item.tile - ty * sd->tilesX;
-    const int R0 = ty * V, C0 = tx * V;
-    const uint8_t* __restrict__ lvl = sd->lvl;
-    const int lp = sd->lvlPitch;
-
-    __syncthreads();   // previous tile finished with maps / work buffers
-    if (t < kTile) {
-      rmap[t] = pad_src(pmod(R0 - kX + t, sd->fftH), sd->dataH, kX);
-    } else if (t < 2 * kTile) {
-      const int i = t - kTile;
-      cmap[i] = pad_src(pmod(C0 - kX + i, sd->fftW), sd->dataW, kX);
-    }
-    __syncthreads();
-
-    // F1: x-dim pass A on packed rows z[r] = in[r] + i in[r+64], r < 64.
-    // Pixel value 255*u8/65536 (convertTo, cuda_bimp.cu:481) enters as
-    // (255*u8 - 32768)/65536 = value - 0.5, exactly; the 0.5 offset is put
-    // back into the DC bin below.  Removing the mean keeps the butterflies'
-    // intermediate magnitudes, and so their float rounding, small.
-    {
-      const int r = t >> 3, n1 = t & 7;
-      const uint8_t* rowA = lvl + (size_t)rmap[r] * lp;
-      const uint8_t* rowB = lvl + (size_t)rmap[r + 64] * lp;
-      const float s = 1.0f / 65536.0f;
-      float2 v[16];
-#pragma unroll
-      for (int m = 0; m < 16; ++m) {
-        const int c = cmap[n1 + 8 * m];
-        v[m] = make_float2(s * (float)(255 * (int)rowA[c] - 32768),
-                           s * (float)(255 * (int)rowB[c] - 32768));
-      }
-      dft16<false>(v);
-#pragma unroll
-      for (int k2 = 0; k2 < 16; ++k2)
-        W[r * kTileLD + phys(n1 + 8 * k2)] = c_mul(v[k2], tw[n1 * 17 + k2]);
-    }
-    __syncthreads();
-    // F2: x-dim pass B
-#pragma unroll
-    for (int it = 0; it < 2; ++it) {
-      const int j = t + it * kTileThreads;
-      const int r = j >> 4, k2 = j & 15;
-      float2 v[8];
-#pragma unroll
-      for (int n1 = 0; n1 < 8; ++n1) v[n1] = W[r * kTileLD + phys(8 * k2 + n1)];
-      dft8<false>(v);
-#pragma unroll
-      for (int k1 = 0; k1 < 8; ++k1) W[r * kTileLD + phys(8 * k2 + k1)] = v[k1];
-    }
-    __syncthreads();
-    // separation of the packed rows into the Hermitian half (kx = 0..64)
-    for (int j = t; j < 64 * kXhCols; j += kTileThreads) {
-      const int r = j / kXhCols, s = j - r * kXhCols;
-      const int kx = s < 64 ? (s >> 2) + 16 * (s & 3) : 64;
-      const int nk = (128 - kx) & 127;
-      const float2 Z = W[r * kTileLD + phys(8 * (kx & 15) + (kx >> 4))];
-      const float2 Zn = W[r * kTileLD + phys(8 * (nk & 15) + (nk >> 4))];
-      Xh[r * kXhCols + s] = make_float2(0.5f * (Z.x + Zn.x), 0.5f * (Z.y - Zn.y));
-      Xh[(r + 64) * kXhCols + s] = make_float2(0.5f * (Z.y + Zn.y), 0.5f * (Zn.x - Z.x));
-    }
-    __syncthreads();
-    // F3: y-dim pass A on the 65 half columns
-    for (int j = t; j < 8 * kXhCols; j += kTileThreads) {
-      const int n1 = j / kXhCols, s = j - n1 * kXhCols;
-      float2 v[16];
-#pragma unroll
-      for (int m = 0; m < 16; ++m) v[m] = Xh[(n1 + 8 * m) * kXhCols + s];
-      dft16<false>(v);
-#pragma unroll
-      for (int k2 = 0; k2 < 16; ++k2)
-        Xh[(n1 + 8 * k2) * kXhCols + s] = c_mul(v[k2], tw[n1 * 17 + k2]);
-    }
-    __syncthreads();
-    // F4: y-dim pass B -> Xh rows in permuted ky order
-    for (int j = t; j < 16 * kXhCols; j += kTileThreads) {
-      const int k2 = j / kXhCols, s = j - k2 * kXhCols;
-      float2 v[8];
-#pragma unroll
-      for (int n1 = 0; n1 < 8; ++n1) v[n1] = Xh[(8 * k2 + n1) * kXhCols + s];
-      dft8<false>(v);
-#pragma unroll
-      for (int k1 = 0; k1 < 8; ++k1) Xh[(8 * k2 + k1) * kXhCols + s] = v[k1];
-    }
-    __syncthreads();
-    if (t == 0) Xh[0].x += 0.5f * (float)(kTile * kTile);   // DC of the removed 0.5 offset
-    __syncthreads();
-
-    const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
-    for (int o = 0; o < kNumOri; ++o) {
-      const float* __restrict__ G = sd->G + (size_t)o * kSpecFloats;
-      float* __restrict__ Cout = sd->C + (size_t)o * sd->cStride;
-      // I1: y-dim pass B' with the spectrum product Z = X * G
-#pragma unroll
-      for (int it = 0; it < 4; ++it) {
-        const int j = t + it * kTileThreads;
-        const int p = j & 127, k2 = j >> 7;
-        float2 v[8];
-#pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) {
-          const int py = 8 * k2 + k1;
-          v[k1] = c_scale(spectrum_at(Xh, py, p), __ldg(G + py * kTile + p));
-        }
-        dft8<true>(v);
-        const int pc = phys(p);
-#pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1)
-          W[(8 * k2 + n1) * kTileLD + pc] = c_mulc(v[n1], tw[n1 * 17 + k2]);
-      }
-      __syncthreads();
-      // I2: y-dim pass A' -> natural y
-#pragma unroll
-      for (int it = 0; it < 2; ++it) {
-        const int j = t + it * kTileThreads;
-        const int p = j & 127, n1 = j >> 7;
-        const int pc = phys(p);
-        float2 v[16];
-#pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[(8 * k2 + n1) * kTileLD + pc];
-        dft16<true>(v);
-#pragma unroll
-        for (int n2 = 0; n2 < 16; ++n2) W[(n1 + 8 * n2) * kTileLD + pc] = v[n2];
-      }
-      __syncthreads();
-      // I3: x-dim pass B' on the rows holding valid outputs
-      for (int j = t; j < V * 16; j += kTileThreads) {
-        const int y = kX + (j >> 4), k2 = j & 15;
-        float2 v[8];
-#pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[y * kTileLD + phys(8 * k2 + k1)];
-        dft8<true>(v);
-#pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1)
-          W[y * kTileLD + phys(8 * k2 + n1)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
-      }
-      __syncthreads();
-      // I4: x-dim pass A' -> natural x; complex magnitude of valid outputs
-      for (int j = t; j < V * 8; j += kTileThreads) {
-        const int y = kX + (j >> 3), n1 = j & 7;
-        float2 v[16];
-#pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[y * kTileLD + phys(8 * k2 + n1)];
-        dft16<true>(v);
-        const int gy = R0 + y - kX;
-        if (gy < cRows) {
-          float* dst = Cout + (size_t)gy * cPitch;
-#pragma unroll
-          for (int n2 = 0; n2 < 16; ++n2) {
-            const int x = n1 + 8 * n2;
-            const int gx = C0 + x - kX;
-            if (x >= kX && x < kX + V && gx < cCols)
-              dst[gx] = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
-          }
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
+#include "gabor_tiles.cuh"
 
 // ---------------------------------------------------------------------------
 // stencil: end-stopping, inhibition, summed keypoint map
@@ -275,95 +99,170 @@ __device__ __forceinline__ float key_float(unsigned int k) {
   return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
-__device__ __forceinline__ bool stencil_ok(int x, int y, int o1, int o2, int W, int H) {
-  // cuda_bimp.cuh:446-449 (inclusive upper bounds)
-  return x - o2 >= 0 && x - o2 <= W && x + o2 >= 0 && x + o2 <= W &&
-         y - o1 >= 0 && y - o1 <= H && y + o1 >= 0 && y + o1 <= H &&
-         x - 2 * o2 >= 0 && x - 2 * o2 <= W && x + 2 * o2 >= 0 && x + 2 * o2 <= W &&
-         y - 2 * o1 >= 0 && y - 2 * o1 <= H && y + 2 * o1 >= 0 && y + 2 * o1 <= H;
+// Per-scale stencil constants, staged once per block in shared memory.
+struct StencilPar {
+  int e1[kNumOri], e2[kNumOri];      // end-stop offsets (row, col)
+  int i1[kNumOri], i2[kNumOri];      // inhibition offsets
+  int h1[kNumOri], h2[kNumOri];      // radial half offsets
+  int exlo[kNumOri], exhi[kNumOri], eylo[kNumOri], eyhi[kNumOri];  // end-stop bounds
+  int ixlo[kNumOri], ixhi[kNumOri], iylo[kNumOri], iyhi[kNumOri];  // inhibition bounds
+};
+
+// Offset k (0..5: es1, es2, in1, in2, ih1, ih2) of orientation o: a
+// compile-time constant for PAT > 0, else the staged runtime value.
+template <int PAT>
+__device__ __forceinline__ int soff(const StencilPar& P, int k, int o) {
+  if constexpr (PAT > 0) {
+    constexpr int sets[kNumOffsetSets][6][8] = BIMP_OFFSET_SETS;
+    return sets[PAT - 1][k][o];
+  } else {
+    const int* base = k == 0 ? P.e1 : k == 1 ? P.e2 : k == 2 ? P.i1 : k == 3 ? P.i2 : k == 4 ? P.h1 : P.h2;
+    return base[o];
+  }
 }
 
-__global__ void __launch_bounds__(256)
-k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
-  extern __shared__ float s_c[];   // kNumOri x kStH x kStW
-  const int2 item = work[blockIdx.x];
-  const ScaleDev* sd = sds + item.x;
-  const int W = sd->dataW, H = sd->dataH;
-  const int nbx = (W + kStX - 1) / kStX;
-  const int by = item.y / nbx, bx = item.y - by * nbx;
-  const int x0 = bx * kStX, y0 = by * kStY;
-  const int t = threadIdx.x;
-
-  // stage C (rows y0-8 .. y0+39, cols x0-8 .. x0+39) of all orientations
-  const float* __restrict__ C = sd->C;
-  const int cPitch = sd->cPitch;
-  const long long cStride = sd->cStride;
-  const int wrapW = sd->wrapW;
-  for (int idx = t; idx < kNumOri * kStH * kStW; idx += 256) {
-    const int o = idx / (kStH * kStW);
-    const int rem = idx - o * (kStH * kStW);
-    const int ly = rem / kStW, lx = rem - ly * kStW;
-    const int gy = y0 - kHalo + ly, gx = x0 - kHalo + lx;
-    float v = 0.f;
-    if (gy >= 0 && gy <= H && gx >= 0 && gx <= W) {
-      int ry = gy, rx = gx;
-      if (wrapW && gx == W) { rx = 0; ry = gy + 1; }   // flat y*fftW + fftW
-      v = C[(size_t)o * cStride + (size_t)ry * cPitch + rx];
-    }
-    s_c[idx] = v;
+// One pixel of end-stopping and inhibition (cuda_bimp.cuh:436-517).  The
+// bounds test of the reference (x -+ o2, x -+ 2 o2 in [0, W], likewise y)
+// reduces to 2|o2| <= x <= W - 2|o2| and 2|o1| <= y <= H - 2|o1|.
+// The double-stopped term c - 0.5 a - 0.5 b, which the reference evaluates
+// in double and rounds once, is two fused float multiply-adds here (at most
+// one float rounding apart).
+template <bool CHECK, int PAT>
+__device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, const StencilPar& P, int x, int y,
+                                              int cy, int cx, float gain, float wT, float wR, float& Dout,
+                                              float& Sout) {
+  float S = 0.f, D = 0.f, T = 0.f, R = 0.f;
+  const float* c0 = s_c + cy * kStW + cx;
+#pragma unroll
+  for (int o = 0; o < kNumOri; ++o) {
+    if (CHECK && !(x >= P.exlo[o] && x <= P.exhi[o] && y >= P.eylo[o] && y <= P.eyhi[o])) continue;
+    const int o1 = soff<PAT>(P, 0, o), o2 = soff<PAT>(P, 1, o);
+    const float* c = c0 + o * (kStH * kStW);
+    float s = c[-o1 * kStW + o2] - c[o1 * kStW - o2];
+    s = s > 0.f ? s : 0.f;
+    if (s > 0.f) S += s;
+    float d = fmaf(-0.5f, c[2 * o1 * kStW - 2 * o2], fmaf(-0.5f, c[-2 * o1 * kStW + 2 * o2], c[0]));
+    d = d > 0.f ? d : 0.f;
+    if (d > 0.f) D += d;
   }
-  __syncthreads();
+#pragma unroll
+  for (int o = 0; o < kNumOri; ++o) {
+    if (CHECK && !(x >= P.ixlo[o] && x <= P.ixhi[o] && y >= P.iylo[o] && y <= P.iyhi[o])) continue;
+    const int o1 = soff<PAT>(P, 2, o), o2 = soff<PAT>(P, 3, o);
+    const float* c = c0 + o * (kStH * kStW);
+    const float* cp = c0 + ((o + kNumOri / 2) % kNumOri) * (kStH * kStW);
+    const float centre = c[0];
+    float v = c[-o1 * kStW - o2] - centre;
+    v = v < 0.f ? 0.f : v;
+    T += v;
+    const int h1 = soff<PAT>(P, 4, o), h2 = soff<PAT>(P, 5, o);
+    float r = centre - gain * cp[h1 * kStW + h2];
+    r = r < 0.f ? 0.f : r;
+    r += centre - gain * cp[-h1 * kStW - h2];
+    r = r < 0.f ? 0.f : r;
+    R += r;
+  }
+  const float inhib = wT * T + wR * R;
+  Dout = D + (-inhib);
+  Sout = S + (-inhib);
+}
 
+template <int PAT>
+__device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, const StencilPar& P, int x0, int y0,
+                                               int W, int H, float gain, float wT, float wR, float* __restrict__ Dmap,
+                                               float* __restrict__ Smap, int dPitch) {
+  const int t = threadIdx.x;
   const int lx = t & 31, ly0 = t >> 5;
   const int x = x0 + lx;
   float dmax = -INFINITY;
-  const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
+  // no bounds test needed when every pixel of the block is >= 8 from the edges
+  const bool inner = x0 >= kHalo && x0 + kStX <= W - kHalo && y0 >= kHalo && y0 + kStY <= H - kHalo;
 #pragma unroll 1
   for (int i = 0; i < 4; ++i) {
     const int ly = ly0 + 8 * i;
     const int y = y0 + ly;
     if (x >= W || y >= H) continue;
-    const int cy = ly + kHalo, cx = lx + kHalo;
-    float S = 0.f, D = 0.f, T = 0.f, R = 0.f;
-#pragma unroll
-    for (int o = 0; o < kNumOri; ++o) {
-      const int o1 = sd->es1[o], o2 = sd->es2[o];
-      if (!stencil_ok(x, y, o1, o2, W, H)) continue;
-      const float* c = s_c + o * (kStH * kStW);
-      float s = c[(cy - o1) * kStW + cx + o2] - c[(cy + o1) * kStW + cx - o2];
-      s = s > 0.f ? s : 0.f;
-      if (s > 0.f) S += s;
-      // the reference evaluates this line in double (0.5 is a double literal)
-      const double dd = (double)c[cy * kStW + cx] - 0.5 * (double)c[(cy - 2 * o1) * kStW + cx + 2 * o2]
-                        - 0.5 * (double)c[(cy + 2 * o1) * kStW + cx - 2 * o2];
-      float d = (float)dd;
-      d = d > 0.f ? d : 0.f;
-      if (d > 0.f) D += d;
-    }
-#pragma unroll
-    for (int o = 0; o < kNumOri; ++o) {
-      const int o1 = sd->in1[o], o2 = sd->in2[o];
-      if (!stencil_ok(x, y, o1, o2, W, H)) continue;
-      const float* c = s_c + o * (kStH * kStW);
-      const float* cp = s_c + ((o + kNumOri / 2) % kNumOri) * (kStH * kStW);
-      const float centre = c[cy * kStW + cx];
-      float v = c[(cy - o1) * kStW + cx - o2] - centre;
-      v = v < 0.f ? 0.f : v;
-      T += v;
-      const int h1 = sd->ih1[o], h2 = sd->ih2[o];
-      float r = centre - gain * cp[(cy + h1) * kStW + cx + h2];
-      r = r < 0.f ? 0.f : r;
-      r += centre - gain * cp[(cy - h1) * kStW + cx - h2];
-      r = r < 0.f ? 0.f : r;
-      R += r;
-    }
-    const float inhib = wT * T + wR * R;
-    D = D + (-inhib);
-    S = S + (-inhib);
-    sd->D[(size_t)y * sd->dPitch + x] = D;
-    sd->S[(size_t)y * sd->dPitch + x] = S;
+    float D, S;
+    if (inner)
+      stencil_pixel<false, PAT>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S);
+    else
+      stencil_pixel<true, PAT>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S);
+    Dmap[(size_t)y * dPitch + x] = D;
+    Smap[(size_t)y * dPitch + x] = S;
     dmax = fmaxf(dmax, D);
   }
+  return dmax;
+}
+
+__global__ void __launch_bounds__(256, 3)
+k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
+  extern __shared__ float4 s_c4[];   // kNumOri x kStH x kStW floats
+  float* s_c = reinterpret_cast<float*>(s_c4);
+  __shared__ StencilPar P;
+  const int2 item = work[blockIdx.x];
+  const ScaleDev* __restrict__ sd = sds + item.x;
+  const int W = sd->dataW, H = sd->dataH;
+  const int nbx = (W + kStX - 1) / kStX;
+  const int by = item.y / nbx, bx = item.y - by * nbx;
+  const int x0 = bx * kStX, y0 = by * kStY;
+  const int t = threadIdx.x;
+  const float* __restrict__ C = sd->C;
+  const int cPitch = sd->cPitch;
+  const long long cStride = sd->cStride;
+  const int wrapW = sd->wrapW;
+  const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
+  float* __restrict__ Dmap = sd->D;
+  float* __restrict__ Smap = sd->S;
+  const int dPitch = sd->dPitch;
+  const int pattern = sd->pattern;
+  unsigned int* maxKey = sd->maxKey;
+  if (t < kNumOri) {
+    const int o = t;
+    const int e1 = sd->es1[o], e2 = sd->es2[o], i1 = sd->in1[o], i2 = sd->in2[o];
+    P.e1[o] = e1; P.e2[o] = e2; P.i1[o] = i1; P.i2[o] = i2;
+    P.h1[o] = sd->ih1[o]; P.h2[o] = sd->ih2[o];
+    P.exlo[o] = 2 * abs(e2); P.exhi[o] = W - 2 * abs(e2);
+    P.eylo[o] = 2 * abs(e1); P.eyhi[o] = H - 2 * abs(e1);
+    P.ixlo[o] = 2 * abs(i2); P.ixhi[o] = W - 2 * abs(i2);
+    P.iylo[o] = 2 * abs(i1); P.iyhi[o] = H - 2 * abs(i1);
+  }
+
+  // stage C (rows y0-8 .. y0+39, cols x0-8 .. x0+39) of all orientations
+  const int gx0 = x0 - kHalo, gy0 = y0 - kHalo;
+  const bool fast_load = gx0 >= 0 && gx0 + kStW <= W && gy0 >= 0 && gy0 + kStH <= H + 1;
+  if (fast_load) {
+    // every staged column lies inside [0, W-1]: rows of 12 aligned float4
+    constexpr int kV = kStW / 4;
+    for (int idx = t; idx < kNumOri * kStH * kV; idx += 256) {
+      const int row = idx / kV, v4 = idx - row * kV;
+      const int o = row / kStH, ly = row - o * kStH;
+      const float4* src =
+          reinterpret_cast<const float4*>(C + (size_t)o * cStride + (size_t)(gy0 + ly) * cPitch + gx0);
+      s_c4[row * kV + v4] = __ldg(src + v4);
+    }
+  } else {
+    for (int idx = t; idx < kNumOri * kStH * kStW; idx += 256) {
+      const int row = idx / kStW, lx = idx - row * kStW;
+      const int o = row / kStH, ly = row - o * kStH;
+      const int gy = gy0 + ly, gx = gx0 + lx;
+      float v = 0.f;
+      if (gy >= 0 && gy <= H && gx >= 0 && gx <= W) {
+        int ry = gy, rx = gx;
+        if (wrapW && gx == W) { rx = 0; ry = gy + 1; }   // flat y*fftW + fftW
+        v = C[(size_t)o * cStride + (size_t)ry * cPitch + rx];
+      }
+      s_c[idx] = v;
+    }
+  }
+  __syncthreads();
+
+  float dmax;
+  if (pattern == 1)
+    dmax = stencil_block<1>(s_c, P, x0, y0, W, H, gain, wT, wR, Dmap, Smap, dPitch);
+  else if (pattern == 2)
+    dmax = stencil_block<2>(s_c, P, x0, y0, W, H, gain, wT, wR, Dmap, Smap, dPitch);
+  else
+    dmax = stencil_block<0>(s_c, P, x0, y0, W, H, gain, wT, wR, Dmap, Smap, dPitch);
   // block max -> one atomic per block
 #pragma unroll
   for (int m = 16; m > 0; m >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
@@ -374,7 +273,7 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
   if (t == 0) {
     float m = s_max[0];
     for (int k = 1; k < 8; ++k) m = fmaxf(m, s_max[k]);
-    if (m > -INFINITY) atomicMax(sd->maxKey, float_key(m));
+    if (m > -INFINITY) atomicMax(maxKey, float_key(m));
   }
 }
 
@@ -550,9 +449,7 @@ cudaError_t upload_twiddles() {
   return cudaMemcpyToSymbol(c_w128, h, sizeof(h));
 }
 
-size_t gabor_smem_bytes() {
-  return sizeof(float2) * (kTile * kTileLD + kTile * kXhCols + 8 * 17) + sizeof(int) * 2 * kTile;
-}
+size_t gabor_smem_bytes() { return kGaborSmem; }
 size_t stencil_smem_bytes() { return sizeof(float) * kNumOri * kStH * kStW; }
 
 cudaError_t configure_kernels() {
@@ -569,8 +466,9 @@ void launch_pyr(const PyrJob* d_jobs, int njobs, int maxW, int maxH, cudaStream_
   dim3 b(32, 8), g((maxW + 31) / 32, (maxH + 7) / 8, njobs);
   k_pyr_down<<<g, b, 0, s>>>(d_jobs);
 }
-void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, cudaStream_t s) {
-  k_gabor_tiles<<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork);
+void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
+                  cudaStream_t s) {
+  k_gabor_tiles<<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
 }
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
   k_stencil<<<nwork, 256, stencil_smem_bytes(), s>>>(d_sd, d_work);

@@ -29,7 +29,9 @@ size_t gabor_smem_bytes();
 size_t stencil_smem_bytes();
 
 void launch_pyr(const PyrJob* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
-void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, cudaStream_t s);
+// d_fault: word that receives 1 if a bounded device wait expired.
+void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
+                  cudaStream_t s);
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,

@@ -187,3 +187,19 @@ def test_batch_matches_single():
     got0 = api.keypoint_matrix_to_records(b.keypoints(0))
     cs = api.CudaStuff(imgs[0].shape[1], imgs[0].shape[0], lam)
     assert np.array_equal(got0, api.keypoint_matrix_to_records(api.getKeypoints(imgs[0], cs, capacity=100000)))
+
+
+def test_persistent_tile_loop_matches(monkeypatch):
+    """Each CTA of the tile kernel walks many tiles (grid capped at 7): the
+    spectrum double buffer's phases carry across tiles; results unchanged."""
+    imgs, lam = synth.workload("vga")
+    img = imgs[0]
+    cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
+    ref = api.keypoint_matrix_to_records(api.getKeypoints(img, cs, capacity=100000))
+    d_ref = [cs.dense_map(i).cpu().numpy() for i in range(len(lam))]
+    monkeypatch.setenv("BIMP_TILE_GRID", "7")
+    cs2 = api.CudaStuff(img.shape[1], img.shape[0], lam)
+    got = api.keypoint_matrix_to_records(api.getKeypoints(img, cs2, capacity=100000))
+    assert np.array_equal(ref, got)
+    for i in range(len(lam)):
+        assert np.array_equal(d_ref[i], cs2.dense_map(i).cpu().numpy())
