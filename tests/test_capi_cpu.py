@@ -68,3 +68,18 @@ def test_keypoint_struct_layout_is_cv_keypoint():
     assert C.sizeof(L.KeyPointC) == 28
     assert [f for f, _ in L.KeyPointC._fields_] == ["x", "y", "size", "angle", "response", "octave", "class_id"]
     assert C.sizeof(L.Params) == 9 * 8
+
+
+def _build_shim_demo():
+    import subprocess
+    out = ROOT / "cuda-bimp_b200" / "_build" / "shim_demo"
+    out.parent.mkdir(parents=True, exist_ok=True)
+    lib = ROOT / "cuda-bimp_b200" / "lib"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", f"-I{ROOT / 'include'}",
+                    str(ROOT / "tests" / "cpp" / "shim_demo.cpp"), f"-L{lib}", "-lbimp_b200",
+                    f"-Wl,-rpath,{lib}", "-o", str(out)], check=True)
+    return out
+
+
+def test_cpp_shim_compiles_and_links():
+    assert _build_shim_demo().exists()
