@@ -203,3 +203,25 @@ def test_persistent_tile_loop_matches(monkeypatch):
     assert np.array_equal(ref, got)
     for i in range(len(lam)):
         assert np.array_equal(d_ref[i], cs2.dense_map(i).cpu().numpy())
+
+
+def test_cpp_context_shim_matches_python_api(tmp_path):
+    """bimp::Context (include/bimp/bimp.hpp) from a C++ program: the same
+    keypoints as the Python path through the C ABI."""
+    import subprocess
+    from test_capi_cpu import _build_shim_demo
+    exe = _build_shim_demo()
+    imgs, lam = synth.workload("vga")
+    img = imgs[0]
+    raw = tmp_path / "img.raw"
+    raw.write_bytes(np.ascontiguousarray(img).tobytes())
+    res = subprocess.run([str(exe), str(img.shape[1]), str(img.shape[0]), str(raw)] + [repr(x) for x in lam],
+                         check=True, capture_output=True, text=True)
+    rows = [ln.split() for ln in res.stdout.splitlines()]
+    cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
+    ref = api.keypoint_matrix_to_records(api.getKeypoints(img, cs, capacity=200000))
+    assert len(rows) == len(ref) > 0
+    got = np.array([[float(r[0]), float(r[1]), float(r[2])] for r in rows], dtype=np.float32)
+    assert np.array_equal(got[:, 0], ref["x"]) and np.array_equal(got[:, 1], ref["y"])
+    assert np.array_equal(got[:, 2], ref["size"])
+    assert all(int(r[5]) == 1 and float(r[6]) == -1.0 for r in rows)
