@@ -73,6 +73,9 @@ _PROTOS = [
                                    C.POINTER(KeyPointC), C.c_int, C.POINTER(C.c_int), C.c_void_p]),
     ("bimp_dense_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("bimp_complex_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
+    ("bimp_extract_keypoints_noalloc", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_float, C.c_float,
+                                                 C.c_double, C.c_void_p, C.c_size_t, C.c_int, C.c_void_p,
+                                                 C.c_void_p]),
     ("bimp_ctx_kernel_launches", C.c_int, [C.c_void_p]),
     ("bimp_ctx_run_stage", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     ("bimp_download_keypoints", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(KeyPointC),

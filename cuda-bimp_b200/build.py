@@ -30,6 +30,7 @@ SOURCES = [
     ("bank.cpp", "cxx"),
     ("kernels.cu", "cuda"),
     ("capi.cu", "cuda"),
+    ("noalloc.cu", "cuda"),
 ]
 HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
 

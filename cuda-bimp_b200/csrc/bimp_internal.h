@@ -97,6 +97,9 @@ bool build_scales(int width, int height, const std::vector<float>& lambdas,
                   const bimp_params& p, std::vector<ScaleHost>& out, std::string& err);
 void tile_spectrum(const ScaleHost& s, std::vector<float>& out);
 
+// Sets the message returned by bimp_last_error() on the calling thread.
+void record_error(const std::string& msg);
+
 // Position of natural frequency k in the digit-permuted 128-point layout.
 inline int perm128(int k) { return 8 * (k & 15) + (k >> 4); }
 

@@ -85,6 +85,9 @@ struct Arena {
 
 }  // namespace
 
+// Lets other translation units report through bimp_last_error().
+void bimp_b200::record_error(const std::string& msg) { g_last_error = msg; }
+
 // ---------------------------------------------------------------------------
 // shared engine: N images with their own sizes, one wavelength bank
 // ---------------------------------------------------------------------------

@@ -160,6 +160,32 @@ int bimp_dense_map(bimp_context* ctx, int scale, int which, float* d_out,
 int bimp_complex_map(bimp_context* ctx, int scale, int orientation, float* d_out,
                      size_t ld, void* stream);
 
+/* ---- keypoint extraction without allocation ------------------------------
+ * No counterpart in the reference (its extraction, cuda_gpu_keypoints,
+ * allocates GpuMats and thrust/NPP temporaries on every call).  For callers
+ * that must not allocate device memory while they run: work being captured
+ * into a CUDA graph, real-time loops kept away from the allocator, or hosts
+ * whose device memory belongs to a pool the library may not touch.
+ *
+ * Threshold (thresh_ratio * max of the map), strict 8-neighbour maxima,
+ * margin (int)lambda_level and parabolic subpixel refinement on one summed
+ * keypoint map `d_map` (height x width floats, row pitch `ld` floats), records
+ * written to the 7 x kp_ld device matrix `d_kp` in (y, x) order, the total to
+ * the device int `d_count`.  Identical results to the extraction step of
+ * bimp_detect_device for the same map.
+ *
+ * All scratch lives in one fixed device array of about 260 KB per device
+ * (held until the process exits); maps with more than 16384 candidate rows
+ * are rejected with BIMP_ERR_UNSUPPORTED.  Nothing is allocated: no
+ * cudaMalloc, cudaFree or allocating library call.  The first call on a
+ * device looks up the array's device address once (with that device
+ * current); make that first call before any stream capture.  Every call
+ * shares the array: calls whose GPU work overlaps (unordered streams) race. */
+int bimp_extract_keypoints_noalloc(const float* d_map, size_t ld, int width, int height,
+                                   float lambda_level, float pyrstep, double thresh_ratio,
+                                   float* d_kp, size_t kp_ld, int capacity, int* d_count,
+                                   void* stream);
+
 /* ---- measurement hooks (no counterpart in the reference) -----------------
  * Number of kernel launches one detection enqueues (all scales). */
 int bimp_ctx_kernel_launches(const bimp_context* ctx);
