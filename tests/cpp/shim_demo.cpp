@@ -34,7 +34,7 @@ int main(int argc, char** argv) {
     ctx.capacity = 1 << 20;
     const std::vector<bimp::KeyPoint> pts = ctx.getKeypointsAndDownload();
     for (const auto& k : pts)
-      std::printf("%.6f %.6f %.6f %.9g %d %d %.1f\n", k.pt.x, k.pt.y, k.size, k.response, k.octave, k.class_id,
+      std::printf("%.9g %.9g %.9g %.9g %d %d %.1f\n", k.pt.x, k.pt.y, k.size, k.response, k.octave, k.class_id,
                   k.angle);
     std::fprintf(stderr, "%zu keypoints\n", pts.size());
   } catch (const bimp::Error& e) {
