@@ -122,6 +122,25 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+# multi-process plumbing (replicas: no collective on the data path)
+# ---------------------------------------------------------------------------
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Max of a per-rank timing over all ranks (all_reduce MAX); identity at N=1."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(pixels_per_step: int, steps: int, world: int, max_ms: float) -> float:
+    """Whole-job Mpixel/s: every rank processed `steps` images of `pixels_per_step`."""
+    return world * steps * pixels_per_step / (max_ms * 1e-3) / 1e6
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def algorithmic_bytes(cs) -> dict:
@@ -187,12 +206,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def max_ms(x: float) -> float:
+        return max_over_ranks(x, world, dev)
 
     for i in range(args.warmup):
         detect(pool[i % POOL])
@@ -212,9 +227,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     barrier()
     ms_local = e0.elapsed_time(e1)
     clk = clocks.stop() if rank == 0 else None
-    ms = max_over_ranks(ms_local)
+    ms = max_ms(ms_local)
     n_kp = int(cnt.item())
-    value = world * args.steps * W_HD * H_HD / (ms * 1e-3) / 1e6
+    value = replica_throughput(W_HD * H_HD, args.steps, world, ms)
 
     # -- dominant kernel timed alone (same stream) --------------------------
     stage_ms = {}
@@ -268,7 +283,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             detect_host(pinned[i % 8])
         b.record(stream)
         torch.cuda.synchronize()
-        ms_e2e = max_over_ranks(a.elapsed_time(b))
+        ms_e2e = max_ms(a.elapsed_time(b))
         e2e = {"value": round(world * k_e2e * W_HD * H_HD / (ms_e2e * 1e-3) / 1e6, 2), "unit": UNIT,
                "h2d_bytes_per_step": W_HD * H_HD, "d2h_bytes_per_step": int(np.mean(d2h)),
                "steps": k_e2e, "api": "bimp_detect_host"}
@@ -292,7 +307,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             bt.run()
         b.record(stream)
         torch.cuda.synchronize()
-        ms_b = max_over_ranks(a.elapsed_time(b))
+        ms_b = max_ms(a.elapsed_time(b))
         # plain: one context per image, detected one after another
         ctxs = [api.CudaStuff(w, h, lam_b) for w, h in sizes]
         gimgs = [torch.from_numpy(im).to(dev) for im in imgs]
@@ -312,7 +327,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             plain_all()
         b.record(stream)
         torch.cuda.synchronize()
-        ms_p = max_over_ranks(a.elapsed_time(b))
+        ms_p = max_ms(a.elapsed_time(b))
         batched = {"workload": "64 mixed images, W in [320,1920], H in [240,1080], 8 scales",
                    "value": round(world * kb * px / (ms_b * 1e-3) / 1e6, 2),
                    "plain_value": round(world * kb * px / (ms_p * 1e-3) / 1e6, 2),

@@ -52,7 +52,7 @@ struct ScaleDev {
   float pyrstep;
   float kpSize;           // lambda*pyrstep
   int kpOctave;           // (int)(lambda*pyrstep)
-  float threshRatio;
+  double threshRatio;     // double, as the reference multiplies max by the literal 0.104
   int rowBase;            // first entry of this scale in the per-row count array
   int image;              // image index inside a batch
   int pattern;            // stencil offsets: 0 = runtime, k > 0 = kOffsetSets[k-1]

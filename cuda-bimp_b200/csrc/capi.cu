@@ -229,7 +229,7 @@ struct Engine {
         d.pyrstep = s.pyrstep;
         d.kpSize = s.lambda * s.pyrstep;
         d.kpOctave = static_cast<int>(s.lambda * s.pyrstep);
-        d.threshRatio = static_cast<float>(p.thresh_ratio);
+        d.threshRatio = p.thresh_ratio;
         d.image = i;
         const int entry = static_cast<int>(sds.size());
         d.rowBase = static_cast<int>(rows.size());

@@ -283,7 +283,7 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
 __device__ __forceinline__ float scale_thresh(const ScaleDev* sd) {
   // cuda_bimp.cu:720-721: float max, double thresh, passed as float
   const float mx = key_float(*sd->maxKey);
-  return (float)((double)mx * (double)sd->threshRatio);
+  return (float)((double)mx * sd->threshRatio);
 }
 
 __device__ __forceinline__ bool is_keypoint(const float* __restrict__ D, int dp, int x, int y, float thr) {

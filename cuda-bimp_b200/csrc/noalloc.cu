@@ -130,7 +130,7 @@ extern "C" int bimp_extract_keypoints_noalloc(const float* d_map, size_t ld, int
   sd.pyrstep = pyrstep;
   sd.kpSize = lambda_level * pyrstep;
   sd.kpOctave = static_cast<int>(lambda_level * pyrstep);
-  sd.threshRatio = static_cast<float>(thresh_ratio);
+  sd.threshRatio = thresh_ratio;
   KpOut out;
   out.kp = d_kp;
   out.ld = kp_ld;
