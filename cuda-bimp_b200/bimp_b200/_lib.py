@@ -73,6 +73,12 @@ _PROTOS = [
                                    C.POINTER(KeyPointC), C.c_int, C.POINTER(C.c_int), C.c_void_p]),
     ("bimp_dense_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("bimp_complex_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
+    ("bimp_min_size_dims", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_double)]),
+    ("bimp_gpu_image", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                 C.c_size_t, C.c_void_p]),
+    ("bimp_color_features", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p, C.c_size_t, C.c_int, C.c_int,
+                                      C.c_void_p, C.c_size_t, C.c_void_p]),
     ("bimp_extract_keypoints_noalloc", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_float, C.c_float,
                                                  C.c_double, C.c_void_p, C.c_size_t, C.c_int, C.c_void_p,
                                                  C.c_void_p]),
@@ -81,6 +87,16 @@ _PROTOS = [
     ("bimp_download_keypoints", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(KeyPointC),
                                           C.c_void_p]),
     ("bimp_upload_keypoints", C.c_int, [C.POINTER(KeyPointC), C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
+    ("bimp_adjoint_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float),
+                                      C.c_int, C.POINTER(Params)]),
+    ("bimp_adjoint_destroy", C.c_int, [C.c_void_p]),
+    ("bimp_adjoint_num_scales", C.c_int, [C.c_void_p]),
+    ("bimp_adjoint_mask_layout", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                           C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    ("bimp_adjoint_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("bimp_adjoint_backward", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    ("bimp_adjoint_dense_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
+    ("bimp_adjoint_device_bytes", C.c_size_t, [C.c_void_p]),
     ("bimp_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int,
                                     C.POINTER(C.c_float), C.c_int, C.POINTER(Params), C.c_int]),
     ("bimp_batch_destroy", C.c_int, [C.c_void_p]),

@@ -221,6 +221,39 @@ def detect_host(cs: CudaStuff, image: np.ndarray, capacity: int = KP_MAX_POINTS)
     return rec, n.value, rc
 
 
+def gpu_image(image: np.ndarray, grayscale: bool = True) -> np.ndarray:
+    """getGPUImage (cuda_bimp.cu:156-180): upscale below 350 px and BGR -> grey
+    on the device; returns the host copy of the result."""
+    torch = _torch()
+    img = np.ascontiguousarray(image, dtype=np.uint8)
+    h, w = img.shape[:2]
+    cn = 1 if img.ndim == 2 else img.shape[2]
+    ow, oh = C.c_int(), C.c_int()
+    L.check(L.lib().bimp_min_size_dims(w, h, C.byref(ow), C.byref(oh), None), "min_size_dims")
+    ocn = 1 if (grayscale or cn == 1) else cn
+    src = torch.from_numpy(img.reshape(h, w * cn)).cuda()
+    dst = torch.empty((oh.value, ow.value * ocn), dtype=torch.uint8, device="cuda")
+    L.check(L.lib().bimp_gpu_image(C.c_void_p(src.data_ptr()), src.stride(0), w, h, cn, int(bool(grayscale)),
+                                   C.c_void_p(dst.data_ptr()), dst.stride(0), _stream_ptr()), "gpu_image")
+    out = dst.cpu().numpy()
+    return out if ocn == 1 else out.reshape(oh.value, ow.value, ocn)
+
+
+def color_features(kp, bgr: np.ndarray) -> np.ndarray:
+    """addColorFeatures (cuda_bimp.cu:950-958): 24-bin colour histograms of
+    the keypoints in the 7 x n device matrix over a BGR image."""
+    torch = _torch()
+    img = np.ascontiguousarray(bgr, dtype=np.uint8)
+    h, w = img.shape[:2]
+    n = kp.shape[1]
+    src = torch.from_numpy(img.reshape(h, w * 3)).cuda()
+    desc = torch.empty((max(n, 1), 24), dtype=torch.float32, device="cuda")
+    L.check(L.lib().bimp_color_features(C.c_void_p(kp.data_ptr()), kp.stride(0), n, C.c_void_p(src.data_ptr()),
+                                        src.stride(0), w, h, C.c_void_p(desc.data_ptr()), desc.stride(0),
+                                        _stream_ptr()), "color_features")
+    return desc[:n].cpu().numpy()
+
+
 def keypoint_matrix_to_records(kp) -> np.ndarray:
     """7 x n device matrix -> structured numpy array (host)."""
     h = kp.detach().cpu().numpy()
@@ -357,6 +390,77 @@ class Batch:
             pass
 
 
+class Adjoint:
+    """Gradient of L = sum M * D (summed keypoint maps) for n float images.
+
+    forward(images, masks) -> loss; backward() -> (dL/dimages, dL/d(alpha,
+    rho, w_tan, w_rad)).  images: float32 CUDA tensor (n, H, W); masks: float32
+    CUDA tensor of n * mask_stride elements laid out by mask_views().
+    """
+
+    def __init__(self, width: int, height: int, n_images: int, lambdas, params=None):
+        lam = (C.c_float * len(lambdas))(*[float(x) for x in lambdas])
+        p = _params(params)
+        h = C.c_void_p()
+        L.check(L.lib().bimp_adjoint_create(C.byref(h), int(width), int(height), int(n_images), lam, len(lambdas),
+                                            C.byref(p) if p is not None else None), "Adjoint")
+        self._h = h
+        self.width, self.height, self.n = int(width), int(height), int(n_images)
+        self.layout = []
+        for s in range(L.lib().bimp_adjoint_num_scales(h)):
+            w, hh, off, stride = C.c_int(), C.c_int(), C.c_size_t(), C.c_size_t()
+            L.check(L.lib().bimp_adjoint_mask_layout(h, s, C.byref(w), C.byref(hh), C.byref(off), C.byref(stride)),
+                    "mask_layout")
+            self.layout.append((off.value, w.value, hh.value))
+            self.mask_stride = stride.value
+        torch = _torch()
+        self._loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        self._gp = torch.zeros(4, dtype=torch.float64, device="cuda")
+
+    def mask_views(self, masks):
+        """[(image, scale) -> (h, w) view] of a flat mask tensor."""
+        return [[masks[i * self.mask_stride + off:i * self.mask_stride + off + w * h].view(h, w)
+                 for (off, w, h) in self.layout] for i in range(self.n)]
+
+    def forward(self, images, masks, stream=None):
+        assert images.dtype == _torch().float32 and images.is_contiguous() and masks.is_contiguous()
+        L.check(L.lib().bimp_adjoint_forward(self._h, C.c_void_p(images.data_ptr()), images.shape[-1],
+                                             C.c_void_p(masks.data_ptr()), C.c_void_p(self._loss.data_ptr()),
+                                             _stream_ptr(stream)), "adjoint_forward")
+        return self._loss
+
+    def backward(self, grad=None, stream=None):
+        torch = _torch()
+        if grad is None:
+            grad = torch.empty((self.n, self.height, self.width), dtype=torch.float32, device="cuda")
+        L.check(L.lib().bimp_adjoint_backward(self._h, C.c_void_p(grad.data_ptr()), grad.shape[-1],
+                                              C.c_void_p(self._gp.data_ptr()), _stream_ptr(stream)),
+                "adjoint_backward")
+        return grad, self._gp
+
+    def dense_map(self, image: int, scale: int):
+        torch = _torch()
+        off, w, h = self.layout[scale]
+        out = torch.empty((h, w), dtype=torch.float32, device="cuda")
+        L.check(L.lib().bimp_adjoint_dense_map(self._h, image, scale, C.c_void_p(out.data_ptr()), out.stride(0),
+                                               _stream_ptr()), "adjoint_dense_map")
+        return out
+
+    def device_bytes(self) -> int:
+        return int(L.lib().bimp_adjoint_device_bytes(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            L.lib().bimp_adjoint_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _wrap_device(ptr: int, shape, strides_bytes, typestr: str):
     """A CUDA tensor aliasing library-owned device memory (no copy)."""
     torch = _torch()
@@ -378,7 +482,7 @@ class _nullcontext:
 
 __all__ = ["KeyPoint", "CudaStuff", "Context", "Batch", "getKeypoints", "downloadKeypoints",
            "uploadKeypoints", "makeLambdasLog", "makeLambdasLin", "snapTransformSize", "detect_host",
-           "keypoint_matrix_to_records", "default_params", "KP_MAX_POINTS"]
+           "keypoint_matrix_to_records", "default_params", "KP_MAX_POINTS", "gpu_image", "color_features", "Adjoint"]
 
 if sys.version_info < (3, 8):  # pragma: no cover
     raise RuntimeError("python >= 3.8 required")

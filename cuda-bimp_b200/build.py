@@ -31,6 +31,8 @@ SOURCES = [
     ("kernels.cu", "cuda"),
     ("capi.cu", "cuda"),
     ("noalloc.cu", "cuda"),
+    ("extras.cu", "cuda"),
+    ("adjoint.cu", "cuda"),
 ]
 HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
 

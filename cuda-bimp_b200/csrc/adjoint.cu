@@ -1,0 +1,376 @@
+// Host side of the adjoint (include/bimp_b200_adjoint.h): one arena holding
+// the float pyramid, saved responses, maps and gradients of n equally sized
+// images, and the launch sequences of the forward and backward.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bimp_b200.h"
+#include "bimp_b200_adjoint.h"
+#include "bimp_internal.h"
+#include "kernels.h"
+
+using namespace bimp_b200;
+
+namespace {
+
+int afail(int code, const std::string& m) {
+  record_error(m);
+  return code;
+}
+
+#define ADJ_CUDA(call)                                                                                  \
+  do {                                                                                                  \
+    cudaError_t e_ = (call);                                                                            \
+    if (e_ != cudaSuccess)                                                                              \
+      return afail(e_ == cudaErrorMemoryAllocation ? BIMP_ERR_NOMEM : BIMP_ERR_CUDA,                     \
+                   std::string(#call) + ": " + cudaGetErrorString(e_));                                 \
+  } while (0)
+
+size_t up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+int rha(double v) { return static_cast<int>(v >= 0 ? std::floor(v + 0.5) : -std::floor(-v + 0.5)); }
+
+}  // namespace
+
+struct bimp_adjoint {
+  int device = 0, W = 0, H = 0, n = 0, nScales = 0, maxLevel = 0;
+  bimp_params params{};
+  std::vector<ScaleHost> geo;
+  char* mem = nullptr;
+  size_t bytes = 0;
+  std::vector<ScaleDev> h_sd;
+  ScaleDev* d_sd = nullptr;
+  TileWork* d_tiles = nullptr;
+  int nTiles = 0;
+  int2* d_sten = nullptr;
+  int nSten = 0;
+  int2* d_stenB = nullptr;
+  int nStenB = 0;
+  int* d_wrap = nullptr;
+  int nWrap = 0;
+  std::vector<float*> lvl, glvl;          // per image per level
+  std::vector<int> lw, lh, lp;            // per level (same for all images)
+  PyrJobF* d_pyr = nullptr;               // [level-1][image] forward jobs
+  PyrJobF* d_pyrAdj = nullptr;            // [level-1][image] transpose jobs
+  float* d_M = nullptr;
+  size_t maskStride = 0;
+  std::vector<size_t> maskOff;
+  float* d_gwin = nullptr;
+  double* d_loss = nullptr;
+  double* d_gp = nullptr;
+  unsigned int* d_max = nullptr;           // per entry + fault word
+  std::vector<size_t> gcOff, gcBytes;
+
+  int build(int dev, int w, int h, int ni, const float* lambdas, int nl, const bimp_params& p) {
+    device = dev;
+    W = w;
+    H = h;
+    n = ni;
+    params = p;
+    std::string err;
+    if (!build_scales(w, h, std::vector<float>(lambdas, lambdas + nl), p, geo, err)) return afail(BIMP_ERR_INVALID, err);
+    nScales = static_cast<int>(geo.size());
+    for (auto& s : geo) maxLevel = std::max(maxLevel, s.level);
+    // derivative spectra
+    std::vector<std::vector<float>> dga(nScales), dgr(nScales);
+    for (int s = 0; s < nScales; ++s) {
+      std::vector<float> ea[kNumOri], oa[kNumOri], er[kNumOri], orr[kNumOri];
+      derivative_taps(geo[s], p, ea, oa, er, orr);
+      tile_spectrum(ea, oa, geo[s].kW, geo[s].kX, dga[s]);
+      tile_spectrum(er, orr, geo[s].kW, geo[s].kX, dgr[s]);
+    }
+    // ---- layout
+    size_t at = 0;
+    auto take = [&](size_t b) { const size_t o = up(at, 256); at = o + b; return o; };
+    const size_t specB = sizeof(float) * (size_t)kNumOri * kSpecFloats;
+    const size_t offG = take(specB * nScales), offGa = take(specB * nScales), offGr = take(specB * nScales);
+    int cw = w, ch = h;
+    for (int l = 0; l <= maxLevel; ++l) {
+      if (l > 0) { cw = (cw + 1) / 2; ch = (ch + 1) / 2; }
+      lw.push_back(cw);
+      lh.push_back(ch);
+      lp.push_back(static_cast<int>(up(cw, 32)));
+    }
+    std::vector<size_t> offL, offGL;
+    for (int i = 0; i < n; ++i)
+      for (int l = 0; l <= maxLevel; ++l) {
+        offL.push_back(take(sizeof(float) * (size_t)lp[l] * lh[l]));
+        offGL.push_back(take(sizeof(float) * (size_t)lp[l] * lh[l]));
+      }
+    maskStride = 0;
+    for (auto& s : geo) {
+      maskOff.push_back(maskStride);
+      maskStride += (size_t)s.dataW * s.dataH;
+    }
+    const size_t offM = take(sizeof(float) * maskStride * n);
+    std::vector<TileWork> tiles;
+    std::vector<int2> sten, stenB;
+    std::vector<int> wraps;
+    std::vector<ScaleDev> sds;
+    std::vector<size_t> offC, offZ, offD, offS, offGC;
+    for (int i = 0; i < n; ++i) {
+      for (int si = 0; si < nScales; ++si) {
+        const ScaleHost& s = geo[si];
+        ScaleDev d;
+        std::memset(&d, 0, sizeof(d));
+        d.dataW = s.dataW; d.dataH = s.dataH; d.fftW = s.fftW; d.fftH = s.fftH;
+        d.kX = s.kX;
+        d.V = kTile - 2 * s.kX;
+        d.cRows = s.dataH + 2;
+        d.cCols = s.dataW + 1;
+        d.tilesX = (d.cCols + d.V - 1) / d.V;
+        d.tilesY = (d.cRows + d.V - 1) / d.V;
+        d.wrapW = s.fftW == s.dataW ? 1 : 0;
+        d.lvlW = lw[s.level];
+        d.lvlH = lh[s.level];
+        d.lvlPitchF = lp[s.level];
+        d.cPitch = static_cast<int>(up(s.dataW + 1, 32));
+        d.cStride = (long long)(s.dataH + 2) * d.cPitch;
+        for (int o = 0; o < kNumOri; ++o) {
+          d.es1[o] = s.es1[o]; d.es2[o] = s.es2[o];
+          d.in1[o] = s.in1[o]; d.in2[o] = s.in2[o];
+          d.ih1[o] = rha(0.5 * s.in1[o]);
+          d.ih2[o] = rha(0.5 * s.in2[o]);
+        }
+        d.pattern = 0;
+        for (int set = 0; set < kNumOffsetSets && d.pattern == 0; ++set) {
+          bool same = true;
+          for (int o = 0; o < kNumOri; ++o)
+            same = same && d.es1[o] == kOffsetSets[set][0][o] && d.es2[o] == kOffsetSets[set][1][o] &&
+                   d.in1[o] == kOffsetSets[set][2][o] && d.in2[o] == kOffsetSets[set][3][o] &&
+                   d.ih1[o] == kOffsetSets[set][4][o] && d.ih2[o] == kOffsetSets[set][5][o];
+          if (same) d.pattern = set + 1;
+        }
+        d.radialGain = static_cast<float>(p.radial_gain);
+        d.wTan = static_cast<float>(p.w_tan);
+        d.wRad = static_cast<float>(p.w_rad);
+        d.dPitch = static_cast<int>(up(s.dataW, 32));
+        d.off = s.off;
+        d.pyrstep = s.pyrstep;
+        d.threshRatio = p.thresh_ratio;
+        d.image = i;
+        const int entry = static_cast<int>(sds.size());
+        for (int tI = 0; tI < d.tilesX * d.tilesY; ++tI) tiles.push_back({entry, tI});
+        const int nbx = (s.dataW + 31) / 32, nby = (s.dataH + 31) / 32;
+        for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
+        const int nbx2 = (s.dataW + 1 + 31) / 32, nby2 = (s.dataH + 1 + 31) / 32;
+        for (int b = 0; b < nbx2 * nby2; ++b) stenB.push_back(make_int2(entry, b));
+        if (d.wrapW) wraps.push_back(entry);
+        offC.push_back(take(sizeof(float) * (size_t)kNumOri * d.cStride));
+        offZ.push_back(take(sizeof(float2) * (size_t)kNumOri * d.cStride));
+        offGC.push_back(take(sizeof(float) * (size_t)kNumOri * d.cStride));
+        offD.push_back(take(sizeof(float) * (size_t)s.dataH * d.dPitch));
+        offS.push_back(take(sizeof(float) * (size_t)s.dataH * d.dPitch));
+        sds.push_back(d);
+      }
+    }
+    nTiles = static_cast<int>(tiles.size());
+    nSten = static_cast<int>(sten.size());
+    nStenB = static_cast<int>(stenB.size());
+    nWrap = static_cast<int>(wraps.size());
+    const size_t offSd = take(sizeof(ScaleDev) * sds.size());
+    const size_t offT = take(sizeof(TileWork) * tiles.size());
+    const size_t offSt = take(sizeof(int2) * sten.size());
+    const size_t offStB = take(sizeof(int2) * stenB.size());
+    const size_t offWr = take(sizeof(int) * std::max<size_t>(1, wraps.size()));
+    const size_t offPyr = take(sizeof(PyrJobF) * std::max(1, maxLevel * n));
+    const size_t offPyrA = take(sizeof(PyrJobF) * std::max(1, maxLevel * n));
+    const size_t offWin = take(sizeof(float) * (size_t)nTiles * kTile * kTile);
+    const size_t offLoss = take(sizeof(double) * 8);
+    const size_t offMax = take(sizeof(unsigned int) * (sds.size() + 1));
+    bytes = at;
+    cudaError_t e = cudaMalloc(&mem, bytes);
+    if (e != cudaSuccess) {
+      mem = nullptr;
+      return afail(BIMP_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    char* b = mem;
+    float* dG = reinterpret_cast<float*>(b + offG);
+    float* dGa = reinterpret_cast<float*>(b + offGa);
+    float* dGr = reinterpret_cast<float*>(b + offGr);
+    for (int i = 0; i < n; ++i)
+      for (int l = 0; l <= maxLevel; ++l) {
+        lvl.push_back(reinterpret_cast<float*>(b + offL[i * (maxLevel + 1) + l]));
+        glvl.push_back(reinterpret_cast<float*>(b + offGL[i * (maxLevel + 1) + l]));
+      }
+    d_M = reinterpret_cast<float*>(b + offM);
+    d_max = reinterpret_cast<unsigned int*>(b + offMax);
+    for (size_t e2 = 0; e2 < sds.size(); ++e2) {
+      ScaleDev& d = sds[e2];
+      const int i = d.image, si = static_cast<int>(e2 % nScales);
+      const ScaleHost& s = geo[si];
+      d.lvlF = lvl[i * (maxLevel + 1) + s.level];
+      d.gLvl = glvl[i * (maxLevel + 1) + s.level];
+      d.G = dG + (size_t)si * kNumOri * kSpecFloats;
+      d.dGa = dGa + (size_t)si * kNumOri * kSpecFloats;
+      d.dGr = dGr + (size_t)si * kNumOri * kSpecFloats;
+      d.C = reinterpret_cast<float*>(b + offC[e2]);
+      d.Z = reinterpret_cast<float2*>(b + offZ[e2]);
+      d.gC = reinterpret_cast<float*>(b + offGC[e2]);
+      d.D = reinterpret_cast<float*>(b + offD[e2]);
+      d.S = reinterpret_cast<float*>(b + offS[e2]);
+      d.M = d_M + (size_t)i * maskStride + maskOff[si];
+      d.maxKey = d_max + e2;
+      gcOff.push_back(offGC[e2]);
+      gcBytes.push_back(sizeof(float) * (size_t)kNumOri * d.cStride);
+    }
+    h_sd = sds;
+    d_sd = reinterpret_cast<ScaleDev*>(b + offSd);
+    d_tiles = reinterpret_cast<TileWork*>(b + offT);
+    d_sten = reinterpret_cast<int2*>(b + offSt);
+    d_stenB = reinterpret_cast<int2*>(b + offStB);
+    d_wrap = reinterpret_cast<int*>(b + offWr);
+    d_pyr = reinterpret_cast<PyrJobF*>(b + offPyr);
+    d_pyrAdj = reinterpret_cast<PyrJobF*>(b + offPyrA);
+    d_gwin = reinterpret_cast<float*>(b + offWin);
+    d_loss = reinterpret_cast<double*>(b + offLoss);
+    d_gp = d_loss + 1;
+    // uploads
+    for (int si = 0; si < nScales; ++si) {
+      ADJ_CUDA(cudaMemcpy(dG + (size_t)si * kNumOri * kSpecFloats, geo[si].spectrum.data(), specB,
+                          cudaMemcpyHostToDevice));
+      ADJ_CUDA(cudaMemcpy(dGa + (size_t)si * kNumOri * kSpecFloats, dga[si].data(), specB, cudaMemcpyHostToDevice));
+      ADJ_CUDA(cudaMemcpy(dGr + (size_t)si * kNumOri * kSpecFloats, dgr[si].data(), specB, cudaMemcpyHostToDevice));
+    }
+    ADJ_CUDA(cudaMemcpy(d_sd, sds.data(), sizeof(ScaleDev) * sds.size(), cudaMemcpyHostToDevice));
+    ADJ_CUDA(cudaMemcpy(d_tiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice));
+    ADJ_CUDA(cudaMemcpy(d_sten, sten.data(), sizeof(int2) * sten.size(), cudaMemcpyHostToDevice));
+    ADJ_CUDA(cudaMemcpy(d_stenB, stenB.data(), sizeof(int2) * stenB.size(), cudaMemcpyHostToDevice));
+    if (!wraps.empty())
+      ADJ_CUDA(cudaMemcpy(d_wrap, wraps.data(), sizeof(int) * wraps.size(), cudaMemcpyHostToDevice));
+    std::vector<PyrJobF> fj, aj;
+    for (int l = 1; l <= maxLevel; ++l)
+      for (int i = 0; i < n; ++i) {
+        PyrJobF j;
+        j.src = lvl[i * (maxLevel + 1) + l - 1];
+        j.sw = lw[l - 1]; j.sh = lh[l - 1]; j.sp = lp[l - 1];
+        j.dst = lvl[i * (maxLevel + 1) + l];
+        j.dw = lw[l]; j.dh = lh[l]; j.dp = lp[l];
+        fj.push_back(j);
+        PyrJobF a = j;   // transpose: read level l gradient, scatter into level l-1
+        a.src = glvl[i * (maxLevel + 1) + l];
+        a.sp = lp[l];
+        a.dst = glvl[i * (maxLevel + 1) + l - 1];
+        a.dp = lp[l - 1];
+        aj.push_back(a);
+      }
+    if (!fj.empty()) {
+      ADJ_CUDA(cudaMemcpy(d_pyr, fj.data(), sizeof(PyrJobF) * fj.size(), cudaMemcpyHostToDevice));
+      ADJ_CUDA(cudaMemcpy(d_pyrAdj, aj.data(), sizeof(PyrJobF) * aj.size(), cudaMemcpyHostToDevice));
+    }
+    return BIMP_OK;
+  }
+
+  int forward(const float* imgs, size_t pitch, const float* masks, double* loss, cudaStream_t s) {
+    for (int i = 0; i < n; ++i)
+      ADJ_CUDA(cudaMemcpy2DAsync(lvl[i * (maxLevel + 1)], sizeof(float) * lp[0], imgs + (size_t)i * H * pitch,
+                                 sizeof(float) * pitch, sizeof(float) * W, H, cudaMemcpyDeviceToDevice, s));
+    ADJ_CUDA(cudaMemcpyAsync(d_M, masks, sizeof(float) * maskStride * n, cudaMemcpyDeviceToDevice, s));
+    for (int l = 1; l <= maxLevel; ++l) launch_pyr_f(d_pyr + (l - 1) * n, n, lw[l], lh[l], s);
+    ADJ_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int) * (h_sd.size() + 1), s));
+    launch_gabor_save(d_sd, d_tiles, nTiles, nTiles, d_max + h_sd.size(), s);
+    launch_stencil(d_sd, d_sten, nSten, s);
+    ADJ_CUDA(cudaMemsetAsync(d_loss, 0, sizeof(double), s));
+    launch_masked_loss(d_sd, d_sten, nSten, d_loss, s);
+    if (loss) ADJ_CUDA(cudaMemcpyAsync(loss, d_loss, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ADJ_CUDA(cudaGetLastError());
+    return BIMP_OK;
+  }
+
+  int backward(float* grad, size_t pitch, double* gparams, cudaStream_t s) {
+    for (size_t k = 0; k < gcOff.size(); ++k) ADJ_CUDA(cudaMemsetAsync(mem + gcOff[k], 0, gcBytes[k], s));
+    for (int i = 0; i < n; ++i)
+      for (int l = 0; l <= maxLevel; ++l)
+        ADJ_CUDA(cudaMemsetAsync(glvl[i * (maxLevel + 1) + l], 0, sizeof(float) * (size_t)lp[l] * lh[l], s));
+    ADJ_CUDA(cudaMemsetAsync(d_gp, 0, sizeof(double) * 4, s));
+    launch_stencil_bwd(d_sd, d_stenB, nStenB, d_gp, s);
+    launch_wrap_merge(d_sd, d_wrap, nWrap, H, s);
+    launch_gabor_bwd(d_sd, d_tiles, nTiles, nTiles, d_gwin, d_gp, s);
+    for (int l = maxLevel; l >= 1; --l) launch_pyr_f_adj(d_pyrAdj + (l - 1) * n, n, lw[l], lh[l], s);
+    for (int i = 0; i < n; ++i)
+      ADJ_CUDA(cudaMemcpy2DAsync(grad + (size_t)i * H * pitch, sizeof(float) * pitch, glvl[i * (maxLevel + 1)],
+                                 sizeof(float) * lp[0], sizeof(float) * W, H, cudaMemcpyDeviceToDevice, s));
+    if (gparams) ADJ_CUDA(cudaMemcpyAsync(gparams, d_gp, sizeof(double) * 4, cudaMemcpyDeviceToDevice, s));
+    ADJ_CUDA(cudaGetLastError());
+    return BIMP_OK;
+  }
+};
+
+extern "C" {
+
+int bimp_adjoint_create(bimp_adjoint** out, int width, int height, int n_images, const float* lambdas,
+                        int n_lambdas, const bimp_params* params) {
+  if (!out) return afail(BIMP_ERR_INVALID, "out is null");
+  *out = nullptr;
+  if (width < 16 || height < 16 || n_images <= 0 || !lambdas || n_lambdas <= 0)
+    return afail(BIMP_ERR_INVALID, "bad adjoint arguments");
+  if (width > 32767 || height > 32767) return afail(BIMP_ERR_UNSUPPORTED, "image sides above 32767");
+  bimp_params p;
+  bimp_default_params(&p);
+  if (params) p = *params;
+  int dev = 0;
+  ADJ_CUDA(cudaGetDevice(&dev));
+  int rc = configure_device(dev);
+  if (rc != BIMP_OK) return rc;
+  bimp_adjoint* a = new bimp_adjoint();
+  rc = a->build(dev, width, height, n_images, lambdas, n_lambdas, p);
+  if (rc != BIMP_OK) {
+    if (a->mem) cudaFree(a->mem);
+    delete a;
+    return rc;
+  }
+  *out = a;
+  return BIMP_OK;
+}
+
+int bimp_adjoint_destroy(bimp_adjoint* a) {
+  if (!a) return BIMP_OK;
+  cudaSetDevice(a->device);
+  if (a->mem) cudaFree(a->mem);
+  delete a;
+  return BIMP_OK;
+}
+
+int bimp_adjoint_num_scales(const bimp_adjoint* a) { return a ? a->nScales : 0; }
+
+size_t bimp_adjoint_device_bytes(const bimp_adjoint* a) { return a ? a->bytes : 0; }
+
+int bimp_adjoint_mask_layout(const bimp_adjoint* a, int scale, int* data_w, int* data_h, size_t* offset,
+                             size_t* mask_stride) {
+  if (!a || scale < 0 || scale >= a->nScales) return afail(BIMP_ERR_INVALID, "bad scale");
+  if (data_w) *data_w = a->geo[scale].dataW;
+  if (data_h) *data_h = a->geo[scale].dataH;
+  if (offset) *offset = a->maskOff[scale];
+  if (mask_stride) *mask_stride = a->maskStride;
+  return BIMP_OK;
+}
+
+int bimp_adjoint_forward(bimp_adjoint* a, const float* d_images, size_t pitch, const float* d_masks, double* d_loss,
+                         void* stream) {
+  if (!a || !d_images || !d_masks || pitch < (size_t)a->W) return afail(BIMP_ERR_INVALID, "bad forward arguments");
+  ADJ_CUDA(cudaSetDevice(a->device));
+  return a->forward(d_images, pitch, d_masks, d_loss, static_cast<cudaStream_t>(stream));
+}
+
+int bimp_adjoint_backward(bimp_adjoint* a, float* d_grad, size_t pitch, double* d_grad_params, void* stream) {
+  if (!a || !d_grad || pitch < (size_t)a->W) return afail(BIMP_ERR_INVALID, "bad backward arguments");
+  ADJ_CUDA(cudaSetDevice(a->device));
+  return a->backward(d_grad, pitch, d_grad_params, static_cast<cudaStream_t>(stream));
+}
+
+int bimp_adjoint_dense_map(bimp_adjoint* a, int image, int scale, float* d_out, size_t ld, void* stream) {
+  if (!a || !d_out || image < 0 || image >= a->n || scale < 0 || scale >= a->nScales)
+    return afail(BIMP_ERR_INVALID, "bad dense-map arguments");
+  const ScaleDev& d = a->h_sd[(size_t)image * a->nScales + scale];
+  if (ld < (size_t)d.dataW) return afail(BIMP_ERR_INVALID, "ld too small");
+  ADJ_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), d.D, d.dPitch * sizeof(float), d.dataW * sizeof(float),
+                             d.dataH, cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)));
+  return BIMP_OK;
+}
+
+}  // extern "C"

@@ -121,7 +121,7 @@ bool build_scales(int width, int height, const std::vector<float>& lambdas_in,
       }
       for (int m = 0; m < n * n; ++m) ev[m] -= evensum / (fs * fs);   // :330-331
     }
-    tile_spectrum(s, s.spectrum);
+    tile_spectrum(s.even, s.odd, s.kW, s.kX, s.spectrum);
     out.push_back(std::move(s));
   }
   return true;
@@ -134,8 +134,9 @@ bool build_scales(int width, int height, const std::vector<float>& lambdas_in,
 // imaginary part is only the float rounding of the taps and is dropped.
 // Stored at [o][perm128(ky)][perm128(kx)], the digit-permuted order in which
 // the kernel's forward transform leaves the image spectrum.
-void tile_spectrum(const ScaleHost& s, std::vector<float>& out) {
-  const int T = kTile, n = s.kW, h = s.kX;
+void tile_spectrum(const std::vector<float>* even, const std::vector<float>* odd, int kW, int kX,
+                   std::vector<float>& out) {
+  const int T = kTile, n = kW, h = kX;
   std::vector<double> cs(T), sn(T);
   for (int m = 0; m < T; ++m) {
     cs[m] = std::cos(2.0 * M_PI * m / T);
@@ -149,7 +150,7 @@ void tile_spectrum(const ScaleHost& s, std::vector<float>& out) {
       for (int kx = 0; kx < T; ++kx) {
         double re = 0, im = 0;
         for (int col = 0; col < n; ++col) {
-          const double qr = s.even[o][row * n + col], qi = s.odd[o][row * n + col];
+          const double qr = even[o][row * n + col], qi = odd[o][row * n + col];
           const int m = ((kx * (col - h)) % T + T) % T;
           // (qr + i qi)(c - i s)
           re += qr * cs[m] + qi * sn[m];
@@ -169,6 +170,57 @@ void tile_spectrum(const ScaleHost& s, std::vector<float>& out) {
         out[(static_cast<size_t>(o) * T + perm128(ky)) * T + perm128(kx)] =
             static_cast<float>(re / (double(T) * T));
       }
+    }
+  }
+}
+
+// Derivatives of the taps with respect to the wavelength scale alpha
+// (lambda = alpha * lambda_level, sigma = rho * lambda, filtersize =
+// size_ratio * lambda + its frozen odd-size increment) and to rho, at the
+// nominal point alpha = 1, rho = sigma_ratio, from the Gabor formula of
+// bimp/src/cuda_bimp.cu:318-331 in double.  Kernel size and centre stay at
+// the nominal geometry.
+void derivative_taps(const ScaleHost& s, const bimp_params& p, std::vector<float>* de_da, std::vector<float>* do_da,
+                     std::vector<float>* de_dr, std::vector<float>* do_dr) {
+  const int n = s.kW;
+  const double lam = s.lambda, rho = p.sigma_ratio, sig = rho * lam;
+  const double fs = s.filtersize;
+  for (int o = 0; o < kNumOri; ++o) {
+    const double th = static_cast<float>(o * M_PI / kNumOri);
+    const double c = std::cos(th), sn = std::sin(th);
+    std::vector<double> e_raw(n * n), ea(n * n), er(n * n), oa(n * n), orr(n * n);
+    double S = 0, Sa = 0, Sr = 0;
+    for (int row = 0; row < n; ++row) {
+      for (int col = 0; col < n; ++col) {
+        const double x = col - s.kX, y = row - s.kX;
+        const double a = x * c + y * sn, b = y * c - x * sn;
+        const double Q = a * a + p.gamma * b * b;
+        const double env = std::exp(-Q / (2 * sig * sig));
+        const double f = 2 * M_PI * a / lam;
+        const double cf = std::cos(f), sf = std::sin(f);
+        const double e_l = env * sf * (f / lam), o_l = -env * cf * (f / lam);
+        const double env_s = env * Q / (sig * sig * sig);
+        const double e_s = env_s * cf, o_s = env_s * sf;
+        const int k = row * n + col;
+        e_raw[k] = env * cf;
+        ea[k] = lam * e_l + rho * lam * e_s;
+        oa[k] = lam * o_l + rho * lam * o_s;
+        er[k] = lam * e_s;
+        orr[k] = lam * o_s;
+        S += e_raw[k];
+        Sa += ea[k];
+        Sr += er[k];
+      }
+    }
+    de_da[o].resize(n * n);
+    do_da[o].resize(n * n);
+    de_dr[o].resize(n * n);
+    do_dr[o].resize(n * n);
+    for (int k = 0; k < n * n; ++k) {
+      de_da[o][k] = static_cast<float>(ea[k] - Sa / (fs * fs) + 2 * S * p.size_ratio * lam / (fs * fs * fs));
+      do_da[o][k] = static_cast<float>(oa[k]);
+      de_dr[o][k] = static_cast<float>(er[k] - Sr / (fs * fs));
+      do_dr[o][k] = static_cast<float>(orr[k]);
     }
   }
 }

@@ -2,6 +2,8 @@
 // C ABI.  Not part of the public interface.
 #pragma once
 
+#include <vector_types.h>   // float2, int2 (CUDA headers, also for the host compiler)
+
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -56,6 +58,15 @@ struct ScaleDev {
   int rowBase;            // first entry of this scale in the per-row count array
   int image;              // image index inside a batch
   int pattern;            // stencil offsets: 0 = runtime, k > 0 = kOffsetSets[k-1]
+  // differentiable path (float pyramid, saved responses, adjoint buffers)
+  const float* lvlF;      // float level (X scale), lvlPitchF floats per row
+  int lvlPitchF;
+  float2* Z;              // saved e + i o, C layout in float2
+  const float* M;         // loss weights, dataH x dataW (row pitch dataW)
+  float* gC;              // d loss / d complex cell, C layout
+  float* gLvl;            // d loss / d float level, lvlPitchF floats per row
+  const float* dGa;       // real tile spectra of d taps / d alpha, G layout
+  const float* dGr;       // ... / d rho
 };
 
 // Stencil offset sets of the two level wavelengths the default bank uses
@@ -95,10 +106,15 @@ std::vector<float> make_lambdas_log(float start, float end, int spo);
 std::vector<float> make_lambdas_lin(float start, float end, int n);
 bool build_scales(int width, int height, const std::vector<float>& lambdas,
                   const bimp_params& p, std::vector<ScaleHost>& out, std::string& err);
-void tile_spectrum(const ScaleHost& s, std::vector<float>& out);
+void tile_spectrum(const std::vector<float>* even, const std::vector<float>* odd, int kW, int kX,
+                   std::vector<float>& out);
+void derivative_taps(const ScaleHost& s, const bimp_params& p, std::vector<float>* de_da, std::vector<float>* do_da,
+                     std::vector<float>* de_dr, std::vector<float>* do_dr);
 
 // Sets the message returned by bimp_last_error() on the calling thread.
 void record_error(const std::string& msg);
+// Sets the kernels' attributes and constants on device `dev` once.
+int configure_device(int dev);
 
 // Position of natural frequency k in the digit-permuted 128-point layout.
 inline int perm128(int k) { return 8 * (k & 15) + (k >> 4); }

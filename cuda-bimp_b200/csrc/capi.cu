@@ -88,6 +88,10 @@ struct Arena {
 // Lets other translation units report through bimp_last_error().
 void bimp_b200::record_error(const std::string& msg) { g_last_error = msg; }
 
+// Kernel attributes and constants of `dev` (once per device), for other
+// translation units that launch the kernels.
+int bimp_b200::configure_device(int dev) { return ensure_device_configured(dev); }
+
 // ---------------------------------------------------------------------------
 // shared engine: N images with their own sizes, one wavelength bank
 // ---------------------------------------------------------------------------

@@ -2,11 +2,12 @@
 // kernels.cu).
 //
 // One CTA (512 threads, 16 warps) per tile.  The tile's real input window is
-// read from the uint8 pyramid level through the reference's padded-torus index
-// map, transformed once (forward 2D FFT, Hermitian half kept in shared
-// memory), and then for each of the 8 orientations the spectrum is multiplied
-// by that orientation's real Gabor spectrum G_o, inverse transformed as one
-// complex FFT (e + i o) and reduced to |e + i o| on the valid outputs.
+// read from the pyramid level through the reference's padded-torus index map,
+// transformed once (forward 2D FFT, Hermitian half kept in shared memory),
+// and then for each of the 8 orientations the spectrum is multiplied by that
+// orientation's real Gabor spectrum G_o, inverse transformed as one complex
+// FFT (e + i o) and reduced to |e + i o| on the valid outputs.  The
+// differentiable variant also stores e + i o for the adjoint.
 //
 // G_o (64 KB per orientation, L2-resident) is streamed into a double buffer of
 // 16 KB chunks with TMA bulk copies (cp.async.bulk + mbarrier): chunk c + 2 is
@@ -30,6 +31,10 @@ constexpr int kSmemMaps = 2 * kTile * 2;                 // int16 row / column m
 constexpr int kSmemBars = 2 * 8;                         // two mbarriers
 constexpr int kGaborSmem = kSmemW + kSmemXh + kSmemG + kSmemTw + kSmemMaps + kSmemBars;
 static_assert(kGaborSmem <= 232448, "tile kernel exceeds the 227 KB shared-memory limit");
+
+// Float levels hold X (a float image, X = u8/255 for the uint8 content);
+// the uint8 path's value 255*u8/65536 is then (255*255/65536) * X.
+constexpr float kFloatLevelScale = 65025.0f / 65536.0f;
 
 // Work-buffer index of row y, position p: the rotate-by-(p>>4) swizzle inside
 // each group of 8 keeps the stride-8 and contiguous-8 passes conflict-free,
@@ -70,6 +75,102 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
+// Mean-removed pixel value of level row r, column c.  uint8: the
+// reference's 255*u8/65536 (convertTo, cuda_bimp.cu:481) minus 0.5, exactly,
+// as (255*u8 - 32768)/65536.  float: kFloatLevelScale * X - 0.5.
+template <bool FLT>
+__device__ __forceinline__ float level_value(const ScaleDev* sd, int r, int c) {
+  if constexpr (FLT) {
+    return kFloatLevelScale * sd->lvlF[(size_t)r * sd->lvlPitchF + c] - 0.5f;
+  } else {
+    return (1.0f / 65536.0f) * (float)(255 * (int)sd->lvl[(size_t)r * sd->lvlPitch + c] - 32768);
+  }
+}
+
+// Index maps of the tile's input window and its forward 2D FFT.
+// rmap/cmap: window row/col -> level row/col through the padded torus.
+// On return Xh holds the Hermitian half X[py][slot] (py = permuted ky,
+// slot = kx 0..64), including the DC of the removed 0.5 offset.  Uses the
+// first 64 rows of W as scratch.  Ends with a barrier.
+template <bool FLT>
+__device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0, int C0, float2* W, float2* Xh,
+                                                      const float2* tw, short* rmap, short* cmap, int t) {
+  const int kX = sd->kX;
+  if (t < kTile) {
+    rmap[t] = (short)pad_src(pmod(R0 - kX + t, sd->fftH), sd->dataH, kX);
+  } else if (t < 2 * kTile) {
+    const int i = t - kTile;
+    cmap[i] = (short)pad_src(pmod(C0 - kX + i, sd->fftW), sd->dataW, kX);
+  }
+  __syncthreads();
+  // F1: x-dim pass A on packed rows z[r] = in[r] + i in[r+64], r < 64.
+  // Removing the mean keeps the butterflies' intermediate magnitudes, and so
+  // their float rounding, small; the 0.5 offset goes back into the DC bin.
+  {
+    const int r = t >> 3, n1 = t & 7;
+    const int ra = rmap[r], rb = rmap[r + 64];
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int c = cmap[n1 + 8 * m];
+      v[m] = make_float2(level_value<FLT>(sd, ra, c), level_value<FLT>(sd, rb, c));
+    }
+    dft16<false>(v);
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) W[widx(r, n1 + 8 * k2)] = c_mul(v[k2], tw[n1 * 17 + k2]);
+  }
+  __syncthreads();
+  // F2: x-dim pass B
+#pragma unroll
+  for (int it = 0; it < 2; ++it) {
+    const int j = t + it * kTileThreads;
+    const int r = j >> 4, k2 = j & 15;
+    float2 v[8];
+#pragma unroll
+    for (int n1 = 0; n1 < 8; ++n1) v[n1] = W[widx(r, 8 * k2 + n1)];
+    dft8<false>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) W[widx(r, 8 * k2 + k1)] = v[k1];
+  }
+  __syncthreads();
+  // separation of the packed rows into the Hermitian half (kx = 0..64)
+  for (int j = t; j < 64 * kXhCols; j += kTileThreads) {
+    const int r = j / kXhCols, s = j - r * kXhCols;
+    const int kx = s < 64 ? (s >> 2) + 16 * (s & 3) : 64;
+    const int nk = (128 - kx) & 127;
+    const float2 Z = W[widx(r, 8 * (kx & 15) + (kx >> 4))];
+    const float2 Zn = W[widx(r, 8 * (nk & 15) + (nk >> 4))];
+    Xh[r * kXhCols + s] = make_float2(0.5f * (Z.x + Zn.x), 0.5f * (Z.y - Zn.y));
+    Xh[(r + 64) * kXhCols + s] = make_float2(0.5f * (Z.y + Zn.y), 0.5f * (Zn.x - Z.x));
+  }
+  __syncthreads();
+  // F3: y-dim pass A on the 65 half columns
+  for (int j = t; j < 8 * kXhCols; j += kTileThreads) {
+    const int n1 = j / kXhCols, s = j - n1 * kXhCols;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = Xh[(n1 + 8 * m) * kXhCols + s];
+    dft16<false>(v);
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) Xh[(n1 + 8 * k2) * kXhCols + s] = c_mul(v[k2], tw[n1 * 17 + k2]);
+  }
+  __syncthreads();
+  // F4: y-dim pass B -> Xh rows in permuted ky order
+  for (int j = t; j < 16 * kXhCols; j += kTileThreads) {
+    const int k2 = j / kXhCols, s = j - k2 * kXhCols;
+    float2 v[8];
+#pragma unroll
+    for (int n1 = 0; n1 < 8; ++n1) v[n1] = Xh[(8 * k2 + n1) * kXhCols + s];
+    dft8<false>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) Xh[(8 * k2 + k1) * kXhCols + s] = v[k1];
+  }
+  __syncthreads();
+  if (t == 0) Xh[0].x += 0.5f * (float)(kTile * kTile);   // DC of the removed 0.5 offset
+  __syncthreads();
+}
+
+template <bool FLT, bool SAVE_Z>
 __global__ void __launch_bounds__(kTileThreads, 1)
 k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ work, int nwork,
               unsigned int* __restrict__ fault_word) {
@@ -106,8 +207,6 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     const int kX = sd->kX, V = sd->V;
     const int ty = item.tile / sd->tilesX, tx = item.tile - ty * sd->tilesX;
     const int R0 = ty * V, C0 = tx * V;
-    const uint8_t* __restrict__ lvl = sd->lvl;
-    const int lp = sd->lvlPitch;
     const float* __restrict__ G0 = sd->G;
 
     __syncthreads();   // previous tile finished with every buffer
@@ -117,86 +216,11 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
       bulk_load(((gc + 1) & 1) ? gdst1 : gdst0, G0 + kGChunkFloats, kGChunkFloats * 4,
                 ((gc + 1) & 1) ? bar1 : bar0);
     }
-    if (t < kTile) {
-      rmap[t] = (short)pad_src(pmod(R0 - kX + t, sd->fftH), sd->dataH, kX);
-    } else if (t < 2 * kTile) {
-      const int i = t - kTile;
-      cmap[i] = (short)pad_src(pmod(C0 - kX + i, sd->fftW), sd->dataW, kX);
-    }
-    __syncthreads();
-
-    // F1: x-dim pass A on packed rows z[r] = in[r] + i in[r+64], r < 64.
-    // Pixel value 255*u8/65536 (convertTo, cuda_bimp.cu:481) enters as
-    // (255*u8 - 32768)/65536 = value - 0.5, exactly; the 0.5 offset is put
-    // back into the DC bin below.  Removing the mean keeps the butterflies'
-    // intermediate magnitudes, and so their float rounding, small.
-    {
-      const int r = t >> 3, n1 = t & 7;
-      const uint8_t* rowA = lvl + (size_t)rmap[r] * lp;
-      const uint8_t* rowB = lvl + (size_t)rmap[r + 64] * lp;
-      const float s = 1.0f / 65536.0f;
-      float2 v[16];
-#pragma unroll
-      for (int m = 0; m < 16; ++m) {
-        const int c = cmap[n1 + 8 * m];
-        v[m] = make_float2(s * (float)(255 * (int)rowA[c] - 32768), s * (float)(255 * (int)rowB[c] - 32768));
-      }
-      dft16<false>(v);
-#pragma unroll
-      for (int k2 = 0; k2 < 16; ++k2) W[widx(r, n1 + 8 * k2)] = c_mul(v[k2], tw[n1 * 17 + k2]);
-    }
-    __syncthreads();
-    // F2: x-dim pass B
-#pragma unroll
-    for (int it = 0; it < 2; ++it) {
-      const int j = t + it * kTileThreads;
-      const int r = j >> 4, k2 = j & 15;
-      float2 v[8];
-#pragma unroll
-      for (int n1 = 0; n1 < 8; ++n1) v[n1] = W[widx(r, 8 * k2 + n1)];
-      dft8<false>(v);
-#pragma unroll
-      for (int k1 = 0; k1 < 8; ++k1) W[widx(r, 8 * k2 + k1)] = v[k1];
-    }
-    __syncthreads();
-    // separation of the packed rows into the Hermitian half (kx = 0..64)
-    for (int j = t; j < 64 * kXhCols; j += kTileThreads) {
-      const int r = j / kXhCols, s = j - r * kXhCols;
-      const int kx = s < 64 ? (s >> 2) + 16 * (s & 3) : 64;
-      const int nk = (128 - kx) & 127;
-      const float2 Z = W[widx(r, 8 * (kx & 15) + (kx >> 4))];
-      const float2 Zn = W[widx(r, 8 * (nk & 15) + (nk >> 4))];
-      Xh[r * kXhCols + s] = make_float2(0.5f * (Z.x + Zn.x), 0.5f * (Z.y - Zn.y));
-      Xh[(r + 64) * kXhCols + s] = make_float2(0.5f * (Z.y + Zn.y), 0.5f * (Zn.x - Z.x));
-    }
-    __syncthreads();
-    // F3: y-dim pass A on the 65 half columns
-    for (int j = t; j < 8 * kXhCols; j += kTileThreads) {
-      const int n1 = j / kXhCols, s = j - n1 * kXhCols;
-      float2 v[16];
-#pragma unroll
-      for (int m = 0; m < 16; ++m) v[m] = Xh[(n1 + 8 * m) * kXhCols + s];
-      dft16<false>(v);
-#pragma unroll
-      for (int k2 = 0; k2 < 16; ++k2) Xh[(n1 + 8 * k2) * kXhCols + s] = c_mul(v[k2], tw[n1 * 17 + k2]);
-    }
-    __syncthreads();
-    // F4: y-dim pass B -> Xh rows in permuted ky order
-    for (int j = t; j < 16 * kXhCols; j += kTileThreads) {
-      const int k2 = j / kXhCols, s = j - k2 * kXhCols;
-      float2 v[8];
-#pragma unroll
-      for (int n1 = 0; n1 < 8; ++n1) v[n1] = Xh[(8 * k2 + n1) * kXhCols + s];
-      dft8<false>(v);
-#pragma unroll
-      for (int k1 = 0; k1 < 8; ++k1) Xh[(8 * k2 + k1) * kXhCols + s] = v[k1];
-    }
-    __syncthreads();
-    if (t == 0) Xh[0].x += 0.5f * (float)(kTile * kTile);   // DC of the removed 0.5 offset
-    __syncthreads();
+    tile_forward_spectrum<FLT>(sd, R0, C0, W, Xh, tw, rmap, cmap, t);
 
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     float* __restrict__ C0p = sd->C;
+    float2* __restrict__ Z0p = sd->Z;
     const long long cStride = sd->cStride;
     for (int o = 0; o < kNumOri; ++o) {
       float* __restrict__ Cout = C0p + (size_t)o * cStride;
@@ -263,7 +287,10 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
           for (int n2 = 0; n2 < 16; ++n2) {
             const int x = n1 + 8 * n2;
             const int gx = C0 + x - kX;
-            if (x >= kX && x < kX + V && gx < cCols) dst[gx] = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
+            if (x >= kX && x < kX + V && gx < cCols) {
+              dst[gx] = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
+              if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)gy * cPitch + gx] = v[n2];
+            }
           }
         }
       }

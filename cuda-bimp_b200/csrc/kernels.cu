@@ -437,6 +437,8 @@ k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows,
   }
 }
 
+#include "adjoint_kernels.cuh"
+
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
@@ -453,11 +455,12 @@ size_t gabor_smem_bytes() { return kGaborSmem; }
 size_t stencil_smem_bytes() { return sizeof(float) * kNumOri * kStH * kStW; }
 
 cudaError_t configure_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(k_gabor_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)gabor_smem_bytes());
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_stencil, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)stencil_smem_bytes());
+  const cudaFuncAttribute big = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(k_gabor_tiles<false, false>, big, (int)gabor_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles<true, true>, big, (int)gabor_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil, big, (int)stencil_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil_bwd, big, (int)kStencilBwdSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles_bwd, big, (int)kGaborBwdSmem);
   if (e != cudaSuccess) return e;
   return upload_twiddles();
 }
@@ -468,7 +471,33 @@ void launch_pyr(const PyrJob* d_jobs, int njobs, int maxW, int maxH, cudaStream_
 }
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                   cudaStream_t s) {
-  k_gabor_tiles<<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+  k_gabor_tiles<false, false><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+}
+void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
+                       cudaStream_t s) {
+  k_gabor_tiles<true, true><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+}
+void launch_pyr_f(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s) {
+  dim3 b(32, 8), g((maxW + 31) / 32, (maxH + 7) / 8, njobs);
+  k_pyr_down_f<<<g, b, 0, s>>>(d_jobs);
+}
+void launch_pyr_f_adj(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s) {
+  dim3 b(32, 8), g((maxW + 31) / 32, (maxH + 7) / 8, njobs);
+  k_pyr_down_f_adj<<<g, b, 0, s>>>(d_jobs);
+}
+void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, cudaStream_t s) {
+  if (nwork > 0) k_masked_loss<<<nwork, 256, 0, s>>>(d_sd, d_work, d_loss);
+}
+void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_gparams, cudaStream_t s) {
+  if (nwork > 0) k_stencil_bwd<<<nwork, 256, kStencilBwdSmem, s>>>(d_sd, d_work, d_gparams);
+}
+void launch_wrap_merge(const ScaleDev* d_sd, const int* d_entries, int n, int maxRows, cudaStream_t s) {
+  if (n > 0) k_wrap_merge<<<dim3((maxRows + 1 + 255) / 256, n), 256, 0, s>>>(d_sd, d_entries, n);
+}
+void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, float* d_gwin,
+                      double* d_gparams, cudaStream_t s) {
+  if (nwork > 0)
+    k_gabor_tiles_bwd<<<grid, kTileThreads, kGaborBwdSmem, s>>>(d_sd, d_work, nwork, d_gwin, d_gparams);
 }
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
   k_stencil<<<nwork, 256, stencil_smem_bytes(), s>>>(d_sd, d_work);

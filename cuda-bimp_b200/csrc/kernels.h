@@ -16,6 +16,16 @@ struct PyrJob {
   int dw, dh, dp;
 };
 
+// One float pyramid step (same fields; for the transpose, src is the level-l
+// gradient with pitch sp and dst the level-(l-1) gradient with pitch dp, while
+// sw/sh stay the level-(l-1) size and dw/dh the level-l size).
+struct PyrJobF {
+  const float* src;
+  int sw, sh, sp;
+  float* dst;
+  int dw, dh, dp;
+};
+
 // Keypoint destination of one image: 7 x ld float matrix, `capacity` columns.
 struct KpOut {
   float* kp;
@@ -36,5 +46,16 @@ void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStr
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,
                 cudaStream_t s);
+
+// differentiable path and its adjoint
+void launch_pyr_f(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
+void launch_pyr_f_adj(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
+void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
+                       cudaStream_t s);
+void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, cudaStream_t s);
+void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_gparams, cudaStream_t s);
+void launch_wrap_merge(const ScaleDev* d_sd, const int* d_entries, int n, int maxRows, cudaStream_t s);
+void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, float* d_gwin,
+                      double* d_gparams, cudaStream_t s);
 
 }  // namespace bimp_b200

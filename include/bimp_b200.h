@@ -160,6 +160,28 @@ int bimp_dense_map(bimp_context* ctx, int scale, int which, float* d_out,
 int bimp_complex_map(bimp_context* ctx, int scale, int orientation, float* d_out,
                      size_t ld, void* stream);
 
+/* ---- input preprocessing and colour features ------------------------------
+ * getGPUImage size rule, bimp/src/cuda_bimp.cu:156-168: images with fewer
+ * than 350 rows (and >= 350 columns) are scaled by 350/rows, otherwise
+ * images with fewer than 350 columns by 350/cols (float factor, sizes
+ * rounded to nearest).  *scale may be NULL. */
+int bimp_min_size_dims(int width, int height, int* out_w, int* out_h, double* scale);
+
+/* getGPUImage(cv::Mat&, bool grayscale), bimp/src/cuda_bimp.cu:156-180, for
+ * an image already on the device: bilinear upscale to bimp_min_size_dims
+ * (cv::resize INTER_LINEAR, 11-bit weights) and, for 3-channel BGR input with
+ * grayscale != 0, BGR -> grey (cv::cuda::cvtColor COLOR_BGR2GRAY).  d_dst
+ * receives out_w x out_h x (1 or channels) bytes at `dst_pitch`. */
+int bimp_gpu_image(const uint8_t* d_src, size_t src_pitch, int width, int height, int channels,
+                   int grayscale, uint8_t* d_dst, size_t dst_pitch, void* stream);
+
+/* addColorFeatures, bimp/src/cuda_bimp.cu:950-958 (kernel
+ * bimp/include/detection/cuda_bimp.cuh:8-71): the 24-bin colour histogram of
+ * each of the n keypoints in the device 7 x kp_ld matrix, over the BGR
+ * device image, into row i of `d_desc` (row pitch desc_ld floats, 24 used). */
+int bimp_color_features(const float* d_kp, size_t kp_ld, int n, const uint8_t* d_bgr, size_t bgr_pitch,
+                        int width, int height, float* d_desc, size_t desc_ld, void* stream);
+
 /* ---- keypoint extraction without allocation ------------------------------
  * No counterpart in the reference (its extraction, cuda_gpu_keypoints,
  * allocates GpuMats and thrust/NPP temporaries on every call).  For callers

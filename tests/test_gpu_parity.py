@@ -225,3 +225,32 @@ def test_cpp_context_shim_matches_python_api(tmp_path):
     assert np.array_equal(got[:, 0], ref["x"]) and np.array_equal(got[:, 1], ref["y"])
     assert np.array_equal(got[:, 2], ref["size"])
     assert all(int(r[5]) == 1 and float(r[6]) == -1.0 for r in rows)
+
+
+@pytest.mark.parametrize("w,h,cn", [(300, 120, 3), (640, 480, 3), (200, 500, 1), (123, 77, 3)])
+def test_gpu_image_matches_oracle(w, h, cn):
+    import torch
+    rng = np.random.default_rng(w * h)
+    img = rng.integers(0, 256, (h, w, cn) if cn == 3 else (h, w), dtype=np.uint8)
+    for gray in (1, 0):
+        if cn == 1 and gray == 0:
+            continue
+        ref = O.gpu_image(img, grayscale=bool(gray))
+        got = api.gpu_image(img, grayscale=bool(gray))
+        assert got.shape == ref.shape and np.array_equal(got, ref), (w, h, cn, gray)
+
+
+def test_color_features_match_oracle():
+    import torch
+    imgs, lam = synth.workload("vga")
+    gray = imgs[0]
+    rng = np.random.default_rng(9)
+    bgr = np.stack([gray, np.roll(gray, 5, 0), rng.integers(0, 256, gray.shape, dtype=np.uint8)], -1)
+    cs = api.CudaStuff(640, 480, lam)
+    kp = api.getKeypoints(gray, cs, capacity=100000)
+    rec = api.keypoint_matrix_to_records(kp)
+    got = api.color_features(kp, bgr)
+    ref = O.color_features(rec["x"], rec["y"], rec["size"], bgr)
+    assert got.shape == (len(rec), 24)
+    assert np.array_equal(np.isnan(got), np.isnan(ref))
+    assert np.array_equal(np.nan_to_num(got), np.nan_to_num(ref))

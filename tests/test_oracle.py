@@ -148,3 +148,42 @@ def test_golden_fixture():
     tab = O.keypoint_table(res)
     assert np.array_equal(tab["ix"], g["kp_ix"]) and np.array_equal(tab["iy"], g["kp_iy"])
     assert np.array_equal(tab["scale"], g["kp_scale"])
+
+
+def test_min_size_rule():
+    # cuda_bimp.cu:160-168: rows < 350 (cols >= 350) -> 350/rows; else cols < 350 -> 350/cols
+    assert O.min_size_dims(640, 480) == (640, 480, 1.0)
+    w, h, sf = O.min_size_dims(500, 250)
+    assert (w, h) == (700, 350) and sf == float(np.float32(350 / 250))
+    w, h, sf = O.min_size_dims(300, 900)
+    assert (w, h) == (350, 1050)
+    w, h, sf = O.min_size_dims(123, 77)     # cols < 350 branch wins for small images
+    assert w == 350 and sf == float(np.float32(350 / 123))
+
+
+def test_resize_and_gray_against_cv2():
+    cv2 = pytest.importorskip("cv2")
+    rng = np.random.default_rng(2)
+    img = rng.integers(0, 256, (120, 300, 3), dtype=np.uint8)
+    w, h, sf = O.min_size_dims(300, 120)
+    ref = cv2.resize(img, None, fx=sf, fy=sf)
+    mine = O.resize_linear_u8(img, sf, w, h)
+    assert mine.shape == ref.shape
+    d = np.abs(mine.astype(int) - ref)
+    assert d.max() <= 1 and (d > 0).mean() < 0.005      # rounding path differs at ~0.1%
+    # grey: 14-bit weights (CUDA colour conversion) vs cv2's 15-bit CPU weights
+    g = O.bgr_to_gray(img).astype(int)
+    gc = cv2.cvtColor(img, cv2.COLOR_BGR2GRAY).astype(int)
+    assert np.abs(g - gc).max() <= 1 and (g != gc).mean() < 0.01
+
+
+def test_color_features_quirks():
+    bgr = np.zeros((20, 20, 3), np.uint8)
+    bgr[..., 0] = 10      # bin 0 of B
+    bgr[..., 1] = 100     # bin 3 of G
+    bgr[..., 2] = 200     # signed char -56: counted nowhere
+    f = O.color_features([10.0], [10.0], [16.0], bgr)[0]   # p = 2: 4x4 window, 48 samples
+    assert f[0] == pytest.approx(0.5 * 16 / 48) and f[8 + 3] == pytest.approx(0.5 * 16 / 48)
+    assert f[16:].sum() == 0 and f[1:8].sum() == 0
+    bgr[..., 0] = 0       # open interval: 0 is not in (0, 31.875)
+    assert O.color_features([10.0], [10.0], [16.0], bgr)[0][:8].sum() == 0
