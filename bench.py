@@ -16,11 +16,15 @@ keypoints out.  Metric: Mpixel/s of full-resolution input pixels.
               with CUDA events, algorithmic bytes per launch / duration;
 * ``batched`` 64 mixed-size images (<= 1080p) in one CUDA-graph replay vs
               the same images detected one by one;
-* ``cpu_baseline`` the FP64 oracle on one 1080p image (rank 0, N=1).
+* ``adjoint``  forward and backward of sum(M * D) on 16 float 512x512 images
+              (6 scales): bwd/fwd time ratio and the gradient against the
+              FP64 CPU reference on one image;
+* ``cpu_baseline`` the FP32 C restatement of the reference pipeline (own
+              FFT, OpenMP) on three 1080p images (rank 0, N=1).
 
-``--impl reference`` times the reference pipeline's CPU restatement (the
-oracle port; the reference itself cannot be built here) on this host's cores
-and prints the same metric with "impl": "reference".
+``--impl reference`` times the reference pipeline's FP32 C restatement
+(oracle/cbimp.c; the reference itself cannot be built here) on all of this
+host's cores and prints the same metric with "impl": "reference".
 
 Multi-GPU (torchrun): one process per GPU, each detecting its own images
 (replicas; the path has no exchange step), value = all pixels / max time.
@@ -336,16 +340,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             c2.close()
         bt.close()
 
+    # -- adjoint: 16 x 512x512 float images, 6 scales, fwd vs bwd ----------
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = run_adjoint_bench(args, rank, world, dev, stream, max_ms)
+
     # -- CPU baseline (rank 0, N=1) -----------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        from oracle import bimp_oracle as O
-        t0 = time.perf_counter()
-        O.run(pool_np[0], lam, keep_maps=False)
-        dt = time.perf_counter() - t0
-        cpu = {"value": round(W_HD * H_HD / dt / 1e6, 4), "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": "one 1920x1080 image, 8 scales x 8 orientations, FP64 numpy oracle, 1 thread",
-               "seconds": round(dt, 2)}
+        cpu = cpu_port_baseline(pool_np, lam, images=3)
 
     if rank == 0:
         line = {
@@ -359,11 +362,78 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                      "rotated per step; each step also streams ~200 MB of maps",
                        "keypoints_last_step": n_kp, "parallelism": f"replicas x{world}"},
             "roofline": roofline, "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
-            "cpu_baseline": cpu, "e2e": e2e, "batched": batched,
+            "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "adjoint": adjoint,
             "gpu_launches": cs_launches(cs) * args.steps, "clocks": clk,
         }
         print(json.dumps(line), flush=True)
     cs.close()
+
+
+def run_adjoint_bench(args, rank, world, dev, stream, max_ms):
+    """Forward (loss) and backward (image + 4 parameter gradients) of the
+    summed keypoint maps on 16 float 512x512 images, 6 scales; bwd/fwd time
+    ratio, Mpixel/s of the training step, and (rank 0, N=1) the gradient of
+    image 0 against the FP64 CPU reference and a finite difference."""
+    import torch
+    from bimp_b200 import api, synth
+    imgs, lam = synth.workload("adjoint", seed_base=1000 + 13 * rank)
+    n, h, w = len(imgs), imgs[0].shape[0], imgs[0].shape[1]
+    x = torch.from_numpy(np.stack(imgs)).to(dev).contiguous()
+    adj = api.Adjoint(w, h, n, lam)
+    rng = np.random.default_rng(99 + rank)
+    masks = torch.from_numpy(rng.standard_normal(n * adj.mask_stride).astype(np.float32)).to(dev)
+    for _ in range(3):
+        adj.forward(x, masks)
+        adj.backward()
+    torch.cuda.synchronize()
+    k = max(5, min(50, args.steps // 20))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd_ms = bwd_ms = 0.0
+    for _ in range(k):
+        ev[0].record(stream)
+        adj.forward(x, masks)
+        ev[1].record(stream)
+        adj.backward()
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        fwd_ms += ev[0].elapsed_time(ev[1])
+        bwd_ms += ev[1].elapsed_time(ev[2])
+    fwd_ms = max_ms(fwd_ms / k)
+    bwd_ms = max_ms(bwd_ms / k)
+    out = {"workload": "16 float 512x512 images, 6 scales x 8 orientations, L = sum(M * D), "
+                       "grads wrt image, lambda scale, sigma ratio, w_tan, w_rad",
+           "fwd_ms": round(fwd_ms, 3), "bwd_ms": round(bwd_ms, 3), "bwd_fwd_ratio": round(bwd_ms / fwd_ms, 3),
+           "train_step_mpixel_s": round(world * n * w * h / ((fwd_ms + bwd_ms) * 1e-3) / 1e6, 1),
+           "device_bytes": adj.device_bytes()}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        # image 0 against the FP64 CPU reference gradient: branch-matched (the
+        # reference takes its ReLU states and magnitude floor from the
+        # device's float32 complex cells) and on its own FP64 branch
+        from oracle import bimp_adjoint as A
+        one = api.Adjoint(w, h, 1, lam)
+        m1 = masks[:adj.mask_stride].contiguous()
+        one.forward(x[:1].contiguous(), m1)
+        g1, gp1 = one.backward()
+        g0 = g1[0].cpu().numpy()
+        gp1 = gp1.cpu().numpy().copy()
+        mv = [m.cpu().numpy().astype(np.float64) for m in one.mask_views(m1)[0]]
+        dec = [np.stack([one.complex_map(0, s, o).cpu().numpy() for o in range(8)]) for s in range(len(one.layout))]
+        x64 = imgs[0].astype(np.float64)
+        _, ref_g, ref_p = A.gradient(x64, lam, mv, decide=dec)
+        _, free_g, free_p = A.gradient(x64, lam, mv)
+        names = ("alpha", "rho", "w_tan", "w_rad")
+        out["grad_rel_err_image0"] = float(np.linalg.norm(g0 - ref_g) / np.linalg.norm(ref_g))
+        out["param_rel_err_image0"] = [float(abs(gp1[k] - ref_p[nm]) / abs(ref_p[nm])) for k, nm in enumerate(names)]
+        out["grad_rel_err_image0_fp64_branch"] = float(np.linalg.norm(g0 - free_g) / np.linalg.norm(free_g))
+        # central finite difference of the FP64 loss along one seeded
+        # direction, step 1e-4: kink-limited on this piecewise-linear loss
+        v = np.random.default_rng(11).standard_normal(x64.shape)
+        hh = 1e-4
+        fd = (A.loss(x64 + hh * v, lam, mv) - A.loss(x64 - hh * v, lam, mv)) / (2 * hh)
+        out["fd_step_1e-4_rel_diff_image0"] = float(abs(fd - float((g0 * v).sum())) / abs(fd))
+        one.close()
+    adj.close()
+    return out
 
 
 def cs_launches(cs) -> int:
@@ -374,44 +444,58 @@ def cs_launches(cs) -> int:
 # ---------------------------------------------------------------------------
 # reference arm: the CPU restatement of the reference pipeline
 # ---------------------------------------------------------------------------
-def _ref_scale(args):
-    img, lam, i = args
-    from oracle import bimp_oracle as O
-    sc = O.scale_geometry(img.shape[1], img.shape[0], lam)[i]
-    data = O.level_image(img, sc)
-    Ct, _, _ = O.complex_cells(data, sc)
-    maps = O.keypoint_maps(O.stencil_window(Ct, sc), sc)
-    kp = O.extract_keypoints(maps["D"], sc, i)
-    return len(kp.ix)
+def cpu_port_baseline(images_np, lam, images: int, warmup: int = 1) -> dict:
+    """The FP32 C restatement of the reference pipeline (oracle/cbimp.c, own
+    FFT, OpenMP over every host thread) on `images` 1080p images."""
+    from oracle.cbimp import CBimp, max_threads
+    with CBimp(W_HD, H_HD, lam) as cb:
+        for i in range(warmup):
+            cb.detect(images_np[i % len(images_np)])
+        times = []
+        for i in range(images):
+            t0 = time.perf_counter()
+            cb.detect(images_np[(warmup + i) % len(images_np)])
+            times.append(time.perf_counter() - t0)
+    dt = sum(times)
+    return {"value": round(images * W_HD * H_HD / dt / 1e6, 4), "unit": UNIT, "cores": max_threads(),
+            "kind": "port",
+            "sample": f"{images} 1920x1080 images after {warmup} warm-up, 8 scales x 8 orientations; FP32 C "
+                      "restatement of the reference pipeline (whole-torus FFT filtering, own mixed-radix FFT, "
+                      "OpenMP over all host threads)",
+            "seconds": round(dt, 3), "median_s_per_image": round(statistics.median(times), 4)}
 
 
 def run_reference(args, rank: int, world: int):
+    """The reference's pipeline on the host cores: the reference itself needs
+    OpenCV-CUDA 3.x, Boost, CUDA-samples headers and texture references
+    (removed in CUDA 12), so its FP32 C restatement stands in for it."""
     if rank != 0:
         return
-    import multiprocessing as mp
     from bimp_b200 import synth
+    from oracle.cbimp import CBimp, max_threads
     lam = synth.bank(8)
     pool_np = hd_pool(0, 8)
-    cores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(min(cores, len(lam))) as pool:
-        def step(img):
-            return sum(pool.map(_ref_scale, [(img, lam, i) for i in range(len(lam))]))
+    with CBimp(W_HD, H_HD, lam) as cb:
         for i in range(args.warmup):
-            step(pool_np[i % 8])
+            cb.detect(pool_np[i % 8])
         t0 = time.perf_counter()
+        n_kp = 0
         for i in range(args.steps):
-            step(pool_np[i % 8])
+            n_kp = cb.detect(pool_np[i % 8])[1]
         dt = time.perf_counter() - t0
     value = args.steps * W_HD * H_HD / dt / 1e6
+    cores = max_threads()
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 2),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "plain BIMP, one 1920x1080 uint8 image per step", "scales": 8,
-                       "orientations": 8},
-            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": min(cores, len(lam)), "kind": "port",
-                             "sample": "whole 1080p image per step; scales in parallel processes (FP64 oracle port; "
-                                       "the reference itself needs OpenCV-CUDA and cannot be built here)"},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "plain BIMP, one 1920x1080 uint8 image per step (1/f^2 noise + 150 polygons)",
+                       "scales": 8, "orientations": 8, "lambdas": [round(x, 6) for x in lam],
+                       "keypoints_last_step": n_kp},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} whole 1080p images after {args.warmup} warm-up; FP32 C "
+                                       "restatement of the reference pipeline, OpenMP over all host threads "
+                                       "(the reference needs OpenCV-CUDA 3.x and CUDA<=11 texture references "
+                                       "and cannot be built here)"},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -425,6 +509,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="only the forward/backward measurement of the adjoint workload (1 GPU)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -432,9 +519,18 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.adjoint_only:
+        import torch
+        torch.cuda.set_device(local_rank)
+        out = run_adjoint_bench(args, 0, 1, torch.device("cuda", local_rank), torch.cuda.current_stream(),
+                                lambda v: float(v))
+        print(json.dumps({"adjoint": out}), flush=True)
+        return
     if args.impl == "reference":
-        if args.steps > 30:
-            args.steps = 30     # keep the CPU run within a few minutes
+        # each step is a whole 1080p image on the CPU (~1 s): keep the run
+        # within a few minutes
+        args.steps = min(args.steps, 30)
+        args.warmup = min(args.warmup, 3)
         run_reference(args, rank, world)
         return
     if world > 1:

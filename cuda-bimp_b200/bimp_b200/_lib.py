@@ -96,6 +96,8 @@ _PROTOS = [
     ("bimp_adjoint_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bimp_adjoint_backward", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
     ("bimp_adjoint_dense_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
+    ("bimp_adjoint_complex_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t,
+                                           C.c_void_p]),
     ("bimp_adjoint_device_bytes", C.c_size_t, [C.c_void_p]),
     ("bimp_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int,
                                     C.POINTER(C.c_float), C.c_int, C.POINTER(Params), C.c_int]),

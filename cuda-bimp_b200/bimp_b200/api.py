@@ -446,6 +446,15 @@ class Adjoint:
                                                _stream_ptr()), "adjoint_dense_map")
         return out
 
+    def complex_map(self, image: int, scale: int, orientation: int):
+        """|e + i o| of the last forward over the stencil window, (h+1, w+1)."""
+        torch = _torch()
+        off, w, h = self.layout[scale]
+        out = torch.empty((h + 1, w + 1), dtype=torch.float32, device="cuda")
+        L.check(L.lib().bimp_adjoint_complex_map(self._h, image, scale, orientation, C.c_void_p(out.data_ptr()),
+                                                 out.stride(0), _stream_ptr()), "adjoint_complex_map")
+        return out
+
     def device_bytes(self) -> int:
         return int(L.lib().bimp_adjoint_device_bytes(self._h))
 

@@ -10,7 +10,7 @@ Workloads (sizes and banks follow the detector's published configurations):
 * ``hd``       one 1920x1080 image, 150 polygons, 8 scales (4*2^(k/2))
 * ``mixed``    64 images, W in [320,1920], H in [240,1080] (multiples of 16),
                about 7 polygons per 100k pixels, 8 scales
-* ``adjoint``  16 float images 512x512 in [0,1], 6 scales
+* ``adjoint``  16 float 512x512 images (the uint8 content / 255), 6 scales
 * ``uhd``      32 correlated 3840x2160 frames (subpixel shifts <= 2 px plus
                N(0,2) noise), 12 scales
 """
@@ -93,6 +93,13 @@ def bank(n_scales: int) -> list[float]:
 VGA_LAMBDAS = [4.0, 8.0, 16.0, 32.0]
 
 
+def dequantised(img_u8: np.ndarray, seed: int) -> np.ndarray:
+    """float32 (u8 + U(-0.5, 0.5)) / 255: the same picture without exactly
+    flat regions."""
+    rng = np.random.default_rng(seed)
+    return ((img_u8.astype(np.float64) + rng.uniform(-0.5, 0.5, img_u8.shape)) / 255.0).astype(np.float32)
+
+
 def workload(name: str, seed_base: int = 1000):
     """Return (images, lambdas) for a named workload."""
     if name == "vga":
@@ -109,7 +116,7 @@ def workload(name: str, seed_base: int = 1000):
             imgs.append(synth_image(w, h, npoly, seed_base + 100 + i))
         return imgs, bank(8)
     if name == "adjoint":
-        imgs = [synth_image(512, 512, 20, seed_base + 300 + i).astype(np.float32) / 255.0
+        imgs = [synth_image(512, 512, 20, seed_base + 300 + i).astype(np.float32) / np.float32(255.0)
                 for i in range(16)]
         return imgs, bank(6)
     if name == "uhd":

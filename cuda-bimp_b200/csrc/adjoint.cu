@@ -37,8 +37,27 @@ int rha(double v) { return static_cast<int>(v >= 0 ? std::floor(v + 0.5) : -std:
 
 }  // namespace
 
+// Coefficients of the tile backward for one orientation, gathered into the
+// Hermitian half layout of the tile spectra (entry j = py * kXhCols + slot,
+// slot -> kx as in the forward transform's separation step):
+//   A[j] = {G(k), G(-k), dGa(k), dGr(k)},  B[j] = {dGa(-k), dGr(-k)},
+// with B = 0 where -k lies in k's own column (kx = 0 or 64), so that the
+// backward's dot products visit every frequency once.
+void gather_half(const float* G, const float* dA, const float* dR, float4* A, float2* B) {
+  for (int j = 0; j < kSpecHalf; ++j) {
+    const int py = j / kXhCols, sl = j - py * kXhCols;
+    const int kx = sl < 64 ? (sl >> 2) + 16 * (sl & 3) : 64;
+    const int ky = 16 * (py & 7) + (py >> 3);
+    const int i1 = py * kTile + perm128(kx);
+    const int i2 = perm128((kTile - ky) & 127) * kTile + perm128((kTile - kx) & 127);
+    A[j] = make_float4(G[i1], G[i2], dA[i1], dR[i1]);
+    const bool self = kx == 0 || kx == 64;
+    B[j] = make_float2(self ? 0.f : dA[i2], self ? 0.f : dR[i2]);
+  }
+}
+
 struct bimp_adjoint {
-  int device = 0, W = 0, H = 0, n = 0, nScales = 0, maxLevel = 0;
+  int device = 0, W = 0, H = 0, n = 0, nScales = 0, maxLevel = 0, maxSide = 0;
   bimp_params params{};
   std::vector<ScaleHost> geo;
   char* mem = nullptr;
@@ -47,24 +66,24 @@ struct bimp_adjoint {
   ScaleDev* d_sd = nullptr;
   TileWork* d_tiles = nullptr;
   int nTiles = 0;
-  int2* d_sten = nullptr;
+  int2* d_sten = nullptr;                 // forward stencil blocks (data)
   int nSten = 0;
-  int2* d_stenB = nullptr;
+  int2* d_stenB = nullptr;                // backward gather blocks (window, data + 1)
   int nStenB = 0;
-  int* d_wrap = nullptr;
-  int nWrap = 0;
-  std::vector<float*> lvl, glvl;          // per image per level
+  std::vector<float*> lvl, glvl;          // [level][image]
   std::vector<int> lw, lh, lp;            // per level (same for all images)
+  float* d_lvl0 = nullptr;                // level 0 of every image, n * H rows of lp[0]
+  float* d_glvl = nullptr;                // every level gradient, one block
+  size_t glvlBytes = 0;
   PyrJobF* d_pyr = nullptr;               // [level-1][image] forward jobs
   PyrJobF* d_pyrAdj = nullptr;            // [level-1][image] transpose jobs
   float* d_M = nullptr;
   size_t maskStride = 0;
   std::vector<size_t> maskOff;
-  float* d_gwin = nullptr;
-  double* d_loss = nullptr;
+  float2* d_xsave = nullptr;              // per work item: the tile image spectrum of the last forward
+  double* d_loss = nullptr;               // [0] loss, [1..4] parameter gradients
   double* d_gp = nullptr;
-  unsigned int* d_max = nullptr;           // per entry + fault word
-  std::vector<size_t> gcOff, gcBytes;
+  unsigned int* d_max = nullptr;          // per entry + fault word
 
   int build(int dev, int w, int h, int ni, const float* lambdas, int nl, const bimp_params& p) {
     device = dev;
@@ -76,19 +95,26 @@ struct bimp_adjoint {
     if (!build_scales(w, h, std::vector<float>(lambdas, lambdas + nl), p, geo, err)) return afail(BIMP_ERR_INVALID, err);
     nScales = static_cast<int>(geo.size());
     for (auto& s : geo) maxLevel = std::max(maxLevel, s.level);
-    // derivative spectra
-    std::vector<std::vector<float>> dga(nScales), dgr(nScales);
+    maxSide = std::max(w, h);
+    // backward coefficients: G and the derivative spectra, gathered
+    std::vector<float4> hA((size_t)nScales * kNumOri * kSpecHalf);
+    std::vector<float2> hB((size_t)nScales * kNumOri * kSpecHalf);
     for (int s = 0; s < nScales; ++s) {
-      std::vector<float> ea[kNumOri], oa[kNumOri], er[kNumOri], orr[kNumOri];
+      std::vector<float> ea[kNumOri], oa[kNumOri], er[kNumOri], orr[kNumOri], dga, dgr;
       derivative_taps(geo[s], p, ea, oa, er, orr);
-      tile_spectrum(ea, oa, geo[s].kW, geo[s].kX, dga[s]);
-      tile_spectrum(er, orr, geo[s].kW, geo[s].kX, dgr[s]);
+      tile_spectrum(ea, oa, geo[s].kW, geo[s].kX, dga);
+      tile_spectrum(er, orr, geo[s].kW, geo[s].kX, dgr);
+      for (int o = 0; o < kNumOri; ++o) {
+        const size_t so = (size_t)o * kSpecFloats, ho = ((size_t)s * kNumOri + o) * kSpecHalf;
+        gather_half(geo[s].spectrum.data() + so, dga.data() + so, dgr.data() + so, hA.data() + ho, hB.data() + ho);
+      }
     }
     // ---- layout
     size_t at = 0;
     auto take = [&](size_t b) { const size_t o = up(at, 256); at = o + b; return o; };
     const size_t specB = sizeof(float) * (size_t)kNumOri * kSpecFloats;
-    const size_t offG = take(specB * nScales), offGa = take(specB * nScales), offGr = take(specB * nScales);
+    const size_t offG = take(specB * nScales);
+    const size_t offBA = take(sizeof(float4) * hA.size()), offBB = take(sizeof(float2) * hB.size());
     int cw = w, ch = h;
     for (int l = 0; l <= maxLevel; ++l) {
       if (l > 0) { cw = (cw + 1) / 2; ch = (ch + 1) / 2; }
@@ -96,12 +122,14 @@ struct bimp_adjoint {
       lh.push_back(ch);
       lp.push_back(static_cast<int>(up(cw, 32)));
     }
-    std::vector<size_t> offL, offGL;
-    for (int i = 0; i < n; ++i)
-      for (int l = 0; l <= maxLevel; ++l) {
-        offL.push_back(take(sizeof(float) * (size_t)lp[l] * lh[l]));
-        offGL.push_back(take(sizeof(float) * (size_t)lp[l] * lh[l]));
-      }
+    // levels grouped by level so that level 0 of all images is one block;
+    // the level gradients form one block (cleared by one memset)
+    std::vector<size_t> offL, offGL;   // one block of n images per level
+    for (int l = 0; l <= maxLevel; ++l) offL.push_back(take(sizeof(float) * (size_t)n * lp[l] * lh[l]));
+    at = up(at, 256);
+    const size_t glBegin = at;
+    for (int l = 0; l <= maxLevel; ++l) offGL.push_back(take(sizeof(float) * (size_t)n * lp[l] * lh[l]));
+    glvlBytes = at - glBegin;
     maskStride = 0;
     for (auto& s : geo) {
       maskOff.push_back(maskStride);
@@ -110,9 +138,8 @@ struct bimp_adjoint {
     const size_t offM = take(sizeof(float) * maskStride * n);
     std::vector<TileWork> tiles;
     std::vector<int2> sten, stenB;
-    std::vector<int> wraps;
     std::vector<ScaleDev> sds;
-    std::vector<size_t> offC, offZ, offD, offS, offGC;
+    std::vector<size_t> offC, offZ, offD, offT, offR, offBits, offGC;
     for (int i = 0; i < n; ++i) {
       for (int si = 0; si < nScales; ++si) {
         const ScaleHost& s = geo[si];
@@ -160,27 +187,27 @@ struct bimp_adjoint {
         for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
         const int nbx2 = (s.dataW + 1 + 31) / 32, nby2 = (s.dataH + 1 + 31) / 32;
         for (int b = 0; b < nbx2 * nby2; ++b) stenB.push_back(make_int2(entry, b));
-        if (d.wrapW) wraps.push_back(entry);
+        const size_t mapB = sizeof(float) * (size_t)s.dataH * d.dPitch;
         offC.push_back(take(sizeof(float) * (size_t)kNumOri * d.cStride));
         offZ.push_back(take(sizeof(float2) * (size_t)kNumOri * d.cStride));
         offGC.push_back(take(sizeof(float) * (size_t)kNumOri * d.cStride));
-        offD.push_back(take(sizeof(float) * (size_t)s.dataH * d.dPitch));
-        offS.push_back(take(sizeof(float) * (size_t)s.dataH * d.dPitch));
+        offD.push_back(take(mapB));
+        offT.push_back(take(mapB));
+        offR.push_back(take(mapB));
+        offBits.push_back(take(mapB));
         sds.push_back(d);
       }
     }
     nTiles = static_cast<int>(tiles.size());
     nSten = static_cast<int>(sten.size());
     nStenB = static_cast<int>(stenB.size());
-    nWrap = static_cast<int>(wraps.size());
     const size_t offSd = take(sizeof(ScaleDev) * sds.size());
-    const size_t offT = take(sizeof(TileWork) * tiles.size());
+    const size_t offT2 = take(sizeof(TileWork) * tiles.size());
     const size_t offSt = take(sizeof(int2) * sten.size());
     const size_t offStB = take(sizeof(int2) * stenB.size());
-    const size_t offWr = take(sizeof(int) * std::max<size_t>(1, wraps.size()));
     const size_t offPyr = take(sizeof(PyrJobF) * std::max(1, maxLevel * n));
     const size_t offPyrA = take(sizeof(PyrJobF) * std::max(1, maxLevel * n));
-    const size_t offWin = take(sizeof(float) * (size_t)nTiles * kTile * kTile);
+    const size_t offXs = take(sizeof(float2) * (size_t)nTiles * kSpecHalf);
     const size_t offLoss = take(sizeof(double) * 8);
     const size_t offMax = take(sizeof(unsigned int) * (sds.size() + 1));
     bytes = at;
@@ -191,71 +218,70 @@ struct bimp_adjoint {
     }
     char* b = mem;
     float* dG = reinterpret_cast<float*>(b + offG);
-    float* dGa = reinterpret_cast<float*>(b + offGa);
-    float* dGr = reinterpret_cast<float*>(b + offGr);
-    for (int i = 0; i < n; ++i)
-      for (int l = 0; l <= maxLevel; ++l) {
-        lvl.push_back(reinterpret_cast<float*>(b + offL[i * (maxLevel + 1) + l]));
-        glvl.push_back(reinterpret_cast<float*>(b + offGL[i * (maxLevel + 1) + l]));
+    float4* dBA = reinterpret_cast<float4*>(b + offBA);
+    float2* dBB = reinterpret_cast<float2*>(b + offBB);
+    for (int l = 0; l <= maxLevel; ++l)
+      for (int i = 0; i < n; ++i) {
+        const size_t img = sizeof(float) * (size_t)i * lp[l] * lh[l];
+        lvl.push_back(reinterpret_cast<float*>(b + offL[l] + img));
+        glvl.push_back(reinterpret_cast<float*>(b + offGL[l] + img));
       }
+    d_lvl0 = lvl[0];
+    d_glvl = glvl[0];
     d_M = reinterpret_cast<float*>(b + offM);
     d_max = reinterpret_cast<unsigned int*>(b + offMax);
     for (size_t e2 = 0; e2 < sds.size(); ++e2) {
       ScaleDev& d = sds[e2];
       const int i = d.image, si = static_cast<int>(e2 % nScales);
       const ScaleHost& s = geo[si];
-      d.lvlF = lvl[i * (maxLevel + 1) + s.level];
-      d.gLvl = glvl[i * (maxLevel + 1) + s.level];
+      d.lvlF = lvl[(size_t)s.level * n + i];
+      d.gLvl = glvl[(size_t)s.level * n + i];
       d.G = dG + (size_t)si * kNumOri * kSpecFloats;
-      d.dGa = dGa + (size_t)si * kNumOri * kSpecFloats;
-      d.dGr = dGr + (size_t)si * kNumOri * kSpecFloats;
+      d.bwA = dBA + (size_t)si * kNumOri * kSpecHalf;
+      d.bwB = dBB + (size_t)si * kNumOri * kSpecHalf;
       d.C = reinterpret_cast<float*>(b + offC[e2]);
       d.Z = reinterpret_cast<float2*>(b + offZ[e2]);
       d.gC = reinterpret_cast<float*>(b + offGC[e2]);
       d.D = reinterpret_cast<float*>(b + offD[e2]);
-      d.S = reinterpret_cast<float*>(b + offS[e2]);
+      d.T = reinterpret_cast<float*>(b + offT[e2]);
+      d.R = reinterpret_cast<float*>(b + offR[e2]);
+      d.bits = reinterpret_cast<unsigned int*>(b + offBits[e2]);
       d.M = d_M + (size_t)i * maskStride + maskOff[si];
       d.maxKey = d_max + e2;
-      gcOff.push_back(offGC[e2]);
-      gcBytes.push_back(sizeof(float) * (size_t)kNumOri * d.cStride);
     }
     h_sd = sds;
     d_sd = reinterpret_cast<ScaleDev*>(b + offSd);
-    d_tiles = reinterpret_cast<TileWork*>(b + offT);
+    d_tiles = reinterpret_cast<TileWork*>(b + offT2);
     d_sten = reinterpret_cast<int2*>(b + offSt);
     d_stenB = reinterpret_cast<int2*>(b + offStB);
-    d_wrap = reinterpret_cast<int*>(b + offWr);
     d_pyr = reinterpret_cast<PyrJobF*>(b + offPyr);
     d_pyrAdj = reinterpret_cast<PyrJobF*>(b + offPyrA);
-    d_gwin = reinterpret_cast<float*>(b + offWin);
+    d_xsave = reinterpret_cast<float2*>(b + offXs);
     d_loss = reinterpret_cast<double*>(b + offLoss);
     d_gp = d_loss + 1;
     // uploads
-    for (int si = 0; si < nScales; ++si) {
+    for (int si = 0; si < nScales; ++si)
       ADJ_CUDA(cudaMemcpy(dG + (size_t)si * kNumOri * kSpecFloats, geo[si].spectrum.data(), specB,
                           cudaMemcpyHostToDevice));
-      ADJ_CUDA(cudaMemcpy(dGa + (size_t)si * kNumOri * kSpecFloats, dga[si].data(), specB, cudaMemcpyHostToDevice));
-      ADJ_CUDA(cudaMemcpy(dGr + (size_t)si * kNumOri * kSpecFloats, dgr[si].data(), specB, cudaMemcpyHostToDevice));
-    }
+    ADJ_CUDA(cudaMemcpy(dBA, hA.data(), sizeof(float4) * hA.size(), cudaMemcpyHostToDevice));
+    ADJ_CUDA(cudaMemcpy(dBB, hB.data(), sizeof(float2) * hB.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(d_sd, sds.data(), sizeof(ScaleDev) * sds.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(d_tiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(d_sten, sten.data(), sizeof(int2) * sten.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(d_stenB, stenB.data(), sizeof(int2) * stenB.size(), cudaMemcpyHostToDevice));
-    if (!wraps.empty())
-      ADJ_CUDA(cudaMemcpy(d_wrap, wraps.data(), sizeof(int) * wraps.size(), cudaMemcpyHostToDevice));
     std::vector<PyrJobF> fj, aj;
     for (int l = 1; l <= maxLevel; ++l)
       for (int i = 0; i < n; ++i) {
         PyrJobF j;
-        j.src = lvl[i * (maxLevel + 1) + l - 1];
+        j.src = lvl[(size_t)(l - 1) * n + i];
         j.sw = lw[l - 1]; j.sh = lh[l - 1]; j.sp = lp[l - 1];
-        j.dst = lvl[i * (maxLevel + 1) + l];
+        j.dst = lvl[(size_t)l * n + i];
         j.dw = lw[l]; j.dh = lh[l]; j.dp = lp[l];
         fj.push_back(j);
         PyrJobF a = j;   // transpose: read level l gradient, scatter into level l-1
-        a.src = glvl[i * (maxLevel + 1) + l];
+        a.src = glvl[(size_t)l * n + i];
         a.sp = lp[l];
-        a.dst = glvl[i * (maxLevel + 1) + l - 1];
+        a.dst = glvl[(size_t)(l - 1) * n + i];
         a.dp = lp[l - 1];
         aj.push_back(a);
       }
@@ -267,34 +293,32 @@ struct bimp_adjoint {
   }
 
   int forward(const float* imgs, size_t pitch, const float* masks, double* loss, cudaStream_t s) {
-    for (int i = 0; i < n; ++i)
-      ADJ_CUDA(cudaMemcpy2DAsync(lvl[i * (maxLevel + 1)], sizeof(float) * lp[0], imgs + (size_t)i * H * pitch,
-                                 sizeof(float) * pitch, sizeof(float) * W, H, cudaMemcpyDeviceToDevice, s));
+    // the n images as one block of n * H rows
+    ADJ_CUDA(cudaMemcpy2DAsync(d_lvl0, sizeof(float) * lp[0], imgs, sizeof(float) * pitch, sizeof(float) * W,
+                               (size_t)n * H, cudaMemcpyDeviceToDevice, s));
     ADJ_CUDA(cudaMemcpyAsync(d_M, masks, sizeof(float) * maskStride * n, cudaMemcpyDeviceToDevice, s));
     for (int l = 1; l <= maxLevel; ++l) launch_pyr_f(d_pyr + (l - 1) * n, n, lw[l], lh[l], s);
     ADJ_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int) * (h_sd.size() + 1), s));
-    launch_gabor_save(d_sd, d_tiles, nTiles, nTiles, d_max + h_sd.size(), s);
-    launch_stencil(d_sd, d_sten, nSten, s);
-    ADJ_CUDA(cudaMemsetAsync(d_loss, 0, sizeof(double), s));
-    launch_masked_loss(d_sd, d_sten, nSten, d_loss, s);
+    ADJ_CUDA(cudaMemsetAsync(d_loss, 0, sizeof(double) * 5, s));
+    launch_gabor_save(d_sd, d_tiles, nTiles, nTiles, d_max + h_sd.size(), d_xsave, s);
+    launch_stencil_adj(d_sd, d_sten, nSten, s);
+    launch_masked_loss(d_sd, d_sten, nSten, d_loss, d_gp, s);
     if (loss) ADJ_CUDA(cudaMemcpyAsync(loss, d_loss, sizeof(double), cudaMemcpyDeviceToDevice, s));
     ADJ_CUDA(cudaGetLastError());
     return BIMP_OK;
   }
 
+  // dL/dw_tan and dL/dw_rad (d_gp[2..3]) come from the forward's masked
+  // sums; the backward accumulates alpha and rho and the image gradient.
   int backward(float* grad, size_t pitch, double* gparams, cudaStream_t s) {
-    for (size_t k = 0; k < gcOff.size(); ++k) ADJ_CUDA(cudaMemsetAsync(mem + gcOff[k], 0, gcBytes[k], s));
-    for (int i = 0; i < n; ++i)
-      for (int l = 0; l <= maxLevel; ++l)
-        ADJ_CUDA(cudaMemsetAsync(glvl[i * (maxLevel + 1) + l], 0, sizeof(float) * (size_t)lp[l] * lh[l], s));
-    ADJ_CUDA(cudaMemsetAsync(d_gp, 0, sizeof(double) * 4, s));
-    launch_stencil_bwd(d_sd, d_stenB, nStenB, d_gp, s);
-    launch_wrap_merge(d_sd, d_wrap, nWrap, H, s);
-    launch_gabor_bwd(d_sd, d_tiles, nTiles, nTiles, d_gwin, d_gp, s);
+    ADJ_CUDA(cudaMemsetAsync(d_glvl, 0, glvlBytes, s));
+    ADJ_CUDA(cudaMemsetAsync(d_gp, 0, sizeof(double) * 2, s));
+    launch_stencil_bwd(d_sd, d_stenB, nStenB, s);
+    launch_gc_finish(d_sd, static_cast<int>(h_sd.size()), maxSide, s);
+    launch_gabor_bwd(d_sd, d_tiles, nTiles, nTiles, d_xsave, d_gp, s);
     for (int l = maxLevel; l >= 1; --l) launch_pyr_f_adj(d_pyrAdj + (l - 1) * n, n, lw[l], lh[l], s);
-    for (int i = 0; i < n; ++i)
-      ADJ_CUDA(cudaMemcpy2DAsync(grad + (size_t)i * H * pitch, sizeof(float) * pitch, glvl[i * (maxLevel + 1)],
-                                 sizeof(float) * lp[0], sizeof(float) * W, H, cudaMemcpyDeviceToDevice, s));
+    ADJ_CUDA(cudaMemcpy2DAsync(grad, sizeof(float) * pitch, d_glvl, sizeof(float) * lp[0], sizeof(float) * W,
+                               (size_t)n * H, cudaMemcpyDeviceToDevice, s));
     if (gparams) ADJ_CUDA(cudaMemcpyAsync(gparams, d_gp, sizeof(double) * 4, cudaMemcpyDeviceToDevice, s));
     ADJ_CUDA(cudaGetLastError());
     return BIMP_OK;
@@ -370,6 +394,23 @@ int bimp_adjoint_dense_map(bimp_adjoint* a, int image, int scale, float* d_out, 
   if (ld < (size_t)d.dataW) return afail(BIMP_ERR_INVALID, "ld too small");
   ADJ_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), d.D, d.dPitch * sizeof(float), d.dataW * sizeof(float),
                              d.dataH, cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)));
+  return BIMP_OK;
+}
+
+int bimp_adjoint_complex_map(bimp_adjoint* a, int image, int scale, int orientation, float* d_out, size_t ld,
+                             void* stream) {
+  if (!a || !d_out || image < 0 || image >= a->n || scale < 0 || scale >= a->nScales || orientation < 0 ||
+      orientation >= kNumOri)
+    return afail(BIMP_ERR_INVALID, "bad complex-map arguments");
+  const ScaleDev& d = a->h_sd[(size_t)image * a->nScales + scale];
+  if (ld < (size_t)d.cCols) return afail(BIMP_ERR_INVALID, "ld smaller than data width + 1");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float* src = d.C + (size_t)orientation * d.cStride;
+  ADJ_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), src, d.cPitch * sizeof(float), d.cCols * sizeof(float),
+                             d.dataH + 1, cudaMemcpyDeviceToDevice, s));
+  if (d.wrapW)   // column dataW of the window is the torus element (r + 1, 0)
+    ADJ_CUDA(cudaMemcpy2DAsync(d_out + d.dataW, ld * sizeof(float), src + d.cPitch, d.cPitch * sizeof(float),
+                               sizeof(float), d.dataH + 1, cudaMemcpyDeviceToDevice, s));
   return BIMP_OK;
 }
 

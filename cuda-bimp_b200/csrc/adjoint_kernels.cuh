@@ -3,14 +3,18 @@
 //
 //   k_pyr_down_f        float pyramid level (pyrDown without uint8 rounding)
 //   k_pyr_down_f_adj    its transpose (scatter-add of the 5x5 taps)
-//   k_masked_loss       sum M * D, T and R terms are handled in k_stencil_bwd
-//   k_stencil_bwd       gather form of d L / d C over the stencil window
-//   k_wrap_merge        column dataW of the window is torus (r+1, 0) when
-//                       fftW == dataW: its gradient moves there
-//   k_gabor_tiles_bwd   per tile: image spectrum X, then per orientation
-//                       a = dL/dC * z/|z|, A = FFT(a), alpha/rho dot products
-//                       sum dG * Re(conj(A) X), and Re IFFT(A G) into the
-//                       window gradient; finally scattered to the level
+//   k_masked_loss       sum M * D (the loss) and the w_tan / w_rad gradients
+//   k_stencil_bwd       gather form of d L / d C over the stencil window from
+//                       the ReLU states the forward stencil recorded
+//   k_gc_finish         zero window row dataH + 1; when fftW == dataW, column
+//                       dataW of the window is torus (r+1, 0): its gradient
+//                       moves there
+//   k_gabor_tiles_bwd   per tile and orientation a = dL/dC * z/|z|, A = FFT(a),
+//                       alpha/rho dot products sum dG Re(conj(A) X) with the
+//                       image spectrum X the forward saved, and the sum of
+//                       A G in the frequency domain; one inverse transform
+//                       per tile gives the window gradient, scattered to
+//                       the level
 #pragma once
 
 __global__ void k_pyr_down_f(const PyrJobF* __restrict__ jobs) {
@@ -69,39 +73,47 @@ __device__ __forceinline__ void block_add_double(double v, double* dst) {
   }
 }
 
-// sum over the 32x32 block of M * D (work list of the forward stencil).
+// Over the 32x32 block: sum M * D into loss[0], and -sum M * T, -sum M * R
+// (dL/dw_tan and dL/dw_rad: D = D0 - w_tan T - w_rad R) into gparams[2..3].
 __global__ void __launch_bounds__(256) k_masked_loss(const ScaleDev* __restrict__ sds, const int2* __restrict__ work,
-                                                     double* __restrict__ loss) {
+                                                     double* __restrict__ loss, double* __restrict__ gparams) {
   const int2 item = work[blockIdx.x];
   const ScaleDev* sd = sds + item.x;
   const int W = sd->dataW, H = sd->dataH;
   const int nbx = (W + kStX - 1) / kStX;
   const int by = item.y / nbx, bx = item.y - by * nbx;
-  double acc = 0.0;
+  double acc = 0.0, accT = 0.0, accR = 0.0;
   const int x = bx * kStX + (threadIdx.x & 31);
   for (int i = threadIdx.x >> 5; i < kStY; i += 8) {
     const int y = by * kStY + i;
-    if (x < W && y < H) acc += (double)sd->M[(size_t)y * W + x] * (double)sd->D[(size_t)y * sd->dPitch + x];
+    if (x < W && y < H) {
+      const double m = sd->M[(size_t)y * W + x];
+      const size_t k = (size_t)y * sd->dPitch + x;
+      acc += m * (double)sd->D[k];
+      accT += m * (double)sd->T[k];
+      accR += m * (double)sd->R[k];
+    }
   }
   block_add_double(acc, loss);
+  block_add_double(-accT, gparams + 2);
+  block_add_double(-accR, gparams + 3);
 }
 
 // --- stencil backward ------------------------------------------------------
-constexpr int kBwHalo = 16;                    // C staged +-16 around the block
-constexpr int kBwCW = kStX + 2 * kBwHalo;      // 64
-constexpr int kBwQW = kStX + 2 * kHalo;        // 48: source pixels +-8
-constexpr size_t kStencilBwdSmem = sizeof(float) * (size_t)kNumOri * kBwCW * kBwCW;   // 128 KB
+constexpr int kBwQW = kStX + 2 * kHalo;        // 48: source pixels +-8 around the block
+constexpr int kStBwThreads = 256;
 
-// Per source pixel q and orientation o, the ReLU states the forward took:
-// bit 4o: double-stopped d > 0, 4o+1: tangential t > 0, 4o+2: radial r > 0,
-// 4o+3: first radial term r1 > 0; each gated by the orientation's bounds test.
-__global__ void __launch_bounds__(256, 1)
-k_stencil_bwd(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, double* __restrict__ gparams) {
-  extern __shared__ float4 s_raw4[];
-  float* sC = reinterpret_cast<float*>(s_raw4);                  // [8][64][64]
-  __shared__ float sM[kBwQW * kBwQW];                            // loss weights +-8
+// Gather form of dL/dC_o(p) for a 32x32 block of window positions p
+// (0 <= p <= (dataH, dataW)): every source pixel q whose stencils read p
+// contributes its loss weight M(q) times the ReLU state the forward recorded
+// at q (ScaleDev::bits).  Sources lie within +-8 of p.  The tangential and
+// radial weights are constants here; their own gradients come from
+// k_masked_loss.
+__global__ void __launch_bounds__(kStBwThreads)
+k_stencil_bwd(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
+  __shared__ float sM[kBwQW * kBwQW];
   __shared__ unsigned int sBits[kBwQW * kBwQW];
-  __shared__ StencilPar P;
+  __shared__ int sOff[kNumOri][6];
   const int2 item = work[blockIdx.x];
   const ScaleDev* __restrict__ sd = sds + item.x;
   const int W = sd->dataW, H = sd->dataH;
@@ -111,148 +123,118 @@ k_stencil_bwd(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, d
   const int t = threadIdx.x;
   const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
   if (t < kNumOri) {
-    const int o = t;
-    const int e1 = sd->es1[o], e2 = sd->es2[o], i1 = sd->in1[o], i2 = sd->in2[o];
-    P.e1[o] = e1; P.e2[o] = e2; P.i1[o] = i1; P.i2[o] = i2;
-    P.h1[o] = sd->ih1[o]; P.h2[o] = sd->ih2[o];
-    P.exlo[o] = 2 * abs(e2); P.exhi[o] = W - 2 * abs(e2);
-    P.eylo[o] = 2 * abs(e1); P.eyhi[o] = H - 2 * abs(e1);
-    P.ixlo[o] = 2 * abs(i2); P.ixhi[o] = W - 2 * abs(i2);
-    P.iylo[o] = 2 * abs(i1); P.iyhi[o] = H - 2 * abs(i1);
+    sOff[t][0] = sd->es1[t]; sOff[t][1] = sd->es2[t];
+    sOff[t][2] = sd->in1[t]; sOff[t][3] = sd->in2[t];
+    sOff[t][4] = sd->ih1[t]; sOff[t][5] = sd->ih2[t];
   }
-  // stage C over rows y0-16 .. y0+47 and cols x0-16 .. x0+47 (window reads)
-  const float* __restrict__ C = sd->C;
-  const int cPitch = sd->cPitch;
-  const long long cStride = sd->cStride;
-  for (int idx = t; idx < kNumOri * kBwCW * kBwCW; idx += 256) {
-    const int row = idx / kBwCW, lx = idx - row * kBwCW;
-    const int o = row / kBwCW, ly = row - o * kBwCW;
-    const int gy = y0 - kBwHalo + ly, gx = x0 - kBwHalo + lx;
-    float v = 0.f;
-    if (gy >= 0 && gy <= H && gx >= 0 && gx <= W) {
-      int ry = gy, rx = gx;
-      if (sd->wrapW && gx == W) { rx = 0; ry = gy + 1; }
-      v = C[(size_t)o * cStride + (size_t)ry * cPitch + rx];
-    }
-    sC[idx] = v;
-  }
-  for (int idx = t; idx < kBwQW * kBwQW; idx += 256) {
+  const int dp = sd->dPitch;
+  for (int idx = t; idx < kBwQW * kBwQW; idx += kStBwThreads) {
     const int ly = idx / kBwQW, lx = idx - ly * kBwQW;
     const int gy = y0 - kHalo + ly, gx = x0 - kHalo + lx;
-    sM[idx] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? sd->M[(size_t)gy * W + gx] : 0.f;
+    const bool in = gy >= 0 && gy < H && gx >= 0 && gx < W;
+    sM[idx] = in ? sd->M[(size_t)gy * W + gx] : 0.f;
+    sBits[idx] = in ? sd->bits[(size_t)gy * dp + gx] : 0u;
   }
   __syncthreads();
-  // phase 1: ReLU states of every source pixel q within +-8 of the block,
-  // and sum M*T, M*R over the block's own pixels
-  double accT = 0.0, accR = 0.0;
-  for (int idx = t; idx < kBwQW * kBwQW; idx += 256) {
-    const int qy = idx / kBwQW, qx = idx - qy * kBwQW;
-    const int y = y0 - kHalo + qy, x = x0 - kHalo + qx;
-    unsigned int bits = 0;
-    if (y >= 0 && y < H && x >= 0 && x < W) {
-      const int cy = qy + (kBwHalo - kHalo), cx = qx + (kBwHalo - kHalo);
-      float T = 0.f, R = 0.f;
-#pragma unroll
-      for (int o = 0; o < kNumOri; ++o) {
-        const float* c = sC + (o * kBwCW + cy) * kBwCW + cx;
-        if (x >= P.exlo[o] && x <= P.exhi[o] && y >= P.eylo[o] && y <= P.eyhi[o]) {
-          const int o1 = P.e1[o], o2 = P.e2[o];
-          const float d = fmaf(-0.5f, c[2 * o1 * kBwCW - 2 * o2], fmaf(-0.5f, c[-2 * o1 * kBwCW + 2 * o2], c[0]));
-          if (d > 0.f) bits |= 1u << (4 * o);
-        }
-        if (x >= P.ixlo[o] && x <= P.ixhi[o] && y >= P.iylo[o] && y <= P.iyhi[o]) {
-          const int i1 = P.i1[o], i2 = P.i2[o], h1 = P.h1[o], h2 = P.h2[o];
-          const float* cp = sC + (((o + 4) & 7) * kBwCW + cy) * kBwCW + cx;
-          const float centre = c[0];
-          const float tt = c[-i1 * kBwCW - i2] - centre;
-          if (tt > 0.f) { bits |= 1u << (4 * o + 1); T += tt; }
-          const float r1 = centre - gain * cp[h1 * kBwCW + h2];
-          const float r = (r1 > 0.f ? r1 : 0.f) + centre - gain * cp[-h1 * kBwCW - h2];
-          if (r > 0.f) { bits |= 1u << (4 * o + 2); R += r; }
-          if (r1 > 0.f) bits |= 1u << (4 * o + 3);
-        }
-      }
-      if (qy >= kHalo && qy < kHalo + kStY && qx >= kHalo && qx < kHalo + kStX) {
-        accT += (double)sM[idx] * T;
-        accR += (double)sM[idx] * R;
-      }
-    }
-    sBits[idx] = bits;
-  }
-  __syncthreads();
-  // phase 2: gather d L / d C_o(p) for the block's window positions p
   float* __restrict__ gC = sd->gC;
+  const int cPitch = sd->cPitch;
+  const long long cStride = sd->cStride;
   const int lx = t & 31;
-  for (int ly = t >> 5; ly < kStY; ly += 8) {
+  for (int ly = t >> 5; ly < kStY; ly += kStBwThreads / 32) {
     const int py = y0 + ly, px = x0 + lx;
     if (py > H || px > W) continue;
     const int qy = ly + kHalo, qx = lx + kHalo;   // p in source-pixel coordinates
+    auto at = [&](int dy, int dx) { return (qy + dy) * kBwQW + (qx + dx); };
+    const unsigned int b0 = sBits[at(0, 0)];
+    const float m0 = sM[at(0, 0)];
 #pragma unroll
     for (int o = 0; o < kNumOri; ++o) {
-      const int o1 = P.e1[o], o2 = P.e2[o], i1 = P.i1[o], i2 = P.i2[o];
-      const int op = (o + 4) & 7;
-      const int ph1 = P.h1[op], ph2 = P.h2[op];
-      auto at = [&](int dy, int dx) { return (qy + dy) * kBwQW + (qx + dx); };
+      const int op = (o + kNumOri / 2) % kNumOri;
+      const int o1 = sOff[o][0], o2 = sOff[o][1], i1 = sOff[o][2], i2 = sOff[o][3];
+      const int ph1 = sOff[op][4], ph2 = sOff[op][5];
+      const unsigned int bd = 1u << (4 * o), bt = 2u << (4 * o), br = 4u << (4 * o), br1 = 8u << (4 * o);
+      const unsigned int pr = 4u << (4 * op), pr1 = 8u << (4 * op);
       float g = 0.f;
-      // double-stopped: centre, and the two -1/2 taps
+      // double-stopped: p is the centre of q = p, and a -1/2 tap of q = p +- 2 offset
+      if (b0 & bd) g += m0;
       {
-        const int k0 = at(0, 0), ka = at(2 * o1, -2 * o2), kb = at(-2 * o1, 2 * o2);
-        if (sBits[k0] & (1u << (4 * o))) g += sM[k0];
-        if (sBits[ka] & (1u << (4 * o))) g -= 0.5f * sM[ka];
-        if (sBits[kb] & (1u << (4 * o))) g -= 0.5f * sM[kb];
+        const int ka = at(2 * o1, -2 * o2), kb = at(-2 * o1, 2 * o2);
+        if (sBits[ka] & bd) g -= 0.5f * sM[ka];
+        if (sBits[kb] & bd) g -= 0.5f * sM[kb];
       }
       // tangential: p is read by q = p + i (as C(q - i)) and by q = p (centre)
       {
-        const int kq = at(i1, i2), k0 = at(0, 0);
-        if (sBits[kq] & (1u << (4 * o + 1))) g += -wT * sM[kq];
-        if (sBits[k0] & (1u << (4 * o + 1))) g -= -wT * sM[k0];
+        const int kq = at(i1, i2);
+        if (sBits[kq] & bt) g -= wT * sM[kq];
+        if (b0 & bt) g += wT * m0;
       }
-      // radial, o as the centre orientation
-      {
-        const int k0 = at(0, 0);
-        const unsigned int b = sBits[k0];
-        if (b & (1u << (4 * o + 2))) g += -wR * sM[k0] * ((b & (1u << (4 * o + 3))) ? 2.f : 1.f);
-      }
+      // radial, o as the centre orientation (both terms when r1 > 0)
+      if (b0 & br) g -= wR * m0 * ((b0 & br1) ? 2.f : 1.f);
       // radial, o as the perpendicular map of op: read at q + h (r1) and q - h (r)
       {
         const int k1 = at(-ph1, -ph2), k2 = at(ph1, ph2);
         const unsigned int b1 = sBits[k1], b2 = sBits[k2];
-        if ((b1 & (1u << (4 * op + 2))) && (b1 & (1u << (4 * op + 3)))) g -= gain * (-wR * sM[k1]);
-        if (b2 & (1u << (4 * op + 2))) g -= gain * (-wR * sM[k2]);
+        if ((b1 & pr) && (b1 & pr1)) g += gain * wR * sM[k1];
+        if (b2 & pr) g += gain * wR * sM[k2];
       }
       gC[(size_t)o * cStride + (size_t)py * cPitch + px] = g;
     }
   }
-  block_add_double(-(double)wT * accT, gparams + 2);
-  block_add_double(-(double)wR * accR, gparams + 3);
 }
 
-// fftW == dataW: the stencils read column dataW of row r from (r+1, 0).
-__global__ void k_wrap_merge(const ScaleDev* __restrict__ sds, const int* __restrict__ entries, int n) {
-  const int e = entries[blockIdx.y];
-  const ScaleDev* sd = sds + e;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r > sd->dataH) return;
+// After k_stencil_bwd, per entry: row dataH + 1 of the window gradient (read
+// by the tile backward, written by no stencil) starts at zero, and when
+// fftW == dataW the gradient of window column dataW of row r moves to
+// (r + 1, 0), the torus element the stencils actually read there.
+__global__ void k_gc_finish(const ScaleDev* __restrict__ sds) {
+  const ScaleDev* sd = sds + blockIdx.y;
+  const int W = sd->dataW, H = sd->dataH;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   for (int o = 0; o < kNumOri; ++o) {
     float* g = sd->gC + (size_t)o * sd->cStride;
-    const float v = g[(size_t)r * sd->cPitch + sd->dataW];
-    g[(size_t)r * sd->cPitch + sd->dataW] = 0.f;
-    g[(size_t)(r + 1) * sd->cPitch] += v;
+    if (i <= W && !(sd->wrapW && i == 0)) g[(size_t)(H + 1) * sd->cPitch + i] = 0.f;
+    if (sd->wrapW && i <= H) {
+      const float v = g[(size_t)i * sd->cPitch + W];
+      g[(size_t)i * sd->cPitch + W] = 0.f;
+      if (i < H) g[(size_t)(i + 1) * sd->cPitch] += v;
+      else g[(size_t)(H + 1) * sd->cPitch] = v;
+    }
   }
 }
 
 // --- tile backward -----------------------------------------------------------
-constexpr int kGaborBwdSmem = kSmemW + kSmemXh + kSmemTw + kSmemMaps;
+// |e + i o| at or below kMagFloor counts as zero: no gradient flows through
+// the magnitude there (the minimal-norm subgradient of |z| at 0).  Exactly
+// flat image regions give |e + i o| = 0 up to rounding (the float taps'
+// residual DC in FP64, FFT rounding of about 1e-6 of the map peak in FP32),
+// where z / |z| is the direction of rounding noise.  The floor is an
+// absolute value for images on the [0, 1] scale.
+constexpr float kMagFloor = 3.0e-5f;
+constexpr int kSmemBh = kSmemXh;   // Hermitian half of the accumulated spectrum
+constexpr int kGaborBwdSmem = kSmemW + kSmemBh + kSmemTw + kSmemMaps;
+static_assert(kGaborBwdSmem <= 232448, "tile backward exceeds the 227 KB shared-memory limit");
 
+// Position of natural frequency k in the digit-permuted order of the 8x16
+// transforms (the order of G and of the saved spectra).
+__device__ __forceinline__ int perm128d(int k) { return 8 * (k & 15) + (k >> 4); }
+
+// One CTA per tile.  The window gradient is linear in the per-orientation
+// spectra, Re IFFT(sum_o A_o G_o), so the products are summed in the
+// frequency domain (Hermitian half, Bh) and ONE inverse transform per tile
+// replaces one per orientation.  Per orientation: a = dL/dC * z/|z| on the
+// valid outputs, A = FFT(a), the alpha/rho dot products sum dG Re(conj(A) X)
+// against the image spectrum X the forward saved (Hermitian half), and
+// Bh += (A G + conj(A G)(-k))/2.  The per-orientation coefficients G(+-k),
+// dGa, dGr come pre-gathered in the half layout (ScaleDev::bwA, bwB).
 __global__ void __launch_bounds__(kTileThreads, 1)
 k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ work, int nwork,
-                  float* __restrict__ gwin, double* __restrict__ gparams) {
+                  const float2* __restrict__ xsave, double* __restrict__ gparams) {
   extern __shared__ float4 smem4b[];
   char* base = reinterpret_cast<char*>(smem4b);
   float2* W = reinterpret_cast<float2*>(base);
-  float2* Xh = reinterpret_cast<float2*>(base + kSmemW);
-  float2* tw = reinterpret_cast<float2*>(base + kSmemW + kSmemXh);
-  short* rmap = reinterpret_cast<short*>(base + kSmemW + kSmemXh + kSmemTw);
+  float2* Bh = reinterpret_cast<float2*>(base + kSmemW);
+  float2* tw = reinterpret_cast<float2*>(base + kSmemW + kSmemBh);
+  short* rmap = reinterpret_cast<short*>(base + kSmemW + kSmemBh + kSmemTw);
   short* cmap = rmap + kTile;
   const int t = threadIdx.x;
   if (t < 8 * 17) {
@@ -266,30 +248,49 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
     const int kX = sd->kX, V = sd->V;
     const int ty = item.tile / sd->tilesX, tx = item.tile - ty * sd->tilesX;
     const int R0 = ty * V, C0 = tx * V;
-    float* __restrict__ acc = gwin + (size_t)w * kTile * kTile;
-    __syncthreads();
-    tile_forward_spectrum<true>(sd, R0, C0, W, Xh, tw, rmap, cmap, t);
+    const float2* __restrict__ Xs = xsave + (size_t)w * kSpecHalf;   // Hermitian half of X
+    __syncthreads();   // previous tile finished with every buffer
+    if (t < kTile) {
+      rmap[t] = (short)pad_src(pmod(R0 - kX + t, sd->fftH), sd->dataH, kX);
+    } else if (t < 2 * kTile) {
+      const int i = t - kTile;
+      cmap[i] = (short)pad_src(pmod(C0 - kX + i, sd->fftW), sd->dataW, kX);
+    }
+    for (int j = t; j < kTile * kXhCols; j += kTileThreads) Bh[j] = make_float2(0.f, 0.f);
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     const long long cStride = sd->cStride;
     for (int o = 0; o < kNumOri; ++o) {
-      // a = dL/dC * z / |z| on the valid outputs, zero elsewhere
-      for (int j = t; j < kTile * kTile; j += kTileThreads) {
-        const int y = j >> 7, x = j & 127;
-        float2 a = make_float2(0.f, 0.f);
-        const int gy = R0 + y - kX, gx = C0 + x - kX;
-        if (y >= kX && y < kX + V && x >= kX && x < kX + V && gy < cRows && gx < cCols) {
-          const size_t k = (size_t)o * cStride + (size_t)gy * cPitch + gx;
-          const float2 z = sd->Z[k];
-          const float m = sqrtf(z.x * z.x + z.y * z.y);
-          if (m > 0.f) {
-            const float s = sd->gC[k] / m;
-            a = make_float2(s * z.x, s * z.y);
-          }
+      // a = dL/dC * z / |z| on the valid outputs, zero elsewhere; four
+      // pixels per thread with their loads issued together
+#pragma unroll 1
+      for (int j0 = t; j0 < kTile * kTile; j0 += 4 * kTileThreads) {
+        float m[4], gc[4];
+        float2 z[4];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = j0 + u * kTileThreads;
+          const int y = j >> 7, x = j & 127;
+          const int gy = R0 + y - kX, gx = C0 + x - kX;
+          ok[u] = y >= kX && y < kX + V && x >= kX && x < kX + V && gy < cRows && gx < cCols;
+          const size_t k = ok[u] ? (size_t)o * cStride + (size_t)gy * cPitch + gx : 0;
+          m[u] = ok[u] ? __ldg(sd->C + k) : 0.f;
+          gc[u] = ok[u] ? __ldg(sd->gC + k) : 0.f;
+          z[u] = ok[u] ? __ldg(sd->Z + k) : make_float2(0.f, 0.f);
         }
-        W[widx(y, x)] = a;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = j0 + u * kTileThreads;
+          float2 a = make_float2(0.f, 0.f);
+          if (ok[u] && m[u] > kMagFloor) {
+            const float sc = gc[u] / m[u];
+            a = make_float2(sc * z[u].x, sc * z[u].y);
+          }
+          W[widx(j >> 7, j & 127)] = a;
+        }
       }
       __syncthreads();
-      // forward FFT of a: x-dim on the valid rows (others are zero), then y-dim
+      // forward FFT of a: x-dim on the valid rows (the others are zero), then y-dim
       for (int j = t; j < V * 8; j += kTileThreads) {
         const int y = kX + (j >> 3), n1 = j & 7;
         float2 v[16];
@@ -334,86 +335,92 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
         for (int k1 = 0; k1 < 8; ++k1) W[widx(8 * k2 + k1, p)] = v[k1];
       }
       __syncthreads();
-      // parameter dot products and the product A * G, at permuted (py, p)
+      // Hermitian accumulation and the parameter dot products.  Entry j of
+      // the half layout holds k = (ky, kx), kx in [0, 64]; its partner -k
+      // covers the columns 65..127, so every frequency enters the dot
+      // products once (columns 0 and 64 pair with themselves: their -k
+      // coefficients are 0).  X is Hermitian, X(-k) = conj(X(k)).
       {
-        const float* G = sd->G + (size_t)o * kSpecFloats;
-        const float* dA = sd->dGa + (size_t)o * kSpecFloats;
-        const float* dR = sd->dGr + (size_t)o * kSpecFloats;
+        const float4* __restrict__ cA = sd->bwA + (size_t)o * kSpecHalf;
+        const float2* __restrict__ cB = sd->bwB + (size_t)o * kSpecHalf;
         float sa = 0.f, sr = 0.f;
-        for (int j = t; j < kTile * kTile; j += kTileThreads) {
-          const int py = j >> 7, p = j & 127;
-          const int k = widx(py, p);
-          const float2 A = W[k];
-          const float2 X = spectrum_at(Xh, py, p);
-          const float re = A.x * X.x + A.y * X.y;     // Re(conj(A) X)
-          sa = fmaf(__ldg(dA + j), re, sa);
-          sr = fmaf(__ldg(dR + j), re, sr);
-          W[k] = c_scale(A, __ldg(G + j));
+        for (int j = t; j < kSpecHalf; j += kTileThreads) {
+          const float4 c4 = __ldg(cA + j);   // G(k), G(-k), dGa(k), dGr(k)
+          const float2 c2 = __ldg(cB + j);   // dGa(-k), dGr(-k)
+          const float2 X = __ldg(Xs + j);
+          const int py = j / kXhCols, sl = j - py * kXhCols;
+          const int kx = sl < 64 ? (sl >> 2) + 16 * (sl & 3) : 64;
+          const int ky = 16 * (py & 7) + (py >> 3);
+          const int p = perm128d(kx);
+          const int np = perm128d((kTile - kx) & 127), npy = perm128d((kTile - ky) & 127);
+          const float2 A1 = W[widx(py, p)], A2 = W[widx(npy, np)];
+          const float2 b = Bh[j];
+          Bh[j] = make_float2(fmaf(0.5f * c4.x, A1.x, fmaf(0.5f * c4.y, A2.x, b.x)),
+                              fmaf(0.5f * c4.x, A1.y, fmaf(-0.5f * c4.y, A2.y, b.y)));
+          const float re1 = A1.x * X.x + A1.y * X.y;   // Re(conj(A(k)) X(k))
+          const float re2 = A2.x * X.x - A2.y * X.y;   // Re(conj(A(-k)) conj(X(k)))
+          sa = fmaf(c4.z, re1, fmaf(c2.x, re2, sa));
+          sr = fmaf(c4.w, re1, fmaf(c2.y, re2, sr));
         }
         accA += sa;
         accR += sr;
       }
       __syncthreads();
-      // inverse FFT of A * G over the whole window; Re -> window gradient
-#pragma unroll
-      for (int it = 0; it < 4; ++it) {
-        const int j = t + it * kTileThreads;
-        const int p = j & 127, k2 = j >> 7;
-        float2 v[8];
-#pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(8 * k2 + k1, p)];
-        dft8<true>(v);
-#pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, p)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
-      }
-      __syncthreads();
-#pragma unroll
-      for (int it = 0; it < 2; ++it) {
-        const int j = t + it * kTileThreads;
-        const int p = j & 127, n1 = j >> 7;
-        float2 v[16];
-#pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(8 * k2 + n1, p)];
-        dft16<true>(v);
-#pragma unroll
-        for (int n2 = 0; n2 < 16; ++n2) W[widx(n1 + 8 * n2, p)] = v[n2];
-      }
-      __syncthreads();
-#pragma unroll
-      for (int it = 0; it < 4; ++it) {
-        const int j = t + it * kTileThreads;
-        const int y = j >> 4, k2 = j & 15;
-        float2 v[8];
-#pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
-        dft8<true>(v);
-#pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
-      }
-      __syncthreads();
-#pragma unroll
-      for (int it = 0; it < 2; ++it) {
-        const int j = t + it * kTileThreads;
-        const int y = j >> 3, n1 = j & 7;
-        float2 v[16];
-#pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(y, 8 * k2 + n1)];
-        dft16<true>(v);
-#pragma unroll
-        for (int n2 = 0; n2 < 16; ++n2) {
-          float* dst = acc + y * kTile + n1 + 8 * n2;
-          *dst = o == 0 ? v[n2].x : *dst + v[n2].x;
-        }
-      }
-      __syncthreads();
     }
-    // window gradient -> float level, through the padded-torus index maps
+    // one inverse transform of the Hermitian sum: Re -> window gradient,
+    // scattered to the float level through the padded-torus index maps
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int j = t + it * kTileThreads;
+      const int p = j & 127, k2 = j >> 7;
+      float2 v[8];
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) v[k1] = spectrum_at(Bh, 8 * k2 + k1, p);
+      dft8<true>(v);
+#pragma unroll
+      for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, p)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int j = t + it * kTileThreads;
+      const int p = j & 127, n1 = j >> 7;
+      float2 v[16];
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(8 * k2 + n1, p)];
+      dft16<true>(v);
+#pragma unroll
+      for (int n2 = 0; n2 < 16; ++n2) W[widx(n1 + 8 * n2, p)] = v[n2];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int j = t + it * kTileThreads;
+      const int y = j >> 4, k2 = j & 15;
+      float2 v[8];
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
+      dft8<true>(v);
+#pragma unroll
+      for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
+    }
+    __syncthreads();
     float* __restrict__ gl = sd->gLvl;
     const int gp = sd->lvlPitchF;
-    for (int j = t; j < kTile * kTile; j += kTileThreads) {
-      const int y = j >> 7, x = j & 127;
-      const float g = acc[j];
-      if (g != 0.f) atomicAdd(gl + (size_t)rmap[y] * gp + cmap[x], kFloatLevelScale * g);
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int j = t + it * kTileThreads;
+      const int y = j >> 3, n1 = j & 7;
+      float2 v[16];
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(y, 8 * k2 + n1)];
+      dft16<true>(v);
+      float* row = gl + (size_t)rmap[y] * gp;
+#pragma unroll
+      for (int n2 = 0; n2 < 16; ++n2) {
+        const float g = v[n2].x;
+        if (g != 0.f) atomicAdd(row + cmap[n1 + 8 * n2], kFloatLevelScale * g);
+      }
     }
   }
   block_add_double(accA, gparams + 0);

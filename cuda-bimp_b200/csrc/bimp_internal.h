@@ -20,6 +20,7 @@ constexpr int kXhCols = 65;                // Hermitian half: kx = 0..64
 constexpr int kTileThreads = 512;
 constexpr int kMaxHalf = 56;               // largest supported kernel half size
 constexpr int kSpecFloats = kTile * kTile; // one orientation's real spectrum
+constexpr int kSpecHalf = kTile * kXhCols;  // Hermitian half of a tile spectrum
 
 // Per (image, scale) descriptor read by every kernel.  Plain old data.
 struct ScaleDev {
@@ -65,8 +66,11 @@ struct ScaleDev {
   const float* M;         // loss weights, dataH x dataW (row pitch dataW)
   float* gC;              // d loss / d complex cell, C layout
   float* gLvl;            // d loss / d float level, lvlPitchF floats per row
-  const float* dGa;       // real tile spectra of d taps / d alpha, G layout
-  const float* dGr;       // ... / d rho
+  float* T;               // tangential inhibition map, dataH x dPitch
+  float* R;               // radial inhibition map, dataH x dPitch
+  unsigned int* bits;     // ReLU states, 4 bits per orientation, dataH x dPitch
+  const float4* bwA;      // per orientation, kSpecHalf entries {G(k), G(-k), dGa(k), dGr(k)}
+  const float2* bwB;      //   {dGa(-k), dGr(-k)}; dG* = spectra of d taps / d alpha, d rho
 };
 
 // Stencil offset sets of the two level wavelengths the default bank uses

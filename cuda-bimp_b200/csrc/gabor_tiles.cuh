@@ -7,7 +7,8 @@
 // and then for each of the 8 orientations the spectrum is multiplied by that
 // orientation's real Gabor spectrum G_o, inverse transformed as one complex
 // FFT (e + i o) and reduced to |e + i o| on the valid outputs.  The
-// differentiable variant also stores e + i o for the adjoint.
+// differentiable variant also stores e + i o and the tile's image spectrum
+// for the adjoint.
 //
 // G_o (64 KB per orientation, L2-resident) is streamed into a double buffer of
 // 16 KB chunks with TMA bulk copies (cp.async.bulk + mbarrier): chunk c + 2 is
@@ -173,7 +174,7 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
 template <bool FLT, bool SAVE_Z>
 __global__ void __launch_bounds__(kTileThreads, 1)
 k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ work, int nwork,
-              unsigned int* __restrict__ fault_word) {
+              unsigned int* __restrict__ fault_word, float2* __restrict__ xsave) {
   extern __shared__ float4 smem4[];
   char* base = reinterpret_cast<char*>(smem4);
   float2* W = reinterpret_cast<float2*>(base);
@@ -217,6 +218,10 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
                 ((gc + 1) & 1) ? bar1 : bar0);
     }
     tile_forward_spectrum<FLT>(sd, R0, C0, W, Xh, tw, rmap, cmap, t);
+    if constexpr (SAVE_Z) {   // the adjoint keeps the tile's image spectrum (Hermitian half)
+      float2* __restrict__ xs = xsave + (size_t)w * kSpecHalf;
+      for (int j = t; j < kSpecHalf; j += kTileThreads) xs[j] = Xh[j];
+    }
 
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     float* __restrict__ C0p = sd->C;

@@ -127,21 +127,29 @@ __device__ __forceinline__ int soff(const StencilPar& P, int k, int o) {
 // The double-stopped term c - 0.5 a - 0.5 b, which the reference evaluates
 // in double and rounds once, is two fused float multiply-adds here (at most
 // one float rounding apart).
-template <bool CHECK, int PAT>
+// ADJ (the differentiable forward) also returns the tangential and radial
+// sums T, R and the ReLU states the adjoint needs: per orientation o, bit 4o
+// double-stopped d > 0, 4o+1 tangential t > 0, 4o+2 radial r > 0, 4o+3 the
+// first radial term r1 > 0 (all 0 where the bounds test fails).
+template <bool CHECK, int PAT, bool ADJ>
 __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, const StencilPar& P, int x, int y,
                                               int cy, int cx, float gain, float wT, float wR, float& Dout,
-                                              float& Sout) {
+                                              float& Sout, float& Tout, float& Rout, unsigned int& bits) {
   float S = 0.f, D = 0.f, T = 0.f, R = 0.f;
+  unsigned int b = 0;
   const float* c0 = s_c + cy * kStW + cx;
 #pragma unroll
   for (int o = 0; o < kNumOri; ++o) {
     if (CHECK && !(x >= P.exlo[o] && x <= P.exhi[o] && y >= P.eylo[o] && y <= P.eyhi[o])) continue;
     const int o1 = soff<PAT>(P, 0, o), o2 = soff<PAT>(P, 1, o);
     const float* c = c0 + o * (kStH * kStW);
-    float s = c[-o1 * kStW + o2] - c[o1 * kStW - o2];
-    s = s > 0.f ? s : 0.f;
-    if (s > 0.f) S += s;
+    if constexpr (!ADJ) {
+      float s = c[-o1 * kStW + o2] - c[o1 * kStW - o2];
+      s = s > 0.f ? s : 0.f;
+      if (s > 0.f) S += s;
+    }
     float d = fmaf(-0.5f, c[2 * o1 * kStW - 2 * o2], fmaf(-0.5f, c[-2 * o1 * kStW + 2 * o2], c[0]));
+    if constexpr (ADJ) b |= (d > 0.f ? 1u : 0u) << (4 * o);
     d = d > 0.f ? d : 0.f;
     if (d > 0.f) D += d;
   }
@@ -153,24 +161,42 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
     const float* cp = c0 + ((o + kNumOri / 2) % kNumOri) * (kStH * kStW);
     const float centre = c[0];
     float v = c[-o1 * kStW - o2] - centre;
+    if constexpr (ADJ) b |= (v > 0.f ? 2u : 0u) << (4 * o);
     v = v < 0.f ? 0.f : v;
     T += v;
     const int h1 = soff<PAT>(P, 4, o), h2 = soff<PAT>(P, 5, o);
     float r = centre - gain * cp[h1 * kStW + h2];
+    if constexpr (ADJ) b |= (r > 0.f ? 8u : 0u) << (4 * o);
     r = r < 0.f ? 0.f : r;
     r += centre - gain * cp[-h1 * kStW - h2];
+    if constexpr (ADJ) b |= (r > 0.f ? 4u : 0u) << (4 * o);
     r = r < 0.f ? 0.f : r;
     R += r;
   }
   const float inhib = wT * T + wR * R;
   Dout = D + (-inhib);
   Sout = S + (-inhib);
+  if constexpr (ADJ) {
+    Tout = T;
+    Rout = R;
+    bits = b;
+  }
 }
 
-template <int PAT>
+// Output maps of one stencil block: D and S, or for ADJ D, T, R and the
+// ReLU-state words.
+struct StencilOut {
+  float* D;
+  float* S;
+  float* T;
+  float* R;
+  unsigned int* bits;
+  int pitch;
+};
+
+template <int PAT, bool ADJ>
 __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, const StencilPar& P, int x0, int y0,
-                                               int W, int H, float gain, float wT, float wR, float* __restrict__ Dmap,
-                                               float* __restrict__ Smap, int dPitch) {
+                                               int W, int H, float gain, float wT, float wR, const StencilOut& out) {
   const int t = threadIdx.x;
   const int lx = t & 31, ly0 = t >> 5;
   const int x = x0 + lx;
@@ -182,18 +208,27 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
     const int ly = ly0 + 8 * i;
     const int y = y0 + ly;
     if (x >= W || y >= H) continue;
-    float D, S;
+    float D, S, T, R;
+    unsigned int b;
     if (inner)
-      stencil_pixel<false, PAT>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S);
+      stencil_pixel<false, PAT, ADJ>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S, T, R, b);
     else
-      stencil_pixel<true, PAT>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S);
-    Dmap[(size_t)y * dPitch + x] = D;
-    Smap[(size_t)y * dPitch + x] = S;
+      stencil_pixel<true, PAT, ADJ>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S, T, R, b);
+    const size_t k = (size_t)y * out.pitch + x;
+    out.D[k] = D;
+    if constexpr (ADJ) {
+      out.T[k] = T;
+      out.R[k] = R;
+      out.bits[k] = b;
+    } else {
+      out.S[k] = S;
+    }
     dmax = fmaxf(dmax, D);
   }
   return dmax;
 }
 
+template <bool ADJ>
 __global__ void __launch_bounds__(256, 3)
 k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
   extern __shared__ float4 s_c4[];   // kNumOri x kStH x kStW floats
@@ -211,9 +246,13 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
   const long long cStride = sd->cStride;
   const int wrapW = sd->wrapW;
   const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
-  float* __restrict__ Dmap = sd->D;
-  float* __restrict__ Smap = sd->S;
-  const int dPitch = sd->dPitch;
+  StencilOut out;
+  out.D = sd->D;
+  out.S = sd->S;
+  out.T = sd->T;
+  out.R = sd->R;
+  out.bits = sd->bits;
+  out.pitch = sd->dPitch;
   const int pattern = sd->pattern;
   unsigned int* maxKey = sd->maxKey;
   if (t < kNumOri) {
@@ -258,11 +297,11 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
 
   float dmax;
   if (pattern == 1)
-    dmax = stencil_block<1>(s_c, P, x0, y0, W, H, gain, wT, wR, Dmap, Smap, dPitch);
+    dmax = stencil_block<1, ADJ>(s_c, P, x0, y0, W, H, gain, wT, wR, out);
   else if (pattern == 2)
-    dmax = stencil_block<2>(s_c, P, x0, y0, W, H, gain, wT, wR, Dmap, Smap, dPitch);
+    dmax = stencil_block<2, ADJ>(s_c, P, x0, y0, W, H, gain, wT, wR, out);
   else
-    dmax = stencil_block<0>(s_c, P, x0, y0, W, H, gain, wT, wR, Dmap, Smap, dPitch);
+    dmax = stencil_block<0, ADJ>(s_c, P, x0, y0, W, H, gain, wT, wR, out);
   // block max -> one atomic per block
 #pragma unroll
   for (int m = 16; m > 0; m >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
@@ -458,8 +497,8 @@ cudaError_t configure_kernels() {
   const cudaFuncAttribute big = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaFuncSetAttribute(k_gabor_tiles<false, false>, big, (int)gabor_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles<true, true>, big, (int)gabor_smem_bytes());
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil, big, (int)stencil_smem_bytes());
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil_bwd, big, (int)kStencilBwdSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<false>, big, (int)stencil_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<true>, big, (int)stencil_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles_bwd, big, (int)kGaborBwdSmem);
   if (e != cudaSuccess) return e;
   return upload_twiddles();
@@ -471,11 +510,12 @@ void launch_pyr(const PyrJob* d_jobs, int njobs, int maxW, int maxH, cudaStream_
 }
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                   cudaStream_t s) {
-  k_gabor_tiles<false, false><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+  k_gabor_tiles<false, false><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault,
+                                                                              nullptr);
 }
 void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
-                       cudaStream_t s) {
-  k_gabor_tiles<true, true><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+                       float2* d_xsave, cudaStream_t s) {
+  k_gabor_tiles<true, true><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault, d_xsave);
 }
 void launch_pyr_f(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s) {
   dim3 b(32, 8), g((maxW + 31) / 32, (maxH + 7) / 8, njobs);
@@ -485,22 +525,26 @@ void launch_pyr_f_adj(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cuda
   dim3 b(32, 8), g((maxW + 31) / 32, (maxH + 7) / 8, njobs);
   k_pyr_down_f_adj<<<g, b, 0, s>>>(d_jobs);
 }
-void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, cudaStream_t s) {
-  if (nwork > 0) k_masked_loss<<<nwork, 256, 0, s>>>(d_sd, d_work, d_loss);
+void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, double* d_gparams,
+                        cudaStream_t s) {
+  if (nwork > 0) k_masked_loss<<<nwork, 256, 0, s>>>(d_sd, d_work, d_loss, d_gparams);
 }
-void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_gparams, cudaStream_t s) {
-  if (nwork > 0) k_stencil_bwd<<<nwork, 256, kStencilBwdSmem, s>>>(d_sd, d_work, d_gparams);
+void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
+  if (nwork > 0) k_stencil_bwd<<<nwork, kStBwThreads, 0, s>>>(d_sd, d_work);
 }
-void launch_wrap_merge(const ScaleDev* d_sd, const int* d_entries, int n, int maxRows, cudaStream_t s) {
-  if (n > 0) k_wrap_merge<<<dim3((maxRows + 1 + 255) / 256, n), 256, 0, s>>>(d_sd, d_entries, n);
+void launch_gc_finish(const ScaleDev* d_sd, int nEntries, int maxSide, cudaStream_t s) {
+  if (nEntries > 0) k_gc_finish<<<dim3((maxSide + 1 + 255) / 256, nEntries), 256, 0, s>>>(d_sd);
 }
-void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, float* d_gwin,
+void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, const float2* d_xsave,
                       double* d_gparams, cudaStream_t s) {
   if (nwork > 0)
-    k_gabor_tiles_bwd<<<grid, kTileThreads, kGaborBwdSmem, s>>>(d_sd, d_work, nwork, d_gwin, d_gparams);
+    k_gabor_tiles_bwd<<<grid, kTileThreads, kGaborBwdSmem, s>>>(d_sd, d_work, nwork, d_xsave, d_gparams);
 }
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
-  k_stencil<<<nwork, 256, stencil_smem_bytes(), s>>>(d_sd, d_work);
+  k_stencil<false><<<nwork, 256, stencil_smem_bytes(), s>>>(d_sd, d_work);
+}
+void launch_stencil_adj(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
+  if (nwork > 0) k_stencil<true><<<nwork, 256, stencil_smem_bytes(), s>>>(d_sd, d_work);
 }
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,

@@ -50,12 +50,18 @@ void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_coun
 // differentiable path and its adjoint
 void launch_pyr_f(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
 void launch_pyr_f_adj(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
+// differentiable forward: also stores e + i o (ScaleDev::Z) and each work
+// item's tile image spectrum (Hermitian half, kSpecHalf float2 at
+// d_xsave + w * kSpecHalf)
 void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
-                       cudaStream_t s);
-void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, cudaStream_t s);
-void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_gparams, cudaStream_t s);
-void launch_wrap_merge(const ScaleDev* d_sd, const int* d_entries, int n, int maxRows, cudaStream_t s);
-void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, float* d_gwin,
+                       float2* d_xsave, cudaStream_t s);
+// differentiable forward stencil: D, T, R and the ReLU states (ScaleDev::bits)
+void launch_stencil_adj(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
+void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, double* d_gparams,
+                        cudaStream_t s);
+void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
+void launch_gc_finish(const ScaleDev* d_sd, int nEntries, int maxSide, cudaStream_t s);
+void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, const float2* d_xsave,
                       double* d_gparams, cudaStream_t s);
 
 }  // namespace bimp_b200

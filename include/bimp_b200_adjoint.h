@@ -17,7 +17,11 @@
  *          D = D_double - w_tan * T - w_rad * R, at the params' values (1, 1).
  * Kernel sizes, stencil offsets, pyramid steps and margins stay at their
  * nominal values (they are integer functions of lambda); ReLU derivatives
- * are 0 at 0.  The forward keeps the complex responses for the backward.
+ * are 0 at 0, and a complex response |e + i o| <= 3e-5 passes no gradient
+ * (exactly flat image regions give |e + i o| = 0 up to rounding, where the
+ * magnitude has no derivative; the value assumes images on the [0, 1] scale).
+ * The forward keeps the complex responses and each tile's image spectrum
+ * for the backward.
  */
 #ifndef BIMP_B200_ADJOINT_H
 #define BIMP_B200_ADJOINT_H
@@ -54,6 +58,14 @@ int bimp_adjoint_backward(bimp_adjoint* a, float* d_grad, size_t pitch, double* 
 /* Summed keypoint map of image i, scale s of the last forward (device copy,
  * data_h x data_w, row pitch ld floats). */
 int bimp_adjoint_dense_map(bimp_adjoint* a, int image, int scale, float* d_out, size_t ld, void* stream);
+
+/* Complex cells |e + i o| of image i, scale s, orientation o of the last
+ * forward over the stencil window: (data_h + 1) x (data_w + 1) floats, row
+ * pitch ld, element (r, c) = the torus element r * fftW + c (so column data_w
+ * is row r + 1, column 0 when fftW == data_w).  The backward's ReLU states and
+ * magnitude floor are functions of these values. */
+int bimp_adjoint_complex_map(bimp_adjoint* a, int image, int scale, int orientation, float* d_out, size_t ld,
+                             void* stream);
 
 /* Device bytes held by the adjoint's buffers. */
 size_t bimp_adjoint_device_bytes(const bimp_adjoint* a);

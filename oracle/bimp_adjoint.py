@@ -18,7 +18,8 @@ bimp/include/detection/cuda_bimp.cuh:436-517).  Gradients with respect to
 The forward restates bimp_oracle's per-scale pipeline in float64 with taps
 computed from the Gabor formula (bimp/src/cuda_bimp.cu:304-331) as
 differentiable functions of (alpha, rho); the backward is written out by hand
-and checked against central finite differences.  ReLU derivatives are 0 at 0.
+and checked against central finite differences.  ReLU derivatives are 0 at
+0, and |e + i o| <= MAG_FLOOR passes no gradient.
 """
 from __future__ import annotations
 
@@ -30,6 +31,10 @@ import numpy as np
 from . import bimp_oracle as O
 
 KAPPA = 255.0 * 255.0 / 65536.0
+# |e + i o| at or below this passes no gradient (the minimal-norm subgradient
+# of |z| at 0): exactly flat image regions give z = 0 up to rounding, where
+# z/|z| is the direction of rounding noise.  Same value as the CUDA backward.
+MAG_FLOOR = 3.0e-5
 
 
 @dataclass
@@ -158,53 +163,89 @@ def loss(X, lambdas, masks, th: Theta = Theta(), p: O.Params = O.Params()) -> fl
     return total
 
 
-def stencil_backward(Cw: np.ndarray, M: np.ndarray, sc: O.Scale, th: Theta, p: O.Params = O.Params()):
+def _relu_states(Cw: np.ndarray, sc: O.Scale, p: O.Params, fp32: bool):
+    """Per orientation, the ReLU states of the stencils at every pixel:
+    d > 0 (double-stopped), t > 0 (tangential), r > 0 and r1 > 0 (radial),
+    each gated by its bounds test.  fp32=True evaluates the arguments from
+    float32 cells with the CUDA kernels' float operation order (fused
+    multiply-adds round once), so the states are the ones the device took."""
+    f = (lambda v: v.astype(np.float32).astype(np.float64)) if fp32 else (lambda v: v)
+    yc, xc = _shift_idx(sc, 0, 0)
+    out = []
+    for o in range(O.NUM_ORI):
+        C = Cw[o]
+        Cp = Cw[(o + O.NUM_ORI // 2) % O.NUM_ORI]
+        o1, o2 = sc.es_off[o]
+        ya, xa = _shift_idx(sc, -2 * o1, 2 * o2)
+        yb, xb = _shift_idx(sc, 2 * o1, -2 * o2)
+        c0 = C[yc, xc]
+        if fp32:
+            d = f(f(c0 - 0.5 * C[ya, xa]) - 0.5 * C[yb, xb])
+        else:
+            d = c0 - 0.5 * C[ya, xa] - 0.5 * C[yb, xb]
+        i1, i2 = sc.in_off[o]
+        m_in = O.stencil_masks(sc, i1, i2)
+        yt, xt = _shift_idx(sc, -i1, -i2)
+        t = f(C[yt, xt] - c0)
+        h1 = O._round_half_away(0.5 * i1)
+        h2 = O._round_half_away(0.5 * i2)
+        yp, xp = _shift_idx(sc, h1, h2)
+        ym, xm = _shift_idx(sc, -h1, -h2)
+        r1 = f(c0 - p.radial_gain * Cp[yp, xp])
+        r = f(np.maximum(r1, 0.0) + f(c0 - p.radial_gain * Cp[ym, xm]))
+        out.append({"d": O.stencil_masks(sc, o1, o2) & (d > 0), "t": m_in & (t > 0), "r": m_in & (r > 0),
+                    "r1": r1 > 0})
+    return out
+
+
+def stencil_backward(Cw: np.ndarray, M: np.ndarray, sc: O.Scale, th: Theta, p: O.Params = O.Params(),
+                     decide: np.ndarray | None = None):
     """Gradient of sum(M * D) with respect to the stencil window Cw
-    (8, dataH+1, dataW+1), plus the T and R maps' loss terms."""
+    (8, dataH+1, dataW+1).  The ReLU states come from Cw in float64, or, when
+    `decide` (float32 cells of the same window) is given, from those with the
+    device's float arithmetic."""
+    st = _relu_states(Cw if decide is None else decide.astype(np.float64), sc, p, fp32=decide is not None)
     g = np.zeros_like(Cw)
     gT = -th.w_tan * M
     gR = -th.w_rad * M
+    yc, xc = _shift_idx(sc, 0, 0)
     for o in range(O.NUM_ORI):
         o1, o2 = sc.es_off[o]
-        m = O.stencil_masks(sc, o1, o2)
-        C = Cw[o]
-        yc, xc = _shift_idx(sc, 0, 0)
         ya, xa = _shift_idx(sc, -2 * o1, 2 * o2)
         yb, xb = _shift_idx(sc, 2 * o1, -2 * o2)
-        d = C[yc, xc] - 0.5 * C[ya, xa] - 0.5 * C[yb, xb]
-        act = m & (d > 0)
-        gd = np.where(act, M, 0.0)
+        gd = np.where(st[o]["d"], M, 0.0)
         np.add.at(g[o], (np.broadcast_to(yc, gd.shape), np.broadcast_to(xc, gd.shape)), gd)
         np.add.at(g[o], (np.broadcast_to(ya, gd.shape), np.broadcast_to(xa, gd.shape)), -0.5 * gd)
         np.add.at(g[o], (np.broadcast_to(yb, gd.shape), np.broadcast_to(xb, gd.shape)), -0.5 * gd)
     for o in range(O.NUM_ORI):
         op = (o + O.NUM_ORI // 2) % O.NUM_ORI
         i1, i2 = sc.in_off[o]
-        m = O.stencil_masks(sc, i1, i2)
-        C = Cw[o]
-        Cp = Cw[op]
-        yc, xc = _shift_idx(sc, 0, 0)
         yt, xt = _shift_idx(sc, -i1, -i2)
-        t = C[yt, xt] - C[yc, xc]
-        gt = np.where(m & (t > 0), gT, 0.0)
+        gt = np.where(st[o]["t"], gT, 0.0)
         np.add.at(g[o], (np.broadcast_to(yt, gt.shape), np.broadcast_to(xt, gt.shape)), gt)
         np.add.at(g[o], (np.broadcast_to(yc, gt.shape), np.broadcast_to(xc, gt.shape)), -gt)
         h1 = O._round_half_away(0.5 * i1)
         h2 = O._round_half_away(0.5 * i2)
         yp, xp = _shift_idx(sc, h1, h2)
         ym, xm = _shift_idx(sc, -h1, -h2)
-        r1 = C[yc, xc] - p.radial_gain * Cp[yp, xp]
-        r = np.maximum(r1, 0.0) + C[yc, xc] - p.radial_gain * Cp[ym, xm]
-        gr = np.where(m & (r > 0), gR, 0.0)
-        gr1 = np.where(r1 > 0, gr, 0.0)
+        gr = np.where(st[o]["r"], gR, 0.0)
+        gr1 = np.where(st[o]["r1"], gr, 0.0)
         np.add.at(g[o], (np.broadcast_to(yc, gr.shape), np.broadcast_to(xc, gr.shape)), gr + gr1)
         np.add.at(g[op], (np.broadcast_to(ym, gr.shape), np.broadcast_to(xm, gr.shape)), -p.radial_gain * gr)
         np.add.at(g[op], (np.broadcast_to(yp, gr.shape), np.broadcast_to(xp, gr.shape)), -p.radial_gain * gr1)
     return g
 
 
-def gradient(X, lambdas, masks, th: Theta = Theta(), p: O.Params = O.Params()):
-    """Loss and its gradient: (L, dL/dX, {alpha, rho, w_tan, w_rad})."""
+def gradient(X, lambdas, masks, th: Theta = Theta(), p: O.Params = O.Params(), decide=None):
+    """Loss and its gradient: (L, dL/dX, {alpha, rho, w_tan, w_rad}).
+
+    decide: optional list (per scale) of float32 complex-cell windows
+    (8, dataH+1, dataW+1), e.g. the device's; the piecewise choices (ReLU
+    states and the magnitude floor) are then taken from them, so that the
+    gradient is that of the same linear piece the device evaluated.  A float32
+    forward sits within its rounding of ReLU kinks wherever an argument is
+    within ~1e-7 of the map peak of zero, and each such kink moves the
+    gradient by one pixel's share."""
     H, W = X.shape
     scales = O.scale_geometry(W, H, lambdas, p)
     maxl = max(s.levels for s in scales)
@@ -219,15 +260,22 @@ def gradient(X, lambdas, masks, th: Theta = Theta(), p: O.Params = O.Params()):
         total += float((M * f["D"]).sum())
         gth["w_tan"] += float(-(M * f["T"]).sum())
         gth["w_rad"] += float(-(M * f["R"]).sum())
-        gCw = stencil_backward(f["Cw"], M, sc, th, p)
+        dec = None if decide is None else decide[s]
+        gCw = stencil_backward(f["Cw"], M, sc, th, p, decide=dec)
         gCt = np.zeros((O.NUM_ORI, sc.fftH * sc.fftW))
         for o in range(O.NUM_ORI):
             np.add.at(gCt[o], f["flat"].ravel(), gCw[o].ravel())
         gCt = gCt.reshape(O.NUM_ORI, sc.fftH, sc.fftW)
         Ct = f["Ct"]
+        if dec is None:
+            Cdec = Ct
+        else:
+            Cdec = np.zeros((O.NUM_ORI, sc.fftH * sc.fftW))
+            Cdec[:, f["flat"].ravel()] = dec.reshape(O.NUM_ORI, -1)
+            Cdec = Cdec.reshape(Ct.shape)
         with np.errstate(divide="ignore", invalid="ignore"):
-            gE = np.where(Ct > 0, gCt * f["E"] / Ct, 0.0)
-            gO = np.where(Ct > 0, gCt * f["O"] / Ct, 0.0)
+            gE = np.where(Cdec > MAG_FLOOR, gCt * f["E"] / Ct, 0.0)
+            gO = np.where(Cdec > MAG_FLOOR, gCt * f["O"] / Ct, 0.0)
         gIp = np.zeros((sc.fftH, sc.fftW))
         for o in range(O.NUM_ORI):
             tp = f["taps"][o]

@@ -85,6 +85,62 @@ def test_hd_keypoints_and_maps():
     assert rep["matched"] > 1000
 
 
+def test_uhd_coarse_scales_match_oracle():
+    """3840x2160, the coarse half of the 12-scale bank (pyramid levels 3-5;
+    level 5 keeps 67 of pyrDown's 68 rows)."""
+    img = synth.uhd_frames(1, seed=1004)[0]
+    lam = synth.bank(12)[6:]
+    res = O.run(img, lam)
+    assert res[-1]["scale"].dataH == 67
+    cs, rec, n = _run_gpu(img, lam)
+    _check_scale_maps(cs, res)
+    _check_keypoints(rec, res)
+
+
+def _decision_margin(D, off, thresh_ratio=0.104):
+    """Per-pixel distance of the keypoint decision from flipping (strict
+    8-neighbour max and threshold), from a summed keypoint map."""
+    H, W = D.shape
+    P = np.pad(D, 1, mode="reflect")
+    dil = np.full(D.shape, -np.inf)
+    for dy in (-1, 0, 1):
+        for dx in (-1, 0, 1):
+            if dy or dx:
+                dil = np.maximum(dil, P[1 + dy:1 + dy + H, 1 + dx:1 + dx + W])
+    loc = D - dil
+    dth = D - np.float32(np.float64(D.max()) * thresh_ratio)
+    return np.minimum(np.abs(loc), np.abs(dth))
+
+
+def test_uhd_full_bank_against_c_restatement():
+    """All 12 scales of a 3840x2160 frame against the FP32 C restatement of
+    the reference pipeline (itself pinned to the oracle on CPU): maps within
+    1e-4 of the peak; keypoints identical except where the restatement's
+    decision is within 1e-4 of the peak of a tie."""
+    from oracle.cbimp import CBimp
+    img = synth.uhd_frames(2, seed=1004)[1]
+    lam = synth.bank(12)
+    cs, rec, n = _run_gpu(img, lam)
+    with CBimp(img.shape[1], img.shape[0], lam) as cb:
+        ref, total = cb.detect(img, capacity=1 << 21)
+        assert total == len(ref)
+        sizes = sorted({float(s) for s in ref["size"]} | {float(s) for s in rec["size"]})
+        assert len(sizes) <= len(lam)
+        for s in range(len(lam)):
+            D = cb.dense_map(s)
+            assert peak_rel_error(cs.dense_map(s, 0).cpu().numpy(), D) <= MAP_TOL
+            info = cb.scales[s]
+            pyr = 2 ** info["level"]
+            size = np.float32(np.float32(lam[s] / pyr) * np.float32(pyr))
+            a = {(int(np.rint(k["x"] / pyr)), int(np.rint(k["y"] / pyr))) for k in ref if k["size"] == size}
+            b = {(int(np.rint(k["x"] / pyr)), int(np.rint(k["y"] / pyr))) for k in rec if k["size"] == size}
+            marg = _decision_margin(D, info["off"])
+            peak = np.abs(D).max()
+            for (x, y) in a ^ b:
+                assert marg[y, x] < 1e-4 * peak, (s, x, y, marg[y, x] / peak)
+            assert len(a ^ b) <= max(2, len(a) // 1000), (s, len(a ^ b), len(a))
+
+
 def test_detect_host_matches_device():
     imgs, lam = synth.workload("vga")
     img = imgs[0]
