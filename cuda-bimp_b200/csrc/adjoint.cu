@@ -57,7 +57,7 @@ void gather_half(const float* G, const float* dA, const float* dR, float4* A, fl
 }
 
 struct bimp_adjoint {
-  int device = 0, W = 0, H = 0, n = 0, nScales = 0, maxLevel = 0, maxSide = 0;
+  int device = 0, W = 0, H = 0, n = 0, nScales = 0, maxLevel = 0;
   bimp_params params{};
   std::vector<ScaleHost> geo;
   char* mem = nullptr;
@@ -68,7 +68,7 @@ struct bimp_adjoint {
   int nTiles = 0;
   int2* d_sten = nullptr;                 // forward stencil blocks (data)
   int nSten = 0;
-  int2* d_stenB = nullptr;                // backward gather blocks (window, data + 1)
+  int2* d_stenB = nullptr;                // backward gather blocks (window rows 0..dataH+1)
   int nStenB = 0;
   std::vector<float*> lvl, glvl;          // [level][image]
   std::vector<int> lw, lh, lp;            // per level (same for all images)
@@ -95,7 +95,6 @@ struct bimp_adjoint {
     if (!build_scales(w, h, std::vector<float>(lambdas, lambdas + nl), p, geo, err)) return afail(BIMP_ERR_INVALID, err);
     nScales = static_cast<int>(geo.size());
     for (auto& s : geo) maxLevel = std::max(maxLevel, s.level);
-    maxSide = std::max(w, h);
     // backward coefficients: G and the derivative spectra, gathered
     std::vector<float4> hA((size_t)nScales * kNumOri * kSpecHalf);
     std::vector<float2> hB((size_t)nScales * kNumOri * kSpecHalf);
@@ -139,7 +138,7 @@ struct bimp_adjoint {
     std::vector<TileWork> tiles;
     std::vector<int2> sten, stenB;
     std::vector<ScaleDev> sds;
-    std::vector<size_t> offC, offZ, offD, offT, offR, offBits, offGC;
+    std::vector<size_t> offC, offZ, offD, offT, offR, offBits, offGC, offGW;
     for (int i = 0; i < n; ++i) {
       for (int si = 0; si < nScales; ++si) {
         const ScaleHost& s = geo[si];
@@ -185,12 +184,13 @@ struct bimp_adjoint {
         for (int tI = 0; tI < d.tilesX * d.tilesY; ++tI) tiles.push_back({entry, tI});
         const int nbx = (s.dataW + 31) / 32, nby = (s.dataH + 31) / 32;
         for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
-        const int nbx2 = (s.dataW + 1 + 31) / 32, nby2 = (s.dataH + 1 + 31) / 32;
+        const int nbx2 = (s.dataW + 1 + 31) / 32, nby2 = (s.dataH + 2 + 31) / 32;   // window + row dataH + 1
         for (int b = 0; b < nbx2 * nby2; ++b) stenB.push_back(make_int2(entry, b));
         const size_t mapB = sizeof(float) * (size_t)s.dataH * d.dPitch;
         offC.push_back(take(sizeof(float) * (size_t)kNumOri * d.cStride));
         offZ.push_back(take(sizeof(float2) * (size_t)kNumOri * d.cStride));
         offGC.push_back(take(sizeof(float) * (size_t)kNumOri * d.cStride));
+        offGW.push_back(take(sizeof(float) * (size_t)kNumOri * (s.dataH + 1)));
         offD.push_back(take(mapB));
         offT.push_back(take(mapB));
         offR.push_back(take(mapB));
@@ -242,6 +242,7 @@ struct bimp_adjoint {
       d.C = reinterpret_cast<float*>(b + offC[e2]);
       d.Z = reinterpret_cast<float2*>(b + offZ[e2]);
       d.gC = reinterpret_cast<float*>(b + offGC[e2]);
+      d.gWrap = reinterpret_cast<float*>(b + offGW[e2]);
       d.D = reinterpret_cast<float*>(b + offD[e2]);
       d.T = reinterpret_cast<float*>(b + offT[e2]);
       d.R = reinterpret_cast<float*>(b + offR[e2]);
@@ -314,7 +315,6 @@ struct bimp_adjoint {
     ADJ_CUDA(cudaMemsetAsync(d_glvl, 0, glvlBytes, s));
     ADJ_CUDA(cudaMemsetAsync(d_gp, 0, sizeof(double) * 2, s));
     launch_stencil_bwd(d_sd, d_stenB, nStenB, s);
-    launch_gc_finish(d_sd, static_cast<int>(h_sd.size()), maxSide, s);
     launch_gabor_bwd(d_sd, d_tiles, nTiles, nTiles, d_xsave, d_gp, s);
     for (int l = maxLevel; l >= 1; --l) launch_pyr_f_adj(d_pyrAdj + (l - 1) * n, n, lw[l], lh[l], s);
     ADJ_CUDA(cudaMemcpy2DAsync(grad, sizeof(float) * pitch, d_glvl, sizeof(float) * lp[0], sizeof(float) * W,

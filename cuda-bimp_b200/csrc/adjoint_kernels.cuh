@@ -5,10 +5,10 @@
 //   k_pyr_down_f_adj    its transpose (scatter-add of the 5x5 taps)
 //   k_masked_loss       sum M * D (the loss) and the w_tan / w_rad gradients
 //   k_stencil_bwd       gather form of d L / d C over the stencil window from
-//                       the ReLU states the forward stencil recorded
-//   k_gc_finish         zero window row dataH + 1; when fftW == dataW, column
-//                       dataW of the window is torus (r+1, 0): its gradient
-//                       moves there
+//                       the ReLU states the forward stencil recorded (when
+//                       fftW == dataW, window column dataW is the torus
+//                       element (r+1, 0): its gradient is kept aside and
+//                       added there by the tile backward)
 //   k_gabor_tiles_bwd   per tile and orientation a = dL/dC * z/|z|, A = FFT(a),
 //                       alpha/rho dot products sum dG Re(conj(A) X) with the
 //                       image spectrum X the forward saved, and the sum of
@@ -122,6 +122,7 @@ k_stencil_bwd(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
   const int x0 = bx * kStX, y0 = by * kStY;
   const int t = threadIdx.x;
   const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
+  const int wrapW = sd->wrapW;
   if (t < kNumOri) {
     sOff[t][0] = sd->es1[t]; sOff[t][1] = sd->es2[t];
     sOff[t][2] = sd->in1[t]; sOff[t][3] = sd->in2[t];
@@ -142,7 +143,7 @@ k_stencil_bwd(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
   const int lx = t & 31;
   for (int ly = t >> 5; ly < kStY; ly += kStBwThreads / 32) {
     const int py = y0 + ly, px = x0 + lx;
-    if (py > H || px > W) continue;
+    if (py > H + 1 || px > W) continue;           // row H + 1: read by no stencil, gathers 0
     const int qy = ly + kHalo, qx = lx + kHalo;   // p in source-pixel coordinates
     auto at = [&](int dy, int dx) { return (qy + dy) * kBwQW + (qx + dx); };
     const unsigned int b0 = sBits[at(0, 0)];
@@ -177,27 +178,14 @@ k_stencil_bwd(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
         if ((b1 & pr) && (b1 & pr1)) g += gain * wR * sM[k1];
         if (b2 & pr) g += gain * wR * sM[k2];
       }
+      // fftW == dataW: window column dataW of row r is the torus element
+      // (r + 1, 0); its gradient goes to gWrap[o][r], which the tile
+      // backward adds at (r + 1, 0)
+      if (wrapW && px == W) {
+        if (py <= H) sd->gWrap[o * (H + 1) + py] = g;
+        g = 0.f;
+      }
       gC[(size_t)o * cStride + (size_t)py * cPitch + px] = g;
-    }
-  }
-}
-
-// After k_stencil_bwd, per entry: row dataH + 1 of the window gradient (read
-// by the tile backward, written by no stencil) starts at zero, and when
-// fftW == dataW the gradient of window column dataW of row r moves to
-// (r + 1, 0), the torus element the stencils actually read there.
-__global__ void k_gc_finish(const ScaleDev* __restrict__ sds) {
-  const ScaleDev* sd = sds + blockIdx.y;
-  const int W = sd->dataW, H = sd->dataH;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int o = 0; o < kNumOri; ++o) {
-    float* g = sd->gC + (size_t)o * sd->cStride;
-    if (i <= W && !(sd->wrapW && i == 0)) g[(size_t)(H + 1) * sd->cPitch + i] = 0.f;
-    if (sd->wrapW && i <= H) {
-      const float v = g[(size_t)i * sd->cPitch + W];
-      g[(size_t)i * sd->cPitch + W] = 0.f;
-      if (i < H) g[(size_t)(i + 1) * sd->cPitch] += v;
-      else g[(size_t)(H + 1) * sd->cPitch] = v;
     }
   }
 }
@@ -259,6 +247,7 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
     for (int j = t; j < kTile * kXhCols; j += kTileThreads) Bh[j] = make_float2(0.f, 0.f);
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     const long long cStride = sd->cStride;
+    const int wrapW = sd->wrapW;
     for (int o = 0; o < kNumOri; ++o) {
       // a = dL/dC * z / |z| on the valid outputs, zero elsewhere; four
       // pixels per thread with their loads issued together
@@ -276,6 +265,7 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
           const size_t k = ok[u] ? (size_t)o * cStride + (size_t)gy * cPitch + gx : 0;
           m[u] = ok[u] ? __ldg(sd->C + k) : 0.f;
           gc[u] = ok[u] ? __ldg(sd->gC + k) : 0.f;
+          if (ok[u] && wrapW && gx == 0 && gy >= 1) gc[u] += __ldg(sd->gWrap + o * (sd->dataH + 1) + gy - 1);
           z[u] = ok[u] ? __ldg(sd->Z + k) : make_float2(0.f, 0.f);
         }
 #pragma unroll

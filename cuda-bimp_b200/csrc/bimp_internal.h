@@ -65,6 +65,7 @@ struct ScaleDev {
   float2* Z;              // saved e + i o, C layout in float2
   const float* M;         // loss weights, dataH x dataW (row pitch dataW)
   float* gC;              // d loss / d complex cell, C layout
+  float* gWrap;           // fftW == dataW: d loss / d window (r, dataW), kNumOri x (dataH + 1)
   float* gLvl;            // d loss / d float level, lvlPitchF floats per row
   float* T;               // tangential inhibition map, dataH x dPitch
   float* R;               // radial inhibition map, dataH x dPitch

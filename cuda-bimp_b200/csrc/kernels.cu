@@ -532,9 +532,7 @@ void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, dou
 void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
   if (nwork > 0) k_stencil_bwd<<<nwork, kStBwThreads, 0, s>>>(d_sd, d_work);
 }
-void launch_gc_finish(const ScaleDev* d_sd, int nEntries, int maxSide, cudaStream_t s) {
-  if (nEntries > 0) k_gc_finish<<<dim3((maxSide + 1 + 255) / 256, nEntries), 256, 0, s>>>(d_sd);
-}
+
 void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, const float2* d_xsave,
                       double* d_gparams, cudaStream_t s) {
   if (nwork > 0)

@@ -60,7 +60,6 @@ void launch_stencil_adj(const ScaleDev* d_sd, const int2* d_work, int nwork, cud
 void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, double* d_gparams,
                         cudaStream_t s);
 void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
-void launch_gc_finish(const ScaleDev* d_sd, int nEntries, int maxSide, cudaStream_t s);
 void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, const float2* d_xsave,
                       double* d_gparams, cudaStream_t s);
 
