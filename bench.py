@@ -436,6 +436,109 @@ def run_adjoint_bench(args, rank, world, dev, stream, max_ms):
     return out
 
 
+def run_configs(args):
+    """The other workload configurations, each next to the FP32 C
+    restatement on the host cores (one JSON object):
+
+    * cfg0: one 640x480 image, 4 scales (4, 8, 16, 32), plain path;
+    * cfg4: 32 correlated 3840x2160 frames, 12 scales: batched forward (one
+      graph replay) and the adjoint forward + backward of all 32 frames,
+      with the device memory it holds.
+    """
+    import torch
+    from bimp_b200 import _lib as L
+    from bimp_b200 import api, synth
+    from oracle.cbimp import CBimp, max_threads
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(int(stream.cuda_stream))
+    lib = L.lib()
+    out = {}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, k):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(k):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / k
+
+    def cpu(img, lam, reps):
+        with CBimp(img.shape[1], img.shape[0], lam) as cb:
+            cb.detect(img)
+            ts = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                cb.detect(img)
+                ts.append(time.perf_counter() - t0)
+        return {"mpixel_s": round(img.size / statistics.median(ts) / 1e6, 3), "cores": max_threads(),
+                "median_s": round(statistics.median(ts), 4), "runs": reps}
+
+    # cfg0: VGA, plain path, 16 distinct shifted copies resident in HBM
+    imgs, lam = synth.workload("vga")
+    pool = [torch.from_numpy(np.ascontiguousarray(np.roll(imgs[0], 37 * i, axis=1))).to(dev) for i in range(16)]
+    cs = api.CudaStuff(640, 480, lam)
+    kp = torch.zeros((7, 65536), dtype=torch.float32, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    it = [0]
+
+    def vga_step():
+        g = pool[it[0] % 16]
+        it[0] += 1
+        L.check(lib.bimp_detect_device_async(cs.handle, C.c_void_p(g.data_ptr()), g.stride(0), 640, 480,
+                                             C.c_void_p(kp.data_ptr()), kp.stride(0), 65536,
+                                             C.c_void_p(cnt.data_ptr()), sp), "vga detect")
+    ms = timed(vga_step, 500)
+    out["cfg0"] = {"workload": "one 640x480 uint8 image, lambdas 4, 8, 16, 32, 8 orientations, plain path",
+                   "ms_per_image": round(ms, 4), "mpixel_s": round(640 * 480 / (ms * 1e-3) / 1e6, 1),
+                   "cpu_baseline": cpu(imgs[0], lam, 5)}
+    cs.close()
+    del pool
+
+    # cfg4: 32 UHD frames, 12 scales
+    frames = synth.uhd_frames(32, 1004)
+    lam12 = synth.bank(12)
+    free0 = torch.cuda.mem_get_info()[0]
+    bt = api.Batch([(3840, 2160)] * 32, lam12, kp_capacity=1 << 20)
+    bt_bytes = free0 - torch.cuda.mem_get_info()[0]
+    bt.load(frames)
+    ms = timed(bt.run, 5)
+    n_kp = int(bt.counts().sum().item())
+    bt.close()
+    torch.cuda.synchronize()
+    fwd = {"ms_per_batch": round(ms, 2), "mpixel_s": round(32 * 3840 * 2160 / (ms * 1e-3) / 1e6, 1),
+           "device_bytes": int(bt_bytes), "keypoints": n_kp, "graph": True}
+    x = torch.from_numpy(np.stack([f.astype(np.float32) / np.float32(255.0) for f in frames])).to(dev)
+    del frames
+    free0 = torch.cuda.mem_get_info()[0]
+    adj = api.Adjoint(3840, 2160, 32, lam12)
+    masks = torch.randn(32 * adj.mask_stride, generator=torch.Generator(device=dev).manual_seed(5), device=dev)
+    adj.forward(x, masks)
+    grad, _ = adj.backward()
+    torch.cuda.synchronize()
+    held = free0 - torch.cuda.mem_get_info()[0]
+    f_ms = timed(lambda: adj.forward(x, masks), 3)
+    b_ms = timed(lambda: adj.backward(grad), 3)
+    out["cfg4"] = {"workload": "32 correlated 3840x2160 frames (subpixel shifts <= 2 px + N(0,2) noise), "
+                               "12 scales x 8 orientations",
+                   "forward_batched": fwd,
+                   "adjoint": {"fwd_ms": round(f_ms, 2), "bwd_ms": round(b_ms, 2),
+                               "bwd_fwd_ratio": round(b_ms / f_ms, 3),
+                               "train_step_mpixel_s": round(32 * 3840 * 2160 / ((f_ms + b_ms) * 1e-3) / 1e6, 1),
+                               "device_bytes_arena": adj.device_bytes(),
+                               "device_bytes_held": int(held),
+                               "note": "responses (e + i o, |e + i o|) are stored, not recomputed: "
+                                       "all 32 frames fit in HBM"},
+                   "cpu_baseline_one_frame": cpu(synth.uhd_frames(1, 1004)[0], lam12, 1)}
+    adj.close()
+    print(json.dumps({"configs": out}), flush=True)
+
+
 def cs_launches(cs) -> int:
     from bimp_b200 import _lib as L
     return int(L.lib().bimp_ctx_kernel_launches(cs.handle))
@@ -510,6 +613,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--configs", action="store_true",
+                    help="the other workload configurations (VGA, 32 UHD frames forward and adjoint), 1 GPU")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="only the forward/backward measurement of the adjoint workload (1 GPU)")
     args = ap.parse_args()
@@ -519,6 +624,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.configs:
+        run_configs(args)
+        return
     if args.adjoint_only:
         import torch
         torch.cuda.set_device(local_rank)
