@@ -11,6 +11,8 @@
 //   k_scan          exclusive scan of the row counts
 //   k_nms_write     keypoint records in (scale, y, x) order
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <cstdint>
 
 #include "bimp_internal.h"
@@ -194,7 +196,7 @@ struct StencilOut {
   int pitch;
 };
 
-template <int PAT, bool ADJ>
+template <int PAT, bool ADJ, int NT>
 __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, const StencilPar& P, int x0, int y0,
                                                int W, int H, float gain, float wT, float wR, const StencilOut& out) {
   const int t = threadIdx.x;
@@ -204,8 +206,8 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
   // no bounds test needed when every pixel of the block is >= 8 from the edges
   const bool inner = x0 >= kHalo && x0 + kStX <= W - kHalo && y0 >= kHalo && y0 + kStY <= H - kHalo;
 #pragma unroll 1
-  for (int i = 0; i < 4; ++i) {
-    const int ly = ly0 + 8 * i;
+  for (int i = 0; i < kStY / (NT / 32); ++i) {
+    const int ly = ly0 + (NT / 32) * i;
     const int y = y0 + ly;
     if (x >= W || y >= H) continue;
     float D, S, T, R;
@@ -228,91 +230,128 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
   return dmax;
 }
 
-template <bool ADJ>
-__global__ void __launch_bounds__(256, 3)
-k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
-  extern __shared__ float4 s_c4[];   // kNumOri x kStH x kStW floats
-  float* s_c = reinterpret_cast<float*>(s_c4);
-  __shared__ StencilPar P;
-  const int2 item = work[blockIdx.x];
-  const ScaleDev* __restrict__ sd = sds + item.x;
+// Persistent stencil kernel: one CTA of 512 threads per SM walks the block
+// list; while it computes block k from one staging buffer, the copies of
+// block k + 1's complex-cell window (8 orientations x 48 x 48 floats, the
+// 32 x 32 block plus an 8-pixel halo) land in the other through cp.async.
+// Chunks of the window outside the map's allocation are not copied: the
+// bounds test keeps every stencil read inside [0, dataW] x [0, dataH].
+constexpr int kStThreads = 512;
+constexpr int kStBuf = kNumOri * kStH * kStW;    // floats per staging buffer
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+__device__ __forceinline__ void block_origin(const ScaleDev* sd, int blk, int& x0, int& y0) {
+  const int nbx = (sd->dataW + kStX - 1) / kStX;
+  const int by = blk / nbx;
+  x0 = (blk - by * nbx) * kStX;
+  y0 = by * kStY;
+}
+
+__device__ __forceinline__ void stencil_params(const ScaleDev* sd, StencilPar& P, int o) {
   const int W = sd->dataW, H = sd->dataH;
-  const int nbx = (W + kStX - 1) / kStX;
-  const int by = item.y / nbx, bx = item.y - by * nbx;
-  const int x0 = bx * kStX, y0 = by * kStY;
-  const int t = threadIdx.x;
+  const int e1 = sd->es1[o], e2 = sd->es2[o], i1 = sd->in1[o], i2 = sd->in2[o];
+  P.e1[o] = e1; P.e2[o] = e2; P.i1[o] = i1; P.i2[o] = i2;
+  P.h1[o] = sd->ih1[o]; P.h2[o] = sd->ih2[o];
+  P.exlo[o] = 2 * abs(e2); P.exhi[o] = W - 2 * abs(e2);
+  P.eylo[o] = 2 * abs(e1); P.eyhi[o] = H - 2 * abs(e1);
+  P.ixlo[o] = 2 * abs(i2); P.ixhi[o] = W - 2 * abs(i2);
+  P.iylo[o] = 2 * abs(i1); P.iyhi[o] = H - 2 * abs(i1);
+}
+
+// Issue the 16-byte copies of one block's window into buf.  The window's
+// first column x0 - 8 is 16-byte aligned (x0 is a multiple of 32, the pitch
+// a multiple of 32 floats).
+__device__ __forceinline__ void stencil_stage(const ScaleDev* sd, int x0, int y0, float* buf, int t) {
   const float* __restrict__ C = sd->C;
-  const int cPitch = sd->cPitch;
+  const int cPitch = sd->cPitch, cRows = sd->cRows;
   const long long cStride = sd->cStride;
-  const int wrapW = sd->wrapW;
-  const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
-  StencilOut out;
-  out.D = sd->D;
-  out.S = sd->S;
-  out.T = sd->T;
-  out.R = sd->R;
-  out.bits = sd->bits;
-  out.pitch = sd->dPitch;
-  const int pattern = sd->pattern;
-  unsigned int* maxKey = sd->maxKey;
-  if (t < kNumOri) {
-    const int o = t;
-    const int e1 = sd->es1[o], e2 = sd->es2[o], i1 = sd->in1[o], i2 = sd->in2[o];
-    P.e1[o] = e1; P.e2[o] = e2; P.i1[o] = i1; P.i2[o] = i2;
-    P.h1[o] = sd->ih1[o]; P.h2[o] = sd->ih2[o];
-    P.exlo[o] = 2 * abs(e2); P.exhi[o] = W - 2 * abs(e2);
-    P.eylo[o] = 2 * abs(e1); P.eyhi[o] = H - 2 * abs(e1);
-    P.ixlo[o] = 2 * abs(i2); P.ixhi[o] = W - 2 * abs(i2);
-    P.iylo[o] = 2 * abs(i1); P.iyhi[o] = H - 2 * abs(i1);
-  }
-
-  // stage C (rows y0-8 .. y0+39, cols x0-8 .. x0+39) of all orientations
   const int gx0 = x0 - kHalo, gy0 = y0 - kHalo;
-  const bool fast_load = gx0 >= 0 && gx0 + kStW <= W && gy0 >= 0 && gy0 + kStH <= H + 1;
-  if (fast_load) {
-    // every staged column lies inside [0, W-1]: rows of 12 aligned float4
-    constexpr int kV = kStW / 4;
-    for (int idx = t; idx < kNumOri * kStH * kV; idx += 256) {
-      const int row = idx / kV, v4 = idx - row * kV;
-      const int o = row / kStH, ly = row - o * kStH;
-      const float4* src =
-          reinterpret_cast<const float4*>(C + (size_t)o * cStride + (size_t)(gy0 + ly) * cPitch + gx0);
-      s_c4[row * kV + v4] = __ldg(src + v4);
-    }
-  } else {
-    for (int idx = t; idx < kNumOri * kStH * kStW; idx += 256) {
-      const int row = idx / kStW, lx = idx - row * kStW;
-      const int o = row / kStH, ly = row - o * kStH;
-      const int gy = gy0 + ly, gx = gx0 + lx;
-      float v = 0.f;
-      if (gy >= 0 && gy <= H && gx >= 0 && gx <= W) {
-        int ry = gy, rx = gx;
-        if (wrapW && gx == W) { rx = 0; ry = gy + 1; }   // flat y*fftW + fftW
-        v = C[(size_t)o * cStride + (size_t)ry * cPitch + rx];
-      }
-      s_c[idx] = v;
-    }
+  constexpr int kV = kStW / 4;
+#pragma unroll 3
+  for (int idx = t; idx < kNumOri * kStH * kV; idx += kStThreads) {
+    const int row = idx / kV, v4 = idx - row * kV;
+    const int o = row / kStH, ly = row - o * kStH;
+    const int gy = gy0 + ly, gx = gx0 + 4 * v4;
+    if (gy >= 0 && gy < cRows && gx >= 0 && gx + 4 <= cPitch)
+      cp_async16(buf + row * kStW + 4 * v4, C + (size_t)o * cStride + (size_t)gy * cPitch + gx);
   }
-  __syncthreads();
+}
 
-  float dmax;
-  if (pattern == 1)
-    dmax = stencil_block<1, ADJ>(s_c, P, x0, y0, W, H, gain, wT, wR, out);
-  else if (pattern == 2)
-    dmax = stencil_block<2, ADJ>(s_c, P, x0, y0, W, H, gain, wT, wR, out);
-  else
-    dmax = stencil_block<0, ADJ>(s_c, P, x0, y0, W, H, gain, wT, wR, out);
-  // block max -> one atomic per block
+template <bool ADJ>
+__global__ void __launch_bounds__(kStThreads, 1)
+k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int nwork) {
+  extern __shared__ float4 s_c4[];   // 2 buffers of kNumOri x kStH x kStW floats
+  float* s_buf = reinterpret_cast<float*>(s_c4);
+  __shared__ StencilPar P[2];
+  const int t = threadIdx.x;
+  int w = blockIdx.x;
+  if (w >= nwork) return;
+  {
+    const int2 item = work[w];
+    const ScaleDev* sd = sds + item.x;
+    int x0, y0;
+    block_origin(sd, item.y, x0, y0);
+    if (t < kNumOri) stencil_params(sd, P[0], t);
+    stencil_stage(sd, x0, y0, s_buf, t);
+  }
+  cp_async_commit();
+  for (int k = 0; w < nwork; ++k, w += gridDim.x) {
+    const int cur = k & 1;
+    const int wn = w + gridDim.x;
+    if (wn < nwork) {   // the next block's window goes into the other buffer
+      const int2 nx = work[wn];
+      const ScaleDev* sdn = sds + nx.x;
+      int nx0, ny0;
+      block_origin(sdn, nx.y, nx0, ny0);
+      if (t < kNumOri) stencil_params(sdn, P[cur ^ 1], t);
+      stencil_stage(sdn, nx0, ny0, s_buf + (cur ^ 1) * kStBuf, t);
+    }
+    cp_async_commit();
+    cp_async_wait_prev();   // this block's copies (every group but the newest) have landed
+    __syncthreads();
+    const int2 item = work[w];
+    const ScaleDev* __restrict__ sd = sds + item.x;
+    const int W = sd->dataW, H = sd->dataH;
+    int x0, y0;
+    block_origin(sd, item.y, x0, y0);
+    float* s_c = s_buf + cur * kStBuf;
+    // fftW == dataW: the stencils' flat address of column dataW is the next
+    // row's column 0 (y*fftW + fftW)
+    const int lxW = W - (x0 - kHalo);
+    if (sd->wrapW && lxW >= 0 && lxW < kStW) {
+      const float* __restrict__ C = sd->C;
+      for (int idx = t; idx < kNumOri * kStH; idx += kStThreads) {
+        const int o = idx / kStH, ly = idx - o * kStH;
+        const int gy = y0 - kHalo + ly;
+        if (gy >= 0 && gy <= H) s_c[idx * kStW + lxW] = C[(size_t)o * sd->cStride + (size_t)(gy + 1) * sd->cPitch];
+      }
+      __syncthreads();
+    }
+    StencilOut out;
+    out.D = sd->D;
+    out.S = sd->S;
+    out.T = sd->T;
+    out.R = sd->R;
+    out.bits = sd->bits;
+    out.pitch = sd->dPitch;
+    const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
+    float dmax;
+    if (sd->pattern == 1)
+      dmax = stencil_block<1, ADJ, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
+    else if (sd->pattern == 2)
+      dmax = stencil_block<2, ADJ, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
+    else
+      dmax = stencil_block<0, ADJ, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
+    // map max: one atomic per warp
 #pragma unroll
-  for (int m = 16; m > 0; m >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
-  __shared__ float s_max[8];
-  __syncthreads();
-  if ((t & 31) == 0) s_max[t >> 5] = dmax;
-  __syncthreads();
-  if (t == 0) {
-    float m = s_max[0];
-    for (int k = 1; k < 8; ++k) m = fmaxf(m, s_max[k]);
-    if (m > -INFINITY) atomicMax(maxKey, float_key(m));
+    for (int m = 16; m > 0; m >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
+    if ((t & 31) == 0 && dmax > -INFINITY) atomicMax(sd->maxKey, float_key(dmax));
+    __syncthreads();   // buffer cur and P[cur] are refilled in the next iteration
   }
 }
 
@@ -491,7 +530,21 @@ cudaError_t upload_twiddles() {
 }
 
 size_t gabor_smem_bytes() { return kGaborSmem; }
-size_t stencil_smem_bytes() { return sizeof(float) * kNumOri * kStH * kStW; }
+size_t stencil_smem_bytes() { return sizeof(float) * 2 * kStBuf; }
+
+// CTAs of the persistent stencil kernel: one per SM.
+static int g_num_sms[64] = {0};
+int num_sms() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (g_num_sms[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    g_num_sms[dev] = n;
+  }
+  return g_num_sms[dev];
+}
 
 cudaError_t configure_kernels() {
   const cudaFuncAttribute big = cudaFuncAttributeMaxDynamicSharedMemorySize;
@@ -539,10 +592,12 @@ void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, i
     k_gabor_tiles_bwd<<<grid, kTileThreads, kGaborBwdSmem, s>>>(d_sd, d_work, nwork, d_xsave, d_gparams);
 }
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
-  k_stencil<false><<<nwork, 256, stencil_smem_bytes(), s>>>(d_sd, d_work);
+  if (nwork > 0)
+    k_stencil<false><<<std::min(nwork, num_sms()), kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork);
 }
 void launch_stencil_adj(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
-  if (nwork > 0) k_stencil<true><<<nwork, 256, stencil_smem_bytes(), s>>>(d_sd, d_work);
+  if (nwork > 0)
+    k_stencil<true><<<std::min(nwork, num_sms()), kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork);
 }
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,
