@@ -154,7 +154,7 @@ def algorithmic_bytes(cs) -> dict:
     for k in cs.ks:
         n = k["data_w"] * k["data_h"]
         gabor += n * (1 + 8 * 4)          # uint8 level read + 8 fp32 magnitude maps written
-        stencil += n * (8 * 4 + 2 * 4)    # 8 magnitude maps read + D and S written
+        stencil += n * (8 * 4 + 4)        # 8 magnitude maps read + D written
         nms += n * 4                      # D read once
     return {"gabor": gabor, "stencil": stencil, "nms": nms}
 

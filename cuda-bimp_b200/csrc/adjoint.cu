@@ -210,6 +210,7 @@ struct bimp_adjoint {
     const size_t offXs = take(sizeof(float2) * (size_t)nTiles * kSpecHalf);
     const size_t offLoss = take(sizeof(double) * 8);
     const size_t offMax = take(sizeof(unsigned int) * (sds.size() + 1));
+    const size_t offMaps = take(kTensorMapBytes * sds.size());
     bytes = at;
     cudaError_t e = cudaMalloc(&mem, bytes);
     if (e != cudaSuccess) {
@@ -250,6 +251,13 @@ struct bimp_adjoint {
       d.M = d_M + (size_t)i * maskStride + maskOff[si];
       d.maxKey = d_max + e2;
     }
+    std::vector<TensorMapBlob> maps(sds.size());
+    {
+      std::string err2;
+      if (!encode_c_maps(sds.data(), static_cast<int>(sds.size()), maps.data(), err2))
+        return afail(BIMP_ERR_CUDA, err2);
+      for (size_t e2 = 0; e2 < sds.size(); ++e2) sds[e2].cMap = b + offMaps + e2 * kTensorMapBytes;
+    }
     h_sd = sds;
     d_sd = reinterpret_cast<ScaleDev*>(b + offSd);
     d_tiles = reinterpret_cast<TileWork*>(b + offT2);
@@ -267,6 +275,7 @@ struct bimp_adjoint {
     ADJ_CUDA(cudaMemcpy(dBA, hA.data(), sizeof(float4) * hA.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(dBB, hB.data(), sizeof(float2) * hB.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(d_sd, sds.data(), sizeof(ScaleDev) * sds.size(), cudaMemcpyHostToDevice));
+    ADJ_CUDA(cudaMemcpy(b + offMaps, maps.data(), kTensorMapBytes * sds.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(d_tiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(d_sten, sten.data(), sizeof(int2) * sten.size(), cudaMemcpyHostToDevice));
     ADJ_CUDA(cudaMemcpy(d_stenB, stenB.data(), sizeof(int2) * stenB.size(), cudaMemcpyHostToDevice));
@@ -302,7 +311,7 @@ struct bimp_adjoint {
     ADJ_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int) * (h_sd.size() + 1), s));
     ADJ_CUDA(cudaMemsetAsync(d_loss, 0, sizeof(double) * 5, s));
     launch_gabor_save(d_sd, d_tiles, nTiles, nTiles, d_max + h_sd.size(), d_xsave, s);
-    launch_stencil_adj(d_sd, d_sten, nSten, s);
+    launch_stencil(d_sd, d_sten, nSten, d_max + h_sd.size(), s, kStencilAdj);
     launch_masked_loss(d_sd, d_sten, nSten, d_loss, d_gp, s);
     if (loss) ADJ_CUDA(cudaMemcpyAsync(loss, d_loss, sizeof(double), cudaMemcpyDeviceToDevice, s));
     ADJ_CUDA(cudaGetLastError());

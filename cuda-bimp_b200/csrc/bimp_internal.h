@@ -40,6 +40,7 @@ struct ScaleDev {
   float* C;
   int cPitch;
   long long cStride;
+  const void* cMap;       // 3-D TMA tensor map of C (device memory, 128 B)
   // stencil offsets (cuda_bimp.cu:533-550)
   int es1[kNumOri], es2[kNumOri];   // end-stop (row, col)
   int in1[kNumOri], in2[kNumOri];   // inhibition (row, col)

@@ -284,6 +284,7 @@ struct Engine {
     const size_t offMax = a.reserve(sizeof(unsigned int) * (sds.size() + 1));
     const size_t offOuts = a.reserve(sizeof(KpOut) * n);
     const size_t offPyr = a.reserve(sizeof(PyrJob) * std::max<size_t>(1, h_pyr.size()));
+    const size_t offMaps = a.reserve(kTensorMapBytes * sds.size());
     size_t offKp = 0;
     kpCapInternal = internalKpCap;
     if (internalKpCap > 0)
@@ -319,6 +320,13 @@ struct Engine {
         h_pyr[k].src = lvl[i][l - 1];
         h_pyr[k].dst = lvl[i][l];
       }
+    // TMA tensor maps of the complex-cell maps (the stencil's staging)
+    std::vector<TensorMapBlob> maps(sds.size());
+    {
+      std::string err;
+      if (!encode_c_maps(sds.data(), static_cast<int>(sds.size()), maps.data(), err)) return fail(BIMP_ERR_CUDA, err);
+      for (size_t e2 = 0; e2 < sds.size(); ++e2) sds[e2].cMap = base + offMaps + e2 * kTensorMapBytes;
+    }
     h_sd = sds;
     d_sd = reinterpret_cast<ScaleDev*>(base + offSd);
     d_tiles = reinterpret_cast<TileWork*>(base + offTiles);
@@ -340,6 +348,7 @@ struct Engine {
                            sizeof(float) * kNumOri * kSpecFloats, cudaMemcpyHostToDevice));
     for (auto& s : bank) { s.spectrum.clear(); s.spectrum.shrink_to_fit(); }
     BIMP_CUDA(cudaMemcpy(d_sd, sds.data(), sizeof(ScaleDev) * sds.size(), cudaMemcpyHostToDevice));
+    BIMP_CUDA(cudaMemcpy(base + offMaps, maps.data(), kTensorMapBytes * sds.size(), cudaMemcpyHostToDevice));
     if (!tiles.empty())
       BIMP_CUDA(cudaMemcpy(d_tiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice));
     if (!sten.empty())
@@ -374,7 +383,7 @@ struct Engine {
         if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s);
         break;
       case 2:
-        if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, s);
+        if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD);
         break;
       case 3:
         launch_nms(d_sd, d_rows, nRows, d_counts, d_offsets, d_imgRowStart, nImages, d_totals, d_outs, s);
@@ -635,10 +644,18 @@ int bimp_dense_map(bimp_context* c, int scale, int which, float* d_out, size_t l
   const ScaleDev& d = c->eng.h_sd[scale];
   if (ld < (size_t)d.dataW) return fail(BIMP_ERR_INVALID, "ld smaller than data width");
   BIMP_CUDA(cudaSetDevice(c->eng.device));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (which == 1) {
+    // S is not on the keypoint path: detection writes D only, and the
+    // single-stopped map is computed here from the last detection's complex
+    // cells (the same stencil pass, which rewrites D with identical values)
+    if (c->eng.nSten > 0)
+      launch_stencil(c->eng.d_sd, c->eng.d_sten, c->eng.nSten, c->eng.d_fault, s, kStencilDS);
+    BIMP_CUDA(cudaGetLastError());
+  }
   const float* src = which == 0 ? d.D : d.S;
   BIMP_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), src, d.dPitch * sizeof(float),
-                              d.dataW * sizeof(float), d.dataH, cudaMemcpyDeviceToDevice,
-                              static_cast<cudaStream_t>(stream)));
+                              d.dataW * sizeof(float), d.dataH, cudaMemcpyDeviceToDevice, s));
   return BIMP_OK;
 }
 

@@ -10,6 +10,8 @@
 //   k_nms_count     strict 8-neighbour maxima above 0.104*max per row
 //   k_scan          exclusive scan of the row counts
 //   k_nms_write     keypoint records in (scale, y, x) order
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -129,11 +131,13 @@ __device__ __forceinline__ int soff(const StencilPar& P, int k, int o) {
 // The double-stopped term c - 0.5 a - 0.5 b, which the reference evaluates
 // in double and rounds once, is two fused float multiply-adds here (at most
 // one float rounding apart).
-// ADJ (the differentiable forward) also returns the tangential and radial
-// sums T, R and the ReLU states the adjoint needs: per orientation o, bit 4o
-// double-stopped d > 0, 4o+1 tangential t > 0, 4o+2 radial r > 0, 4o+3 the
-// first radial term r1 > 0 (all 0 where the bounds test fails).
-template <bool CHECK, int PAT, bool ADJ>
+// Stencil modes: detection writes D only (the single-stopped map S is not on
+// the keypoint path); responses write D and S; the differentiable forward
+// writes D, the tangential and radial sums T, R and the ReLU states the
+// adjoint needs: per orientation o, bit 4o double-stopped d > 0, 4o+1
+// tangential t > 0, 4o+2 radial r > 0, 4o+3 the first radial term r1 > 0
+// (all 0 where the bounds test fails).
+template <bool CHECK, int PAT, int MODE>
 __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, const StencilPar& P, int x, int y,
                                               int cy, int cx, float gain, float wT, float wR, float& Dout,
                                               float& Sout, float& Tout, float& Rout, unsigned int& bits) {
@@ -145,15 +149,10 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
     if (CHECK && !(x >= P.exlo[o] && x <= P.exhi[o] && y >= P.eylo[o] && y <= P.eyhi[o])) continue;
     const int o1 = soff<PAT>(P, 0, o), o2 = soff<PAT>(P, 1, o);
     const float* c = c0 + o * (kStH * kStW);
-    if constexpr (!ADJ) {
-      float s = c[-o1 * kStW + o2] - c[o1 * kStW - o2];
-      s = s > 0.f ? s : 0.f;
-      if (s > 0.f) S += s;
-    }
-    float d = fmaf(-0.5f, c[2 * o1 * kStW - 2 * o2], fmaf(-0.5f, c[-2 * o1 * kStW + 2 * o2], c[0]));
-    if constexpr (ADJ) b |= (d > 0.f ? 1u : 0u) << (4 * o);
-    d = d > 0.f ? d : 0.f;
-    if (d > 0.f) D += d;
+    if constexpr (MODE == kStencilDS) S += fmaxf(c[-o1 * kStW + o2] - c[o1 * kStW - o2], 0.f);
+    const float d = fmaf(-0.5f, c[2 * o1 * kStW - 2 * o2], fmaf(-0.5f, c[-2 * o1 * kStW + 2 * o2], c[0]));
+    if constexpr (MODE == kStencilAdj) b |= (d > 0.f ? 1u : 0u) << (4 * o);
+    D += fmaxf(d, 0.f);
   }
 #pragma unroll
   for (int o = 0; o < kNumOri; ++o) {
@@ -162,31 +161,28 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
     const float* c = c0 + o * (kStH * kStW);
     const float* cp = c0 + ((o + kNumOri / 2) % kNumOri) * (kStH * kStW);
     const float centre = c[0];
-    float v = c[-o1 * kStW - o2] - centre;
-    if constexpr (ADJ) b |= (v > 0.f ? 2u : 0u) << (4 * o);
-    v = v < 0.f ? 0.f : v;
-    T += v;
+    const float v = c[-o1 * kStW - o2] - centre;
+    if constexpr (MODE == kStencilAdj) b |= (v > 0.f ? 2u : 0u) << (4 * o);
+    T += fmaxf(v, 0.f);
     const int h1 = soff<PAT>(P, 4, o), h2 = soff<PAT>(P, 5, o);
     float r = centre - gain * cp[h1 * kStW + h2];
-    if constexpr (ADJ) b |= (r > 0.f ? 8u : 0u) << (4 * o);
-    r = r < 0.f ? 0.f : r;
+    if constexpr (MODE == kStencilAdj) b |= (r > 0.f ? 8u : 0u) << (4 * o);
+    r = fmaxf(r, 0.f);
     r += centre - gain * cp[-h1 * kStW - h2];
-    if constexpr (ADJ) b |= (r > 0.f ? 4u : 0u) << (4 * o);
-    r = r < 0.f ? 0.f : r;
-    R += r;
+    if constexpr (MODE == kStencilAdj) b |= (r > 0.f ? 4u : 0u) << (4 * o);
+    R += fmaxf(r, 0.f);
   }
   const float inhib = wT * T + wR * R;
   Dout = D + (-inhib);
   Sout = S + (-inhib);
-  if constexpr (ADJ) {
+  if constexpr (MODE == kStencilAdj) {
     Tout = T;
     Rout = R;
     bits = b;
   }
 }
 
-// Output maps of one stencil block: D and S, or for ADJ D, T, R and the
-// ReLU-state words.
+// Output maps of one stencil block.
 struct StencilOut {
   float* D;
   float* S;
@@ -196,7 +192,7 @@ struct StencilOut {
   int pitch;
 };
 
-template <int PAT, bool ADJ, int NT>
+template <int PAT, int MODE, int NT>
 __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, const StencilPar& P, int x0, int y0,
                                                int W, int H, float gain, float wT, float wR, const StencilOut& out) {
   const int t = threadIdx.x;
@@ -213,17 +209,16 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
     float D, S, T, R;
     unsigned int b;
     if (inner)
-      stencil_pixel<false, PAT, ADJ>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S, T, R, b);
+      stencil_pixel<false, PAT, MODE>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S, T, R, b);
     else
-      stencil_pixel<true, PAT, ADJ>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S, T, R, b);
+      stencil_pixel<true, PAT, MODE>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S, T, R, b);
     const size_t k = (size_t)y * out.pitch + x;
     out.D[k] = D;
-    if constexpr (ADJ) {
+    if constexpr (MODE == kStencilDS) out.S[k] = S;
+    if constexpr (MODE == kStencilAdj) {
       out.T[k] = T;
       out.R[k] = R;
       out.bits[k] = b;
-    } else {
-      out.S[k] = S;
     }
     dmax = fmaxf(dmax, D);
   }
@@ -231,19 +226,15 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
 }
 
 // Persistent stencil kernel: one CTA of 512 threads per SM walks the block
-// list; while it computes block k from one staging buffer, the copies of
-// block k + 1's complex-cell window (8 orientations x 48 x 48 floats, the
-// 32 x 32 block plus an 8-pixel halo) land in the other through cp.async.
-// Chunks of the window outside the map's allocation are not copied: the
-// bounds test keeps every stencil read inside [0, dataW] x [0, dataH].
+// list.  While it computes block k from one staging buffer, block k + 1's
+// complex-cell window (8 orientations x 48 rows x 48 floats: the 32 x 32
+// block plus an 8-pixel halo) lands in the other as one TMA tensor box,
+// completion counted on the buffer's mbarrier.  Every mbarrier wait is
+// bounded; on expiry the kernel sets *fault, lets its copies land (bounded)
+// and stops.
 constexpr int kStThreads = 512;
 constexpr int kStBuf = kNumOri * kStH * kStW;    // floats per staging buffer
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+constexpr int kStRows = kNumOri * kStH;          // window rows per buffer (384)
 
 __device__ __forceinline__ void block_origin(const ScaleDev* sd, int blk, int& x0, int& y0) {
   const int nbx = (sd->dataW + kStX - 1) / kStX;
@@ -263,44 +254,50 @@ __device__ __forceinline__ void stencil_params(const ScaleDev* sd, StencilPar& P
   P.iylo[o] = 2 * abs(i1); P.iyhi[o] = H - 2 * abs(i1);
 }
 
-// Issue the 16-byte copies of one block's window into buf.  The window's
-// first column x0 - 8 is 16-byte aligned (x0 is a multiple of 32, the pitch
-// a multiple of 32 floats).
-__device__ __forceinline__ void stencil_stage(const ScaleDev* sd, int x0, int y0, float* buf, int t) {
-  const float* __restrict__ C = sd->C;
-  const int cPitch = sd->cPitch, cRows = sd->cRows;
-  const long long cStride = sd->cStride;
-  const int gx0 = x0 - kHalo, gy0 = y0 - kHalo;
-  constexpr int kV = kStW / 4;
-#pragma unroll 3
-  for (int idx = t; idx < kNumOri * kStH * kV; idx += kStThreads) {
-    const int row = idx / kV, v4 = idx - row * kV;
-    const int o = row / kStH, ly = row - o * kStH;
-    const int gy = gy0 + ly, gx = gx0 + 4 * v4;
-    if (gy >= 0 && gy < cRows && gx >= 0 && gx + 4 <= cPitch)
-      cp_async16(buf + row * kStW + 4 * v4, C + (size_t)o * cStride + (size_t)gy * cPitch + gx);
-  }
+// One thread: the block's window as one TMA box (48 x 48 x 8 floats at
+// x0 - 8, y0 - 8) through the entry's tensor map.  x0 - 8 is a multiple of 4
+// floats (16 bytes); parts of the box outside the maps read as zero.
+__device__ __forceinline__ void stencil_stage_tma(const ScaleDev* sd, int x0, int y0, float* buf, uint32_t bar) {
+  fence_proxy_async();   // the buffer was last read (and patched) through the generic proxy
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((uint32_t)(kStBuf * 4))
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(smem_u32(buf)),
+      "l"(sd->cMap), "r"(x0 - kHalo), "r"(y0 - kHalo), "r"(0), "r"(bar)
+      : "memory");
 }
 
-template <bool ADJ>
+template <int MODE>
 __global__ void __launch_bounds__(kStThreads, 1)
-k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int nwork) {
-  extern __shared__ float4 s_c4[];   // 2 buffers of kNumOri x kStH x kStW floats
-  float* s_buf = reinterpret_cast<float*>(s_c4);
+k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int nwork,
+          unsigned int* __restrict__ fault_word) {
+  extern __shared__ float4 s_c4[];   // 2 buffers of kNumOri x kStH x kStW floats (+128 B for alignment)
+  // TMA box destinations are 128-byte aligned
+  float* s_buf = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(s_c4) + 127) & ~uintptr_t(127));
   __shared__ StencilPar P[2];
-  const int t = threadIdx.x;
+  __shared__ __align__(8) uint64_t s_bar[2];
+  const int t = threadIdx.x, lane = t & 31;
   int w = blockIdx.x;
   if (w >= nwork) return;
+  const uint32_t bar0 = smem_u32(&s_bar[0]), bar1 = smem_u32(&s_bar[1]);
+  if (t == 0) {
+    mbar_init(bar0);
+    mbar_init(bar1);
+    fence_mbar_init();
+  }
+  __syncthreads();
   {
     const int2 item = work[w];
     const ScaleDev* sd = sds + item.x;
     int x0, y0;
     block_origin(sd, item.y, x0, y0);
     if (t < kNumOri) stencil_params(sd, P[0], t);
-    stencil_stage(sd, x0, y0, s_buf, t);
+    if (t == 0) stencil_stage_tma(sd, x0, y0, s_buf, bar0);
   }
-  cp_async_commit();
-  for (int k = 0; w < nwork; ++k, w += gridDim.x) {
+  bool fault = false;
+  int k = 0;
+  for (; w < nwork; ++k, w += gridDim.x) {
     const int cur = k & 1;
     const int wn = w + gridDim.x;
     if (wn < nwork) {   // the next block's window goes into the other buffer
@@ -309,11 +306,13 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
       int nx0, ny0;
       block_origin(sdn, nx.y, nx0, ny0);
       if (t < kNumOri) stencil_params(sdn, P[cur ^ 1], t);
-      stencil_stage(sdn, nx0, ny0, s_buf + (cur ^ 1) * kStBuf, t);
+      if (t == 0) stencil_stage_tma(sdn, nx0, ny0, s_buf + (cur ^ 1) * kStBuf, cur ? bar0 : bar1);
     }
-    cp_async_commit();
-    cp_async_wait_prev();   // this block's copies (every group but the newest) have landed
-    __syncthreads();
+    const bool expired = !mbar_wait(cur ? bar1 : bar0, (k >> 1) & 1);
+    if (__syncthreads_or(expired)) {   // also the barrier that makes P[cur] visible
+      fault = true;
+      break;
+    }
     const int2 item = work[w];
     const ScaleDev* __restrict__ sd = sds + item.x;
     const int W = sd->dataW, H = sd->dataH;
@@ -325,7 +324,7 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
     const int lxW = W - (x0 - kHalo);
     if (sd->wrapW && lxW >= 0 && lxW < kStW) {
       const float* __restrict__ C = sd->C;
-      for (int idx = t; idx < kNumOri * kStH; idx += kStThreads) {
+      for (int idx = t; idx < kStRows; idx += kStThreads) {
         const int o = idx / kStH, ly = idx - o * kStH;
         const int gy = y0 - kHalo + ly;
         if (gy >= 0 && gy <= H) s_c[idx * kStW + lxW] = C[(size_t)o * sd->cStride + (size_t)(gy + 1) * sd->cPitch];
@@ -342,16 +341,24 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
     const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
     float dmax;
     if (sd->pattern == 1)
-      dmax = stencil_block<1, ADJ, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
+      dmax = stencil_block<1, MODE, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
     else if (sd->pattern == 2)
-      dmax = stencil_block<2, ADJ, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
+      dmax = stencil_block<2, MODE, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
     else
-      dmax = stencil_block<0, ADJ, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
+      dmax = stencil_block<0, MODE, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
     // map max: one atomic per warp
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
-    if ((t & 31) == 0 && dmax > -INFINITY) atomicMax(sd->maxKey, float_key(dmax));
+    if (lane == 0 && dmax > -INFINITY) atomicMax(sd->maxKey, float_key(dmax));
     __syncthreads();   // buffer cur and P[cur] are refilled in the next iteration
+  }
+  if (fault) {
+    // a wait expired: record it and give the copies in flight (the current
+    // buffer's and possibly the next one's) a second bounded chance to land
+    // before the CTA releases its shared memory
+    if (t == 0) atomicOr(fault_word, 2u);
+    mbar_wait(k & 1 ? bar1 : bar0, (k >> 1) & 1);
+    mbar_wait(k & 1 ? bar0 : bar1, ((k + 1) >> 1) & 1);
   }
 }
 
@@ -530,7 +537,46 @@ cudaError_t upload_twiddles() {
 }
 
 size_t gabor_smem_bytes() { return kGaborSmem; }
-size_t stencil_smem_bytes() { return sizeof(float) * 2 * kStBuf; }
+size_t stencil_smem_bytes() { return sizeof(float) * 2 * kStBuf + 128; }
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+}  // namespace
+
+bool encode_c_maps(const ScaleDev* sds, int n, void* maps, std::string& err) {
+  static_assert(sizeof(CUtensorMap) == kTensorMapBytes, "tensor map size");
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) {
+    err = "cuTensorMapEncodeTiled is not available from the driver";
+    return false;
+  }
+  CUtensorMap* out = static_cast<CUtensorMap*>(maps);
+  for (int e = 0; e < n; ++e) {
+    const ScaleDev& d = sds[e];
+    const cuuint64_t dims[3] = {(cuuint64_t)d.cPitch, (cuuint64_t)d.cRows, (cuuint64_t)kNumOri};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.cPitch * sizeof(float), (cuuint64_t)d.cStride * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)kStW, (cuuint32_t)kStH, (cuuint32_t)kNumOri};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    const CUresult r = enc(&out[e], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, d.C, dims, strides, box, elem,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      err = "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r);
+      return false;
+    }
+  }
+  return true;
+}
 
 // CTAs of the persistent stencil kernel: one per SM.
 static int g_num_sms[64] = {0};
@@ -550,8 +596,9 @@ cudaError_t configure_kernels() {
   const cudaFuncAttribute big = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaFuncSetAttribute(k_gabor_tiles<false, false>, big, (int)gabor_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles<true, true>, big, (int)gabor_smem_bytes());
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<false>, big, (int)stencil_smem_bytes());
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<true>, big, (int)stencil_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilD>, big, (int)stencil_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilDS>, big, (int)stencil_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilAdj>, big, (int)stencil_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles_bwd, big, (int)kGaborBwdSmem);
   if (e != cudaSuccess) return e;
   return upload_twiddles();
@@ -591,13 +638,16 @@ void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, i
   if (nwork > 0)
     k_gabor_tiles_bwd<<<grid, kTileThreads, kGaborBwdSmem, s>>>(d_sd, d_work, nwork, d_xsave, d_gparams);
 }
-void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
-  if (nwork > 0)
-    k_stencil<false><<<std::min(nwork, num_sms()), kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork);
-}
-void launch_stencil_adj(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
-  if (nwork > 0)
-    k_stencil<true><<<std::min(nwork, num_sms()), kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork);
+void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigned int* d_fault, cudaStream_t s,
+                    int mode) {
+  if (nwork <= 0) return;
+  const int grid = std::min(nwork, num_sms());
+  if (mode == kStencilDS)
+    k_stencil<kStencilDS><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+  else if (mode == kStencilAdj)
+    k_stencil<kStencilAdj><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+  else
+    k_stencil<kStencilD><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
 }
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,

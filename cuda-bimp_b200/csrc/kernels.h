@@ -1,6 +1,8 @@
 // Launch interface of the BIMP kernels (kernels.cu).
 #pragma once
 
+#include <string>
+
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -42,7 +44,22 @@ void launch_pyr(const PyrJob* d_jobs, int njobs, int maxW, int maxH, cudaStream_
 // d_fault: word that receives 1 if a bounded device wait expired.
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                   cudaStream_t s);
-void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
+// One TMA tensor map per scale entry over its complex-cell maps (x: cPitch
+// columns, y: cRows rows, z: the 8 orientations; box 48 x 48 x 8 floats,
+// zero fill outside), written to maps[e] (128-byte CUtensorMap blobs).
+constexpr size_t kTensorMapBytes = 128;
+struct alignas(64) TensorMapBlob {
+  unsigned char bytes[kTensorMapBytes];
+};
+bool encode_c_maps(const ScaleDev* sds, int n, void* maps, std::string& err);
+
+// Stencil output modes: D only (detection), D and S (responses), and the
+// differentiable forward (D, T, R, ReLU states).
+enum StencilMode { kStencilD = 0, kStencilDS = 1, kStencilAdj = 2 };
+// Persistent stencil (one CTA per SM); an expired staging wait sets bit 1 of
+// *d_fault.
+void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigned int* d_fault, cudaStream_t s,
+                    int mode = kStencilD);
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,
                 cudaStream_t s);
@@ -55,8 +72,6 @@ void launch_pyr_f_adj(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cuda
 // d_xsave + w * kSpecHalf)
 void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                        float2* d_xsave, cudaStream_t s);
-// differentiable forward stencil: D, T, R and the ReLU states (ScaleDev::bits)
-void launch_stencil_adj(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
 void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, double* d_gparams,
                         cudaStream_t s);
 void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
