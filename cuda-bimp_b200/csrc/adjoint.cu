@@ -417,9 +417,6 @@ int bimp_adjoint_complex_map(bimp_adjoint* a, int image, int scale, int orientat
   const float* src = d.C + (size_t)orientation * d.cStride;
   ADJ_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), src, d.cPitch * sizeof(float), d.cCols * sizeof(float),
                              d.dataH + 1, cudaMemcpyDeviceToDevice, s));
-  if (d.wrapW)   // column dataW of the window is the torus element (r + 1, 0)
-    ADJ_CUDA(cudaMemcpy2DAsync(d_out + d.dataW, ld * sizeof(float), src + d.cPitch, d.cPitch * sizeof(float),
-                               sizeof(float), d.dataH + 1, cudaMemcpyDeviceToDevice, s));
   return BIMP_OK;
 }
 

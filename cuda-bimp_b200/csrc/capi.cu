@@ -669,13 +669,6 @@ int bimp_complex_map(bimp_context* c, int scale, int o, float* d_out, size_t ld,
   const float* src = d.C + (size_t)o * d.cStride;
   BIMP_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), src, d.cPitch * sizeof(float),
                               d.cCols * sizeof(float), d.dataH + 1, cudaMemcpyDeviceToDevice, s));
-  if (d.wrapW) {
-    // the stencils address y*fftW + x: with fftW == dataW, column dataW is
-    // the next row's column 0
-    BIMP_CUDA(cudaMemcpy2DAsync(d_out + d.dataW, ld * sizeof(float), src + d.cPitch,
-                                d.cPitch * sizeof(float), sizeof(float), d.dataH + 1,
-                                cudaMemcpyDeviceToDevice, s));
-  }
   return BIMP_OK;
 }
 

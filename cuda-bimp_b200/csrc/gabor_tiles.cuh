@@ -224,6 +224,8 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     }
 
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
+    // tiles holding window column 0 or column dataW of a map with fftW == dataW
+    const bool wrapTile = sd->wrapW != 0 && (C0 == 0 || C0 + V >= cCols);
     float* __restrict__ C0p = sd->C;
     float2* __restrict__ Z0p = sd->Z;
     const long long cStride = sd->cStride;
@@ -288,13 +290,36 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         const int gy = R0 + y - kX;
         if (gy < cRows) {
           float* dst = Cout + (size_t)gy * cPitch;
+          if (!wrapTile) {
 #pragma unroll
-          for (int n2 = 0; n2 < 16; ++n2) {
-            const int x = n1 + 8 * n2;
-            const int gx = C0 + x - kX;
-            if (x >= kX && x < kX + V && gx < cCols) {
-              dst[gx] = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
-              if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)gy * cPitch + gx] = v[n2];
+            for (int n2 = 0; n2 < 16; ++n2) {
+              const int x = n1 + 8 * n2;
+              const int gx = C0 + x - kX;
+              if (x >= kX && x < kX + V && gx < cCols) {
+                dst[gx] = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
+                if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)gy * cPitch + gx] = v[n2];
+              }
+            }
+          } else {
+            // fftW == dataW: the stencils read window column dataW of row r
+            // at the flat address r*fftW + fftW, the torus element (r + 1, 0),
+            // so that element also goes to (r, dataW); the window's own
+            // (r, dataW) output is kept only on the last row
+#pragma unroll
+            for (int n2 = 0; n2 < 16; ++n2) {
+              const int x = n1 + 8 * n2;
+              const int gx = C0 + x - kX;
+              if (x >= kX && x < kX + V && gx < cCols) {
+                const float m = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
+                if (!(gx == cCols - 1 && gy < cRows - 1)) {
+                  dst[gx] = m;
+                  if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)gy * cPitch + gx] = v[n2];
+                }
+                if (gx == 0 && gy >= 1) {
+                  Cout[(size_t)(gy - 1) * cPitch + cCols - 1] = m;
+                  if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)(gy - 1) * cPitch + cCols - 1] = v[n2];
+                }
+              }
             }
           }
         }

@@ -225,16 +225,26 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
   return dmax;
 }
 
-// Persistent stencil kernel: one CTA of 512 threads per SM walks the block
-// list.  While it computes block k from one staging buffer, block k + 1's
-// complex-cell window (8 orientations x 48 rows x 48 floats: the 32 x 32
-// block plus an 8-pixel halo) lands in the other as one TMA tensor box,
-// completion counted on the buffer's mbarrier.  Every mbarrier wait is
-// bounded; on expiry the kernel sets *fault, lets its copies land (bounded)
-// and stops.
-constexpr int kStThreads = 512;
-constexpr int kStBuf = kNumOri * kStH * kStW;    // floats per staging buffer
-constexpr int kStRows = kNumOri * kStH;          // window rows per buffer (384)
+// Persistent, warp-specialised stencil kernel: one CTA per SM walks the block
+// list.  A producer warp stages block k + 1's complex-cell window (8
+// orientations x 48 rows x 48 floats: the 32 x 32 block plus an 8-pixel halo)
+// as one TMA tensor box into the free one of two buffers, with the block's
+// parameters, while 16 consumer warps compute block k from the other.  Full
+// barriers (TMA bytes) and empty barriers (one arrival per consumer warp)
+// order the two sides; there is no CTA-wide barrier in the loop.  Every wait
+// is bounded; on expiry the kernel sets *fault and stops.
+constexpr int kStConsumers = 512;                    // 16 compute warps
+constexpr int kStThreads = kStConsumers + 32;        // + the producer warp
+constexpr int kStBuf = kNumOri * kStH * kStW;        // floats per staging buffer
+
+// Everything a consumer needs about its block, written by the producer.
+struct StencilBlk {
+  StencilPar P;
+  int x0, y0, W, H, pattern;
+  float gain, wT, wR;
+  StencilOut out;
+  unsigned int* maxKey;
+};
 
 __device__ __forceinline__ void block_origin(const ScaleDev* sd, int blk, int& x0, int& y0) {
   const int nbx = (sd->dataW + kStX - 1) / kStX;
@@ -243,22 +253,34 @@ __device__ __forceinline__ void block_origin(const ScaleDev* sd, int blk, int& x
   y0 = by * kStY;
 }
 
-__device__ __forceinline__ void stencil_params(const ScaleDev* sd, StencilPar& P, int o) {
+// Lane `lane` (< 8: orientation lane) of the producer fills the block record.
+__device__ __forceinline__ void stencil_record(const ScaleDev* sd, int x0, int y0, StencilBlk& B, int lane) {
   const int W = sd->dataW, H = sd->dataH;
-  const int e1 = sd->es1[o], e2 = sd->es2[o], i1 = sd->in1[o], i2 = sd->in2[o];
-  P.e1[o] = e1; P.e2[o] = e2; P.i1[o] = i1; P.i2[o] = i2;
-  P.h1[o] = sd->ih1[o]; P.h2[o] = sd->ih2[o];
-  P.exlo[o] = 2 * abs(e2); P.exhi[o] = W - 2 * abs(e2);
-  P.eylo[o] = 2 * abs(e1); P.eyhi[o] = H - 2 * abs(e1);
-  P.ixlo[o] = 2 * abs(i2); P.ixhi[o] = W - 2 * abs(i2);
-  P.iylo[o] = 2 * abs(i1); P.iyhi[o] = H - 2 * abs(i1);
+  if (lane < kNumOri) {
+    const int o = lane;
+    StencilPar& P = B.P;
+    const int e1 = sd->es1[o], e2 = sd->es2[o], i1 = sd->in1[o], i2 = sd->in2[o];
+    P.e1[o] = e1; P.e2[o] = e2; P.i1[o] = i1; P.i2[o] = i2;
+    P.h1[o] = sd->ih1[o]; P.h2[o] = sd->ih2[o];
+    P.exlo[o] = 2 * abs(e2); P.exhi[o] = W - 2 * abs(e2);
+    P.eylo[o] = 2 * abs(e1); P.eyhi[o] = H - 2 * abs(e1);
+    P.ixlo[o] = 2 * abs(i2); P.ixhi[o] = W - 2 * abs(i2);
+    P.iylo[o] = 2 * abs(i1); P.iyhi[o] = H - 2 * abs(i1);
+  } else if (lane == kNumOri) {
+    B.x0 = x0; B.y0 = y0; B.W = W; B.H = H; B.pattern = sd->pattern;
+    B.gain = sd->radialGain; B.wT = sd->wTan; B.wR = sd->wRad;
+    B.out.D = sd->D; B.out.S = sd->S; B.out.T = sd->T; B.out.R = sd->R; B.out.bits = sd->bits;
+    B.out.pitch = sd->dPitch;
+    B.maxKey = sd->maxKey;
+  }
 }
 
 // One thread: the block's window as one TMA box (48 x 48 x 8 floats at
 // x0 - 8, y0 - 8) through the entry's tensor map.  x0 - 8 is a multiple of 4
-// floats (16 bytes); parts of the box outside the maps read as zero.
+// floats (16 bytes); parts of the box outside the maps read as zero.  The
+// arrive releases the block record written before it.
 __device__ __forceinline__ void stencil_stage_tma(const ScaleDev* sd, int x0, int y0, float* buf, uint32_t bar) {
-  fence_proxy_async();   // the buffer was last read (and patched) through the generic proxy
+  fence_proxy_async();   // the buffer was last read through the generic proxy
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((uint32_t)(kStBuf * 4))
                : "memory");
   asm volatile(
@@ -268,6 +290,13 @@ __device__ __forceinline__ void stencil_stage_tma(const ScaleDev* sd, int x0, in
       : "memory");
 }
 
+__device__ __forceinline__ void mbar_init_count(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kStThreads, 1)
 k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int nwork,
@@ -275,90 +304,71 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
   extern __shared__ float4 s_c4[];   // 2 buffers of kNumOri x kStH x kStW floats (+128 B for alignment)
   // TMA box destinations are 128-byte aligned
   float* s_buf = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(s_c4) + 127) & ~uintptr_t(127));
-  __shared__ StencilPar P[2];
-  __shared__ __align__(8) uint64_t s_bar[2];
-  const int t = threadIdx.x, lane = t & 31;
-  int w = blockIdx.x;
-  if (w >= nwork) return;
-  const uint32_t bar0 = smem_u32(&s_bar[0]), bar1 = smem_u32(&s_bar[1]);
+  __shared__ StencilBlk blk[2];
+  __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if ((int)blockIdx.x >= nwork) return;
+  const uint32_t full0 = smem_u32(&s_full[0]), full1 = smem_u32(&s_full[1]);
+  const uint32_t empty0 = smem_u32(&s_empty[0]), empty1 = smem_u32(&s_empty[1]);
   if (t == 0) {
-    mbar_init(bar0);
-    mbar_init(bar1);
+    mbar_init_count(full0, 1);
+    mbar_init_count(full1, 1);
+    mbar_init_count(empty0, kStConsumers / 32);
+    mbar_init_count(empty1, kStConsumers / 32);
     fence_mbar_init();
   }
   __syncthreads();
-  {
-    const int2 item = work[w];
-    const ScaleDev* sd = sds + item.x;
-    int x0, y0;
-    block_origin(sd, item.y, x0, y0);
-    if (t < kNumOri) stencil_params(sd, P[0], t);
-    if (t == 0) stencil_stage_tma(sd, x0, y0, s_buf, bar0);
-  }
-  bool fault = false;
-  int k = 0;
-  for (; w < nwork; ++k, w += gridDim.x) {
-    const int cur = k & 1;
-    const int wn = w + gridDim.x;
-    if (wn < nwork) {   // the next block's window goes into the other buffer
-      const int2 nx = work[wn];
-      const ScaleDev* sdn = sds + nx.x;
-      int nx0, ny0;
-      block_origin(sdn, nx.y, nx0, ny0);
-      if (t < kNumOri) stencil_params(sdn, P[cur ^ 1], t);
-      if (t == 0) stencil_stage_tma(sdn, nx0, ny0, s_buf + (cur ^ 1) * kStBuf, cur ? bar0 : bar1);
+  const int nk = (nwork - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;   // blocks of this CTA
+  if (warp == kStConsumers / 32) {
+    // producer warp
+    int issued = 0;
+    bool expired = false;
+    for (int k = 0; k < nk; ++k) {
+      const int b = k & 1, u = k >> 1;
+      if (u >= 1 && !mbar_wait(b ? empty1 : empty0, (u - 1) & 1)) {   // consumers released use u - 1
+        expired = true;
+        break;
+      }
+      const int2 item = work[blockIdx.x + k * gridDim.x];
+      const ScaleDev* sd = sds + item.x;
+      int x0, y0;
+      block_origin(sd, item.y, x0, y0);
+      stencil_record(sd, x0, y0, blk[b], lane);
+      __syncwarp();
+      if (lane == 0) stencil_stage_tma(sd, x0, y0, s_buf + b * kStBuf, b ? full1 : full0);
+      __syncwarp();
+      issued = k + 1;
     }
-    const bool expired = !mbar_wait(cur ? bar1 : bar0, (k >> 1) & 1);
-    if (__syncthreads_or(expired)) {   // also the barrier that makes P[cur] visible
-      fault = true;
+    if (expired && lane == 0) atomicOr(fault_word, 2u);
+    // before the CTA can end, the last copies into each buffer must land
+    if (lane == 0) {
+      if (issued >= 1) mbar_wait(((issued - 1) & 1) ? full1 : full0, ((issued - 1) >> 1) & 1);
+      if (issued >= 2) mbar_wait(((issued - 2) & 1) ? full1 : full0, ((issued - 2) >> 1) & 1);
+    }
+    return;
+  }
+  // consumer warps
+  for (int k = 0; k < nk; ++k) {
+    const int b = k & 1, u = k >> 1;
+    if (!mbar_wait(b ? full1 : full0, u & 1)) {
+      if (lane == 0) atomicOr(fault_word, 2u);
       break;
     }
-    const int2 item = work[w];
-    const ScaleDev* __restrict__ sd = sds + item.x;
-    const int W = sd->dataW, H = sd->dataH;
-    int x0, y0;
-    block_origin(sd, item.y, x0, y0);
-    float* s_c = s_buf + cur * kStBuf;
-    // fftW == dataW: the stencils' flat address of column dataW is the next
-    // row's column 0 (y*fftW + fftW)
-    const int lxW = W - (x0 - kHalo);
-    if (sd->wrapW && lxW >= 0 && lxW < kStW) {
-      const float* __restrict__ C = sd->C;
-      for (int idx = t; idx < kStRows; idx += kStThreads) {
-        const int o = idx / kStH, ly = idx - o * kStH;
-        const int gy = y0 - kHalo + ly;
-        if (gy >= 0 && gy <= H) s_c[idx * kStW + lxW] = C[(size_t)o * sd->cStride + (size_t)(gy + 1) * sd->cPitch];
-      }
-      __syncthreads();
-    }
-    StencilOut out;
-    out.D = sd->D;
-    out.S = sd->S;
-    out.T = sd->T;
-    out.R = sd->R;
-    out.bits = sd->bits;
-    out.pitch = sd->dPitch;
-    const float gain = sd->radialGain, wT = sd->wTan, wR = sd->wRad;
+    const StencilBlk& B = blk[b];
+    const float* s_c = s_buf + b * kStBuf;
     float dmax;
-    if (sd->pattern == 1)
-      dmax = stencil_block<1, MODE, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
-    else if (sd->pattern == 2)
-      dmax = stencil_block<2, MODE, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
+    if (B.pattern == 1)
+      dmax = stencil_block<1, MODE, kStConsumers>(s_c, B.P, B.x0, B.y0, B.W, B.H, B.gain, B.wT, B.wR, B.out);
+    else if (B.pattern == 2)
+      dmax = stencil_block<2, MODE, kStConsumers>(s_c, B.P, B.x0, B.y0, B.W, B.H, B.gain, B.wT, B.wR, B.out);
     else
-      dmax = stencil_block<0, MODE, kStThreads>(s_c, P[cur], x0, y0, W, H, gain, wT, wR, out);
+      dmax = stencil_block<0, MODE, kStConsumers>(s_c, B.P, B.x0, B.y0, B.W, B.H, B.gain, B.wT, B.wR, B.out);
     // map max: one atomic per warp
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
-    if (lane == 0 && dmax > -INFINITY) atomicMax(sd->maxKey, float_key(dmax));
-    __syncthreads();   // buffer cur and P[cur] are refilled in the next iteration
-  }
-  if (fault) {
-    // a wait expired: record it and give the copies in flight (the current
-    // buffer's and possibly the next one's) a second bounded chance to land
-    // before the CTA releases its shared memory
-    if (t == 0) atomicOr(fault_word, 2u);
-    mbar_wait(k & 1 ? bar1 : bar0, (k >> 1) & 1);
-    mbar_wait(k & 1 ? bar0 : bar1, ((k + 1) >> 1) & 1);
+    if (lane == 0 && dmax > -INFINITY) atomicMax(B.maxKey, float_key(dmax));
+    __syncwarp();
+    if (lane == 0) mbar_arrive(b ? empty1 : empty0);   // this warp is done with buffer b and blk[b]
   }
 }
 
