@@ -58,6 +58,8 @@ struct ScaleDev {
   int kpOctave;           // (int)(lambda*pyrstep)
   double threshRatio;     // double, as the reference multiplies max by the literal 0.104
   int rowBase;            // first entry of this scale in the per-row count array
+  unsigned int* nmsMask;  // keypoint decisions per candidate row, nmsChunks words of 32 pixels (or null)
+  int nmsChunks;
   int image;              // image index inside a batch
   int pattern;            // stencil offsets: 0 = runtime, k > 0 = kOffsetSets[k-1]
   // differentiable path (float pyramid, saved responses, adjoint buffers)

@@ -188,6 +188,7 @@ struct Engine {
     // work lists
     std::vector<TileWork> tiles;
     std::vector<int2> sten, rows;
+    std::vector<size_t> maskWords;   // per entry
     std::vector<int> imgRowStart;
     std::vector<ScaleDev> sds;
     for (int i = 0; i < n; ++i) {
@@ -242,6 +243,10 @@ struct Engine {
         for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
         const int yEnd = std::min(s.dataH - s.off - 1, s.dataH - 2);
         for (int y = s.off + 1; y <= yEnd; ++y) rows.push_back(make_int2(entry, y - s.off - 1));
+        // keypoint-decision words: one per 32 candidate pixels of a row
+        const int xEnd = std::min(s.dataW - s.off, s.dataW - 1);
+        d.nmsChunks = std::max(0, (xEnd - s.off - 1 + 31) / 32);
+        maskWords.push_back((size_t)std::max(0, yEnd - s.off) * d.nmsChunks);
         sds.push_back(d);
       }
     }
@@ -285,6 +290,8 @@ struct Engine {
     const size_t offOuts = a.reserve(sizeof(KpOut) * n);
     const size_t offPyr = a.reserve(sizeof(PyrJob) * std::max<size_t>(1, h_pyr.size()));
     const size_t offMaps = a.reserve(kTensorMapBytes * sds.size());
+    std::vector<size_t> offMask;
+    for (size_t w : maskWords) offMask.push_back(a.reserve(sizeof(unsigned int) * std::max<size_t>(1, w)));
     size_t offKp = 0;
     kpCapInternal = internalKpCap;
     if (internalKpCap > 0)
@@ -313,6 +320,7 @@ struct Engine {
         d.D = reinterpret_cast<float*>(base + offD[i][si]);
         d.S = reinterpret_cast<float*>(base + offS[i][si]);
         d.maxKey = reinterpret_cast<unsigned int*>(base + offMax) + e2;
+        d.nmsMask = reinterpret_cast<unsigned int*>(base + offMask[e2]);
       }
     }
     for (int l = 1, k = 0; l <= maxLevel; ++l)

@@ -386,34 +386,57 @@ __device__ __forceinline__ bool is_keypoint(const float* __restrict__ D, int dp,
   const float* r1 = r0 + dp;
   const float* r2 = r1 + dp;
   const float v = r1[x];
+  if (!(v > thr)) return false;   // most pixels: one load
   float dil = fmaxf(fmaxf(r0[x - 1], r0[x]), r0[x + 1]);
   dil = fmaxf(dil, fmaxf(r1[x - 1], r1[x + 1]));
   dil = fmaxf(dil, fmaxf(fmaxf(r2[x - 1], r2[x]), r2[x + 1]));
-  return (v - dil > 0.f) && (v > thr);
+  return v - dil > 0.f;
 }
 
-__global__ void __launch_bounds__(256)
-k_nms_count(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int* __restrict__ counts) {
-  const int2 item = rows[blockIdx.x];
-  const ScaleDev* sd = sds + item.x;
-  const int off = sd->off;
-  const int y = off + 1 + item.y;
-  const float thr = scale_thresh(sd);
-  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
-  int n = 0;
-  for (int x = off + 1 + threadIdx.x; x < xEnd; x += blockDim.x)
-    n += is_keypoint(sd->D, sd->dPitch, x, y, thr) ? 1 : 0;
-#pragma unroll
-  for (int m = 16; m > 0; m >>= 1) n += __shfl_xor_sync(0xffffffffu, n, m);
-  __shared__ int s_n[8];
-  if ((threadIdx.x & 31) == 0) s_n[threadIdx.x >> 5] = n;
+// Candidate rows are counted by 4 warps each (2 rows per 256-thread block):
+// warp q of a row tests the 32-pixel chunks q, q + 4, ... -- strict
+// 8-neighbour maximum above the threshold -- and, when the map has decision
+// words, stores the chunk's ballot for the write pass.
+constexpr int kNmsWarpsPerRow = 4;
+constexpr int kNmsRowsPerBlock = 2;
+constexpr int kNmsThreads = 32 * kNmsWarpsPerRow * kNmsRowsPerBlock;
+
+__global__ void __launch_bounds__(kNmsThreads)
+k_nms_count(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int nrows, int* __restrict__ counts) {
+  __shared__ int s_cnt[kNmsRowsPerBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int q = warp % kNmsWarpsPerRow, rl = warp / kNmsWarpsPerRow;
+  const int r = blockIdx.x * kNmsRowsPerBlock + rl;
+  if (threadIdx.x < kNmsRowsPerBlock) s_cnt[threadIdx.x] = 0;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int tot = 0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tot += s_n[k];
-    counts[blockIdx.x] = tot;
+  if (r < nrows) {
+    const int2 item = rows[r];
+    const ScaleDev* sd = sds + item.x;
+    const int off = sd->off;
+    const int y = off + 1 + item.y;
+    const float thr = scale_thresh(sd);
+    const int xEnd = min(sd->dataW - off, sd->dataW - 1);
+    const float* __restrict__ D = sd->D;
+    const int dp = sd->dPitch;
+    unsigned int* __restrict__ mask = sd->nmsMask ? sd->nmsMask + (size_t)item.y * sd->nmsChunks : nullptr;
+    const int nch = (xEnd - off - 1 + 31) / 32;
+    int n = 0;
+#pragma unroll 4
+    for (int c = q; c < nch; c += kNmsWarpsPerRow) {
+      const int x = off + 1 + 32 * c + lane;
+      const unsigned int bal = __ballot_sync(0xffffffffu, x < xEnd && is_keypoint(D, dp, x, y, thr));
+      n += __popc(bal);
+      if (mask && lane == 0) mask[c] = bal;   // the write pass reads the decisions back
+    }
+    if (lane == 0 && n) atomicAdd(&s_cnt[rl], n);
   }
+  __syncthreads();
+  if (threadIdx.x < kNmsRowsPerBlock && blockIdx.x * kNmsRowsPerBlock + threadIdx.x < nrows)
+    counts[blockIdx.x * kNmsRowsPerBlock + threadIdx.x] = s_cnt[threadIdx.x];
 }
+
+// One warp per candidate row for the write pass.
+constexpr int kNmsWriteRows = 8;
 
 // Exclusive scan of counts[0..n) into offsets; per-image totals from the
 // image boundaries.  One block of 1024 threads, 4 elements per thread per
@@ -473,62 +496,74 @@ k_scan(const int* __restrict__ counts, int* __restrict__ offsets, int n,
   }
 }
 
-__global__ void __launch_bounds__(256)
-k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows,
+// Records of a row in x order at the row's offset (one warp per row).
+__global__ void __launch_bounds__(32 * kNmsWriteRows)
+k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int nrows,
             const int* __restrict__ offsets, const int* __restrict__ imageRowStart,
             const KpOut* __restrict__ outs) {
-  const int2 item = rows[blockIdx.x];
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * kNmsWriteRows + (threadIdx.x >> 5);
+  if (r >= nrows) return;
+  const int2 item = rows[r];
   const ScaleDev* sd = sds + item.x;
   const KpOut out = outs[sd->image];
   const int off = sd->off;
   const int y = off + 1 + item.y;
   const float thr = scale_thresh(sd);
-  int base = offsets[blockIdx.x] - offsets[imageRowStart[sd->image]];
+  int base = offsets[r] - offsets[imageRowStart[sd->image]];
   if (base >= out.capacity) return;
-  const float* D = sd->D;
+  const float* __restrict__ D = sd->D;
   const int dp = sd->dPitch;
-  __shared__ int s_w[8];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int xEnd = min(sd->dataW - off, sd->dataW - 1);
-  for (int xs = off + 1; xs < xEnd; xs += blockDim.x) {
-    const int x = xs + threadIdx.x;
-    const bool kp = x < xEnd && is_keypoint(D, dp, x, y, thr);
-    const unsigned int bal = __ballot_sync(0xffffffffu, kp);
-    if (lane == 0) s_w[wid] = __popc(bal);
-    __syncthreads();
-    int before = 0, total = 0;
-    for (int k = 0; k < 8; ++k) {
-      before += k < wid ? s_w[k] : 0;
-      total += s_w[k];
+  const float pyr = sd->pyrstep, kpSize = sd->kpSize;
+  const int kpOctave = sd->kpOctave;
+  const unsigned int* __restrict__ mask = sd->nmsMask ? sd->nmsMask + (size_t)item.y * sd->nmsChunks : nullptr;
+  const int nch = (xEnd - off - 1 + 31) / 32;
+  // chunks with a keypoint: 32 decision words per load when they are stored
+  for (int c0 = 0; c0 < nch; c0 += 32) {
+    unsigned int words = 0, live;
+    if (mask) {
+      words = c0 + lane < nch ? mask[c0 + lane] : 0u;
+      live = __ballot_sync(0xffffffffu, words != 0u);
+    } else {
+      live = nch - c0 >= 32 ? 0xffffffffu : (1u << (nch - c0)) - 1u;
     }
-    if (kp) {
-      const int idx = base + before + __popc(bal & ((1u << lane) - 1u));
-      if (idx < out.capacity) {
-        const float* r1 = D + (size_t)y * dp;
-        const float xv1 = r1[x - 1], xv2 = r1[x], xv3 = r1[x + 1];
-        const float yv1 = r1[x - dp], yv3 = r1[x + dp];
-        float xpos = (float)x, ypos = (float)y;
-        // cuda_bimp.cuh:114-132 (parabola through the 3 samples per axis)
-        const float denx = xv1 + xv3 - 2.f * xv2;
-        const float deny = yv1 + yv3 - 2.f * xv2;
-        const float numx = 0.5f * (xv1 - xv3);
-        const float numy = 0.5f * (yv1 - yv3);
-        if (denx != 0.f) xpos += __fdiv_rn(numx, denx);
-        if (deny != 0.f) ypos += __fdiv_rn(numy, deny);
-        float* kpm = out.kp;
-        const size_t ld = out.ld;
-        kpm[0 * ld + idx] = xpos * sd->pyrstep;
-        kpm[1 * ld + idx] = ypos * sd->pyrstep;
-        reinterpret_cast<int*>(kpm)[2 * ld + idx] = 1;
-        reinterpret_cast<int*>(kpm)[3 * ld + idx] = sd->kpOctave;
-        kpm[4 * ld + idx] = sd->kpSize;
-        kpm[5 * ld + idx] = -1.f;
-        kpm[6 * ld + idx] = xv2;
+    while (live) {
+      const int cc = __ffs(live) - 1;
+      live &= live - 1u;
+      const int c = c0 + cc;
+      const int x = off + 1 + 32 * c + lane;
+      const unsigned int bal = mask ? __shfl_sync(0xffffffffu, words, cc)
+                                    : __ballot_sync(0xffffffffu, x < xEnd && is_keypoint(D, dp, x, y, thr));
+      const bool kp = (bal >> lane) & 1u;
+      if (kp) {
+        const int idx = base + __popc(bal & ((1u << lane) - 1u));
+        if (idx < out.capacity) {
+          const float* r1 = D + (size_t)y * dp;
+          const float xv1 = r1[x - 1], xv2 = r1[x], xv3 = r1[x + 1];
+          const float yv1 = r1[x - dp], yv3 = r1[x + dp];
+          float xpos = (float)x, ypos = (float)y;
+          // cuda_bimp.cuh:114-132 (parabola through the 3 samples per axis)
+          const float denx = xv1 + xv3 - 2.f * xv2;
+          const float deny = yv1 + yv3 - 2.f * xv2;
+          const float numx = 0.5f * (xv1 - xv3);
+          const float numy = 0.5f * (yv1 - yv3);
+          if (denx != 0.f) xpos += __fdiv_rn(numx, denx);
+          if (deny != 0.f) ypos += __fdiv_rn(numy, deny);
+          float* kpm = out.kp;
+          const size_t ld = out.ld;
+          kpm[0 * ld + idx] = xpos * pyr;
+          kpm[1 * ld + idx] = ypos * pyr;
+          reinterpret_cast<int*>(kpm)[2 * ld + idx] = 1;
+          reinterpret_cast<int*>(kpm)[3 * ld + idx] = kpOctave;
+          kpm[4 * ld + idx] = kpSize;
+          kpm[5 * ld + idx] = -1.f;
+          kpm[6 * ld + idx] = xv2;
+        }
       }
+      base += __popc(bal);
+      if (base >= out.capacity) return;
     }
-    base += total;
-    __syncthreads();
-    if (base >= out.capacity) break;
   }
 }
 
@@ -662,9 +697,13 @@ void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigne
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,
                 cudaStream_t s) {
-  if (nrows > 0) k_nms_count<<<nrows, 256, 0, s>>>(d_sd, d_rows, d_counts);
+  if (nrows > 0)
+    k_nms_count<<<(nrows + kNmsRowsPerBlock - 1) / kNmsRowsPerBlock, kNmsThreads, 0, s>>>(d_sd, d_rows, nrows,
+                                                                                           d_counts);
   k_scan<<<1, 1024, 0, s>>>(d_counts, d_offsets, nrows, d_imageRowStart, nImages, d_totals);
-  if (nrows > 0) k_nms_write<<<nrows, 256, 0, s>>>(d_sd, d_rows, d_offsets, d_imageRowStart, d_outs);
+  if (nrows > 0)
+    k_nms_write<<<(nrows + kNmsWriteRows - 1) / kNmsWriteRows, 32 * kNmsWriteRows, 0, s>>>(
+        d_sd, d_rows, nrows, d_offsets, d_imageRowStart, d_outs);
 }
 
 }  // namespace bimp_b200
