@@ -33,6 +33,15 @@ constexpr int kSmemBars = 2 * 8;                         // two mbarriers
 constexpr int kGaborSmem = kSmemW + kSmemXh + kSmemG + kSmemTw + kSmemMaps + kSmemBars;
 static_assert(kGaborSmem <= 232448, "tile kernel exceeds the 227 KB shared-memory limit");
 
+// |z| as s * rsqrt(s), s = |z|^2 (hardware reciprocal square root, relative
+// error a few 1e-7); exactly 0 for z = 0.
+__device__ __forceinline__ float cmag(float2 z) {
+  const float s = fmaf(z.x, z.x, z.y * z.y);
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(s));
+  return s > 0.f ? s * r : 0.f;
+}
+
 // Float levels hold X (a float image, X = u8/255 for the uint8 content);
 // the uint8 path's value 255*u8/65536 is then (255*255/65536) * X.
 constexpr float kFloatLevelScale = 65025.0f / 65536.0f;
@@ -226,6 +235,8 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     // tiles holding window column 0 or column dataW of a map with fftW == dataW
     const bool wrapTile = sd->wrapW != 0 && (C0 == 0 || C0 + V >= cCols);
+    // window positions x in [kX, xHi) are this tile's valid outputs
+    const int xHi = min(kX + V, cCols - C0 + kX);
     float* __restrict__ C0p = sd->C;
     float2* __restrict__ Z0p = sd->Z;
     const long long cStride = sd->cStride;
@@ -291,13 +302,13 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         if (gy < cRows) {
           float* dst = Cout + (size_t)gy * cPitch;
           if (!wrapTile) {
+            float* dstx = dst + (C0 - kX);
 #pragma unroll
             for (int n2 = 0; n2 < 16; ++n2) {
               const int x = n1 + 8 * n2;
-              const int gx = C0 + x - kX;
-              if (x >= kX && x < kX + V && gx < cCols) {
-                dst[gx] = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
-                if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)gy * cPitch + gx] = v[n2];
+              if (x >= kX && x < xHi) {
+                dstx[x] = cmag(v[n2]);
+                if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)gy * cPitch + (C0 - kX) + x] = v[n2];
               }
             }
           } else {
@@ -310,7 +321,7 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
               const int x = n1 + 8 * n2;
               const int gx = C0 + x - kX;
               if (x >= kX && x < kX + V && gx < cCols) {
-                const float m = sqrtf(v[n2].x * v[n2].x + v[n2].y * v[n2].y);
+                const float m = cmag(v[n2]);
                 if (!(gx == cCols - 1 && gy < cRows - 1)) {
                   dst[gx] = m;
                   if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)gy * cPitch + gx] = v[n2];
