@@ -210,6 +210,16 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
 
   uint32_t gc = 0;       // G chunks consumed by this CTA (identical in every thread)
   bool fault = false;
+  // Where this thread's column p of the full spectrum lives in the
+  // Hermitian half Xh (the same for every tile and orientation): the half
+  // holds kx = 0..64; the other columns are conj(X(-k)), read from row
+  // -ky.  Resolved once, so that the spectrum product pass has no branch.
+  const int pI1 = t & 127;
+  const int pa = pI1 >> 3, pb = pI1 & 7;
+  const bool pNyq = pb == 4 && pa == 0;
+  const bool pConj = pb >= 4 && !pNyq;
+  const int pSlot = pb < 4 ? 4 * pa + pb : (pNyq ? 64 : (pa > 0 ? 4 * (16 - pa) + (7 - pb) : 8 - pb));
+  const float pSign = pConj ? -1.f : 1.f;
 
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const TileWork item = work[w];
@@ -249,12 +259,16 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         const uint32_t buf = gc & 1;
         if (!mbar_wait(buf ? bar1 : bar0, (gc >> 1) & 1)) fault = true;
         const float* Gq = Gbuf + buf * kGChunkFloats;
-        const int p = t & 127, k2 = (t >> 7) + 4 * q;
+        const int p = pI1, k2 = (t >> 7) + 4 * q;
         float2 v[8];
 #pragma unroll
         for (int k1 = 0; k1 < 8; ++k1) {
           const int py = 8 * k2 + k1;
-          v[k1] = c_scale(spectrum_at(Xh, py, p), Gq[(py - kGChunkRows * q) * kTile + p]);
+          // row of -ky in the permuted order (ky = 16 k1 + k2 for py = 8 k2 + k1)
+          const int row = pConj ? (k2 > 0 ? 8 * (16 - k2) + (7 - k1) : (8 - k1) & 7) : py;
+          float2 x = Xh[row * kXhCols + pSlot];
+          x.y *= pSign;
+          v[k1] = c_scale(x, Gq[(py - kGChunkRows * q) * kTile + p]);
         }
         dft8<true>(v);
 #pragma unroll
