@@ -358,14 +358,25 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
       __syncthreads();
     }
     // one inverse transform of the Hermitian sum: Re -> window gradient,
-    // scattered to the float level through the padded-torus index maps
+    // scattered to the float level through the padded-torus index maps.
+    // Column p = t & 127 of the full spectrum is read from the half Bh
+    // without a branch (conj(Bh(-k)) for kx > 64).
+    const int pa = (t & 127) >> 3, pb = t & 7;
+    const bool pNyq = pb == 4 && pa == 0;
+    const bool pConj = pb >= 4 && !pNyq;
+    const int pSlot = pb < 4 ? 4 * pa + pb : (pNyq ? 64 : (pa > 0 ? 4 * (16 - pa) + (7 - pb) : 8 - pb));
+    const float pSign = pConj ? -1.f : 1.f;
 #pragma unroll
     for (int it = 0; it < 4; ++it) {
       const int j = t + it * kTileThreads;
       const int p = j & 127, k2 = j >> 7;
       float2 v[8];
 #pragma unroll
-      for (int k1 = 0; k1 < 8; ++k1) v[k1] = spectrum_at(Bh, 8 * k2 + k1, p);
+      for (int k1 = 0; k1 < 8; ++k1) {
+        const int row = pConj ? (k2 > 0 ? 8 * (16 - k2) + (7 - k1) : (8 - k1) & 7) : 8 * k2 + k1;
+        v[k1] = Bh[row * kXhCols + pSlot];
+        v[k1].y *= pSign;
+      }
       dft8<true>(v);
 #pragma unroll
       for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, p)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
