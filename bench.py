@@ -300,6 +300,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         px = sum(w * h for w, h in sizes)
         bt = api.Batch(sizes, lam_b, kp_capacity=65536)
         bt.load(imgs)
+        tune = bt.autotune(reps=3)   # tile plan: valid-block policy, tile order, tile-kernel grid
         for _ in range(3):
             bt.run()
         torch.cuda.synchronize()
@@ -335,7 +336,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         batched = {"workload": "64 mixed images, W in [320,1920], H in [240,1080], 8 scales",
                    "value": round(world * kb * px / (ms_b * 1e-3) / 1e6, 2),
                    "plain_value": round(world * kb * px / (ms_p * 1e-3) / 1e6, 2),
-                   "ratio": round(ms_p / ms_b, 3), "unit": UNIT, "graph": True}
+                   "ratio": round(ms_p / ms_b, 3), "unit": UNIT, "graph": True,
+                   "autotune": {"chosen": tune["chosen"], "plans_timed": len(tune["tried"]),
+                                "default_plan_ms": next((t["ms"] for t in tune["tried"]
+                                                         if t["policy"] == 0 and t["order"] == 0
+                                                         and t["grid"] == t["tiles"]), None)}}
         for c2 in ctxs:
             c2.close()
         bt.close()

@@ -361,6 +361,20 @@ class Batch:
     def run(self, stream=None):
         L.check(L.lib().bimp_batch_run(self._h, _stream_ptr(stream)), "batch_run")
 
+    def set_tile_plan(self, policy: int, order: int, grid: int = 0):
+        """Use a tile plan (bimp_batch_set_tile_plan); grid <= 0: one CTA per tile."""
+        L.check(L.lib().bimp_batch_set_tile_plan(self._h, int(policy), int(order), int(grid)), "batch_tile_plan")
+
+    def autotune(self, reps: int = 5, stream=None) -> dict:
+        """Time every tile plan on the loaded images, keep the fastest
+        (bimp_batch_autotune); returns the chosen plan and all timings."""
+        chosen = L.TilePlan()
+        tried = (L.TilePlan * 32)()
+        n = C.c_int()
+        L.check(L.lib().bimp_batch_autotune(self._h, _stream_ptr(stream), int(reps), C.byref(chosen), tried, 32,
+                                            C.byref(n)), "batch_autotune")
+        return {"chosen": chosen.as_dict(), "tried": [tried[i].as_dict() for i in range(n.value)]}
+
     def counts(self, stream=None):
         L.check(L.lib().bimp_batch_counts(self._h, C.c_void_p(self._counts.data_ptr()),
                                           _stream_ptr(stream)), "batch_counts")

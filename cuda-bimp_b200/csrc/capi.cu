@@ -131,6 +131,58 @@ struct Engine {
   float* d_kpInternal = nullptr;
   int kpCapInternal = 0;
   int tileGrid = 0;    // CTAs of the tile kernel (each loops over tiles)
+  int tileCap = 0;     // capacity of d_tiles (the largest tile plan)
+  int tilePolicy = 0, tileOrder = 0;
+
+  // Tile plan (what the batch autotuner chooses between).
+  // policy 0: V = 128 - 2 kX valid outputs per tile side (the largest);
+  //        1: V rounded down to a multiple of 32 when that keeps at least
+  //           3/4 of it, so that the valid-row passes split evenly over the
+  //           16 warps of a tile (more tiles, fewer idle warps per tile).
+  // order 0: tiles entry by entry; 1: the entries' tiles interleaved.
+  // grid: CTAs of the tile kernel (<= 0: one per tile).
+  static int plan_v(int kX, int policy) {
+    const int vmax = kTile - 2 * kX;
+    const int v32 = vmax / 32 * 32;
+    return (policy == 1 && v32 * 4 >= vmax * 3) ? v32 : vmax;
+  }
+  static std::vector<TileWork> tile_plan(std::vector<ScaleDev>& sds, int policy, int order) {
+    std::vector<std::vector<TileWork>> per(sds.size());
+    for (size_t e = 0; e < sds.size(); ++e) {
+      ScaleDev& d = sds[e];
+      d.V = plan_v(d.kX, policy);
+      d.tilesX = (d.cCols + d.V - 1) / d.V;
+      d.tilesY = (d.cRows + d.V - 1) / d.V;
+      for (int k = 0; k < d.tilesX * d.tilesY; ++k) per[e].push_back({static_cast<int>(e), k});
+    }
+    std::vector<TileWork> out;
+    if (order == 0) {
+      for (auto& v : per) out.insert(out.end(), v.begin(), v.end());
+    } else {
+      for (size_t k = 0;; ++k) {
+        bool any = false;
+        for (auto& v : per)
+          if (k < v.size()) { out.push_back(v[k]); any = true; }
+        if (!any) break;
+      }
+    }
+    return out;
+  }
+  int retile(int policy, int order, int grid) {
+    std::vector<ScaleDev> sds = h_sd;
+    const std::vector<TileWork> tiles = tile_plan(sds, policy, order);
+    if ((int)tiles.size() > tileCap) return fail(BIMP_ERR_INVALID, "tile plan larger than its buffer");
+    BIMP_CUDA(cudaSetDevice(device));
+    BIMP_CUDA(cudaMemcpy(d_sd, sds.data(), sizeof(ScaleDev) * sds.size(), cudaMemcpyHostToDevice));
+    if (!tiles.empty())
+      BIMP_CUDA(cudaMemcpy(d_tiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice));
+    h_sd = sds;
+    nTiles = static_cast<int>(tiles.size());
+    tileGrid = grid > 0 ? std::min(grid, nTiles) : nTiles;
+    tilePolicy = policy;
+    tileOrder = order;
+    return BIMP_OK;
+  }
 
   int build(int dev, const int* w, const int* h, int n, const float* lambdas, int nl,
             const bimp_params& p, int internalKpCap) {
@@ -279,7 +331,11 @@ struct Engine {
     nSten = static_cast<int>(sten.size());
     nRows = static_cast<int>(rows.size());
     const size_t offSd = a.reserve(sizeof(ScaleDev) * sds.size());
-    const size_t offTiles = a.reserve(sizeof(TileWork) * std::max<size_t>(1, tiles.size()));
+    {   // the tile buffer holds the largest plan the autotuner may choose
+      std::vector<ScaleDev> tmp = sds;
+      tileCap = static_cast<int>(std::max(tiles.size(), tile_plan(tmp, 1, 0).size()));
+    }
+    const size_t offTiles = a.reserve(sizeof(TileWork) * std::max<size_t>(1, (size_t)tileCap));
     const size_t offSten = a.reserve(sizeof(int2) * std::max<size_t>(1, sten.size()));
     const size_t offRows = a.reserve(sizeof(int2) * std::max<size_t>(1, rows.size()));
     const size_t offCounts = a.reserve(sizeof(int) * std::max<size_t>(1, rows.size()));
@@ -450,6 +506,23 @@ struct bimp_batch {
   int* h_totals = nullptr;   // pinned: n_images totals, then the device fault word
   std::vector<bimp_keypoint> tmp;
 };
+
+namespace {
+// (Re)captures the batch's detection into its CUDA graph.
+int capture_batch(bimp_batch* b) {
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  cudaError_t e = cudaStreamBeginCapture(b->capStream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const int rc2 = b->eng.enqueue(b->capStream);
+    const cudaError_t e2 = cudaStreamEndCapture(b->capStream, &b->graph);
+    e = rc2 != BIMP_OK ? cudaErrorUnknown : e2;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e != cudaSuccess) return fail(BIMP_ERR_CUDA, std::string("batch graph setup: ") + cudaGetErrorString(e));
+  return BIMP_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -756,18 +829,16 @@ int bimp_batch_create(bimp_batch** out, const int* widths, const int* heights, i
   }
   cudaError_t e = cudaMallocHost(&b->h_totals, sizeof(int) * (n_images + 1));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capStream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamBeginCapture(b->capStream, cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    const int rc2 = b->eng.enqueue(b->capStream);
-    cudaError_t e2 = cudaStreamEndCapture(b->capStream, &b->graph);
-    if (rc2 != BIMP_OK) e = cudaErrorUnknown;
-    else e = e2;
-  }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
   if (e != cudaSuccess) {
-    const std::string msg = std::string("batch graph setup: ") + cudaGetErrorString(e);
+    const std::string msg = std::string("batch setup: ") + cudaGetErrorString(e);
     bimp_batch_destroy(b);
     return fail(BIMP_ERR_CUDA, msg);
+  }
+  rc = capture_batch(b);
+  if (rc != BIMP_OK) {
+    const std::string msg = g_last_error;
+    bimp_batch_destroy(b);
+    return fail(rc, msg);
   }
   *out = b;
   return BIMP_OK;
@@ -792,6 +863,61 @@ int bimp_batch_image(bimp_batch* b, int i, uint8_t** d_image, size_t* pitch) {
     return fail(BIMP_ERR_INVALID, "bad batch image arguments");
   *d_image = b->eng.lvl[i][0];
   *pitch = (size_t)b->eng.lvlP[i][0];
+  return BIMP_OK;
+}
+
+int bimp_batch_set_tile_plan(bimp_batch* b, int policy, int order, int grid) {
+  if (!b || policy < 0 || policy > 1 || order < 0 || order > 1) return fail(BIMP_ERR_INVALID, "bad tile plan");
+  BIMP_CUDA(cudaSetDevice(b->eng.device));
+  const int rc = b->eng.retile(policy, order, grid);
+  if (rc != BIMP_OK) return rc;
+  return capture_batch(b);
+}
+
+int bimp_batch_autotune(bimp_batch* b, void* stream, int reps, bimp_tile_plan* chosen, bimp_tile_plan* tried,
+                        int max_tried, int* n_tried) {
+  if (!b || reps <= 0 || (max_tried > 0 && !tried)) return fail(BIMP_ERR_INVALID, "bad autotune arguments");
+  BIMP_CUDA(cudaSetDevice(b->eng.device));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int sms = 148;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->eng.device) != cudaSuccess || sms <= 0)
+    sms = 148;
+  const int grids[3] = {0, sms, 2 * sms};
+  cudaEvent_t e0, e1;
+  BIMP_CUDA(cudaEventCreate(&e0));
+  BIMP_CUDA(cudaEventCreate(&e1));
+  bimp_tile_plan best{};
+  best.ms = -1.f;
+  int count = 0, rc = BIMP_OK;
+  for (int policy = 0; policy < 2 && rc == BIMP_OK; ++policy)
+    for (int order = 0; order < 2 && rc == BIMP_OK; ++order)
+      for (int g = 0; g < 3 && rc == BIMP_OK; ++g) {
+        rc = b->eng.retile(policy, order, grids[g]);
+        for (int i = 0; i < 2 && rc == BIMP_OK; ++i) rc = b->eng.enqueue(s);
+        if (rc != BIMP_OK) break;
+        cudaEventRecord(e0, s);
+        for (int i = 0; i < reps && rc == BIMP_OK; ++i) rc = b->eng.enqueue(s);
+        cudaEventRecord(e1, s);
+        if (rc != BIMP_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+          rc = fail(BIMP_ERR_CUDA, "autotune timing failed");
+          break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const bimp_tile_plan pl{policy, order, b->eng.tileGrid, b->eng.nTiles, ms / reps};
+        if (count < max_tried) tried[count] = pl;
+        ++count;
+        if (best.ms < 0.f || pl.ms < best.ms) best = pl;
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != BIMP_OK) return rc;
+  rc = b->eng.retile(best.policy, best.order, best.grid >= best.tiles ? 0 : best.grid);
+  if (rc == BIMP_OK) rc = capture_batch(b);
+  if (rc != BIMP_OK) return rc;
+  if (chosen) *chosen = best;
+  if (n_tried) *n_tried = count;
   return BIMP_OK;
 }
 

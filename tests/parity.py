@@ -11,7 +11,9 @@ Tolerances (written here, used by the tests):
   every pixel, so near-zero magnitudes have no meaningful relative error;
 * keypoints: identical (scale, integer x, integer y) sets except where the
   oracle's decision is within TIE_EPS * max|D| of a tie (with a neighbour, or
-  with the threshold), and subpixel positions within SUBPIX_TOL pixels.
+  with the threshold), and subpixel positions within SUBPIX_TOL pixels
+  of the scale's pyramid level (the parabola is fitted on the level grid;
+  records carry level position x pyrstep).
 """
 from __future__ import annotations
 
@@ -92,7 +94,8 @@ def compare_keypoints(rec: np.ndarray, oracle_result, tie_eps: float = TIE_EPS) 
                 continue
             report["matched"] += 1
             gx, gy, gv = g[key]
-            report["max_subpix"] = max(report["max_subpix"], abs(gx - val[0]), abs(gy - val[1]))
+            pyr = r["scale"].pyrstep
+            report["max_subpix"] = max(report["max_subpix"], abs(gx - val[0]) / pyr, abs(gy - val[1]) / pyr)
             report["max_resp_rel"] = max(report["max_resp_rel"], abs(gv - val[2]) / scale)
         for key in g:
             if key in ref:

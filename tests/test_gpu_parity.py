@@ -245,6 +245,35 @@ def test_batch_matches_single():
     assert np.array_equal(got0, api.keypoint_matrix_to_records(api.getKeypoints(imgs[0], cs, capacity=100000)))
 
 
+def test_batch_tile_plans_and_autotune():
+    """Every tile plan keeps parity with the oracle; plans of one policy are
+    bitwise identical; the autotuner times all 12 and keeps the fastest."""
+    rng = np.random.default_rng(9)
+    sizes = [(int(rng.integers(20, 50)) * 16, int(rng.integers(15, 35)) * 16) for _ in range(3)]
+    imgs = [synth.synth_image(w, h, 8, seed=90 + i) for i, (w, h) in enumerate(sizes)]
+    lam = synth.bank(8)
+    refs = [O.run(img, lam) for img in imgs]
+    b = api.Batch(sizes, lam, kp_capacity=100000)
+    b.load(imgs)
+    outs = {}
+    for policy in (0, 1):
+        for order, grid in ((0, 0), (1, 148)):
+            b.set_tile_plan(policy, order, grid)
+            b.run()
+            outs[(policy, order)] = [api.keypoint_matrix_to_records(b.keypoints(i)) for i in range(len(imgs))]
+        for i in range(len(imgs)):
+            assert np.array_equal(outs[(policy, 0)][i], outs[(policy, 1)][i])
+            _check_keypoints(outs[(policy, 0)][i], refs[i])
+    rep = b.autotune(reps=2)
+    assert len(rep["tried"]) == 12 and rep["chosen"]["ms"] > 0
+    assert rep["chosen"]["ms"] == min(t["ms"] for t in rep["tried"])
+    b.run()
+    for i in range(len(imgs)):
+        got = api.keypoint_matrix_to_records(b.keypoints(i))
+        assert np.array_equal(got, outs[(rep["chosen"]["policy"], 0)][i])
+    b.close()
+
+
 def test_persistent_tile_loop_matches(monkeypatch):
     """Each CTA of the tile kernel walks many tiles (grid capped at 7): the
     spectrum double buffer's phases carry across tiles; results unchanged."""
