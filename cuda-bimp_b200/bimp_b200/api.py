@@ -145,6 +145,23 @@ class CudaStuff:
                                          out.stride(0), _stream_ptr()), "complex_map")
         return out
 
+    def lines_edges(self, scale: int, ch=None):
+        """Line/edge detection on one scale of the last detection
+        (bimp_detect_lines_edges): (strength, orientation, type) maps.
+        ch: optional summed complex response (data_h x data_w float32 CUDA
+        tensor); default the sum of the scale's complex cells."""
+        torch = _torch()
+        k = self.ks[scale]
+        h, w = k["data_h"], k["data_w"]
+        res = torch.empty((h, w), dtype=torch.float32, device="cuda")
+        ori = torch.empty((h, w), dtype=torch.float32, device="cuda")
+        typ = torch.empty((h, w), dtype=torch.int8, device="cuda")
+        chp, chld = (None, 0) if ch is None else (C.c_void_p(ch.data_ptr()), ch.stride(0))
+        L.check(L.lib().bimp_detect_lines_edges(self.handle, scale, chp, chld, C.c_void_p(res.data_ptr()),
+                                                C.c_void_p(ori.data_ptr()), C.c_void_p(typ.data_ptr()), w,
+                                                _stream_ptr()), "detect_lines_edges")
+        return res, ori, typ
+
 
 def _as_gpu_u8(image):
     torch = _torch()

@@ -496,6 +496,11 @@ struct bimp_context {
   int* h_count = nullptr;   // pinned: [0] keypoint total, [1] device fault word
   float* d_kpScratch = nullptr;
   int d_kpScratchCap = 0;
+  // line/edge detection, allocated on first use: e + i o of one scale, that
+  // scale's descriptor and tile list
+  float2* d_leZ = nullptr;
+  ScaleDev* d_leSd = nullptr;
+  TileWork* d_leTiles = nullptr;
 };
 
 struct bimp_batch {
@@ -591,6 +596,9 @@ int bimp_ctx_destroy(bimp_context* c) {
   if (c->h_count) cudaFreeHost(c->h_count);
   if (c->d_aos) cudaFree(c->d_aos);
   if (c->d_kpScratch) cudaFree(c->d_kpScratch);
+  if (c->d_leZ) cudaFree(c->d_leZ);
+  if (c->d_leSd) cudaFree(c->d_leSd);
+  if (c->d_leTiles) cudaFree(c->d_leTiles);
   delete c;
   return BIMP_OK;
 }
@@ -737,6 +745,43 @@ int bimp_dense_map(bimp_context* c, int scale, int which, float* d_out, size_t l
   const float* src = which == 0 ? d.D : d.S;
   BIMP_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), src, d.dPitch * sizeof(float),
                               d.dataW * sizeof(float), d.dataH, cudaMemcpyDeviceToDevice, s));
+  return BIMP_OK;
+}
+
+int bimp_detect_lines_edges(bimp_context* c, int scale, const float* d_ch, size_t ch_ld, float* d_result,
+                            float* d_ori, int8_t* d_type, size_t ld, void* stream) {
+  if (!c || scale < 0 || scale >= c->eng.nScales || !d_result || !d_ori || !d_type)
+    return fail(BIMP_ERR_INVALID, "bad line/edge arguments");
+  const Engine& e = c->eng;
+  ScaleDev d = e.h_sd[scale];
+  if (ld < (size_t)d.dataW || (d_ch && ch_ld < (size_t)d.dataW))
+    return fail(BIMP_ERR_INVALID, "ld smaller than data width");
+  BIMP_CUDA(cudaSetDevice(e.device));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!c->d_leZ) {   // sized for the largest scale
+    long long maxStride = 0;
+    int maxTiles = 0;
+    for (const ScaleDev& q : e.h_sd) {
+      maxStride = std::max(maxStride, q.cStride);
+      maxTiles = std::max(maxTiles, q.tilesX * q.tilesY);
+    }
+    BIMP_CUDA(cudaMalloc(&c->d_leZ, sizeof(float2) * kNumOri * (size_t)maxStride));
+    BIMP_CUDA(cudaMalloc(&c->d_leSd, sizeof(ScaleDev)));
+    BIMP_CUDA(cudaMalloc(&c->d_leTiles, sizeof(TileWork) * (size_t)std::max(1, maxTiles)));
+  }
+  // rerun this scale's tile FFT keeping e + i o (the magnitudes it rewrites
+  // are the same numbers)
+  d.Z = c->d_leZ;
+  std::vector<TileWork> tiles;
+  for (int k = 0; k < d.tilesX * d.tilesY; ++k) tiles.push_back({0, k});
+  BIMP_CUDA(cudaMemcpyAsync(c->d_leSd, &d, sizeof(ScaleDev), cudaMemcpyHostToDevice, s));
+  BIMP_CUDA(cudaMemcpyAsync(c->d_leTiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice, s));
+  launch_gabor_keep_z(c->d_leSd, c->d_leTiles, static_cast<int>(tiles.size()), e.d_fault, s);
+  launch_detect_le(c->d_leSd, d.dataW, d.dataH, d_ch, static_cast<int>(ch_ld), d_result, d_ori, d_type,
+                   static_cast<int>(ld), s);
+  BIMP_CUDA(cudaGetLastError());
+  // the host copies above read stack memory: finish before returning
+  BIMP_CUDA(cudaStreamSynchronize(s));
   return BIMP_OK;
 }
 

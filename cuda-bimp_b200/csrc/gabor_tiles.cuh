@@ -238,8 +238,10 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     }
     tile_forward_spectrum<FLT>(sd, R0, C0, W, Xh, tw, rmap, cmap, t);
     if constexpr (SAVE_Z) {   // the adjoint keeps the tile's image spectrum (Hermitian half)
-      float2* __restrict__ xs = xsave + (size_t)w * kSpecHalf;
-      for (int j = t; j < kSpecHalf; j += kTileThreads) xs[j] = Xh[j];
+      if (xsave) {
+        float2* __restrict__ xs = xsave + (size_t)w * kSpecHalf;
+        for (int j = t; j < kSpecHalf; j += kTileThreads) xs[j] = Xh[j];
+      }
     }
 
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;

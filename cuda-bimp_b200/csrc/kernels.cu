@@ -567,6 +567,77 @@ k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int
   }
 }
 
+// ---------------------------------------------------------------------------
+// line and edge detection (detectLE_kernel, cuda_bimp.cuh:362-432)
+// ---------------------------------------------------------------------------
+// Per pixel of one scale: if the summed complex response Ch (the caller's
+// map, or sum_o C_o when d_ch is null) is at least 0.1, take the dominant
+// orientation (the first strict maximum of C_o > 0), step one pixel along
+// (round(cos t), round(sin t)), t = o * 0.392699, and keep the pixel if its
+// odd or even response is a strict extremum along that step, the other
+// (or the same) response crosses zero across it, and C is a strict maximum
+// along it.  Type: 1 positive / 2 negative line (odd zero crossing at an
+// even maximum / minimum), 3 positive / 4 negative edge (even zero crossing
+// at an odd maximum / minimum; edges override lines, as the reference's
+// assignment order does).  Result = C at kept pixels, else 0; orientation t
+// at kept pixels, else 0; type 0 where nothing is assigned.  The reference
+// reads its neighbours by flat address, which leaves the data at the
+// border; here a pixel whose step leaves the data is not kept.
+__global__ void __launch_bounds__(256)
+k_detect_le(const ScaleDev* __restrict__ sd, const float* __restrict__ ch, int chLd, float* __restrict__ result,
+            float* __restrict__ ori, int8_t* __restrict__ type, int ld) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int W = sd->dataW, H = sd->dataH;
+  if (x >= W || y >= H) return;
+  const float* __restrict__ C = sd->C;
+  const float2* __restrict__ Z = sd->Z;
+  const long long cs = sd->cStride;
+  const size_t at = (size_t)y * sd->cPitch + x;
+  float chv;
+  if (ch) {
+    chv = ch[(size_t)y * chLd + x];
+  } else {
+    chv = 0.f;
+#pragma unroll
+    for (int o = 0; o < kNumOri; ++o) chv += C[o * cs + at];
+  }
+  float res = 0.f, th = 0.f;
+  int ty = 0;
+  if (!(chv < 0.1f)) {
+    int maxori = -1;
+    float maxresp = 0.f;
+#pragma unroll
+    for (int o = 0; o < kNumOri; ++o) {
+      const float cur = C[o * cs + at];
+      if (cur > maxresp) { maxresp = cur; maxori = o; }
+    }
+    if (maxori >= 0) {
+      const float theta = (float)(maxori * 0.392699);   // cuda_bimp.cuh:400 (double literal)
+      const int ox = (int)roundf(cosf(theta)), oy = (int)roundf(sinf(theta));
+      const int xp = x + ox, yp = y + oy, xm = x - ox, ym = y - oy;
+      if (xp >= 0 && xp < W && yp >= 0 && yp < H && xm >= 0 && xm < W && ym >= 0 && ym < H) {
+        const size_t ap = (size_t)yp * sd->cPitch + xp, am = (size_t)ym * sd->cPitch + xm;
+        const float2 z0 = Z[maxori * cs + at], zp = Z[maxori * cs + ap], zm = Z[maxori * cs + am];
+        const float o0 = z0.y, op = zp.y, om = zm.y, e0 = z0.x, ep = zp.x, em = zm.x;
+        const bool romax = o0 > op && o0 > om, romin = o0 < op && o0 < om, rozc = op * om < 0.f;
+        const bool remax = e0 > ep && e0 > em, remin = e0 < ep && e0 < em, rezc = ep * em < 0.f;
+        const float c0 = C[maxori * cs + at], cp = C[maxori * cs + ap], cm = C[maxori * cs + am];
+        const bool keep = (romax || romin || remax || remin) && (rezc || rozc) && !(c0 <= cp || c0 <= cm);
+        if (keep) {
+          ty = (rezc && romin) ? 4 : (rezc && romax) ? 3 : (rozc && remin) ? 2 : (rozc && remax) ? 1 : 0;
+          th = theta;
+          res = c0;
+        }
+      }
+    }
+  }
+  const size_t k = (size_t)y * ld + x;
+  result[k] = res;
+  ori[k] = th;
+  type[k] = (int8_t)ty;
+}
+
 #include "adjoint_kernels.cuh"
 
 // ---------------------------------------------------------------------------
@@ -641,6 +712,7 @@ cudaError_t configure_kernels() {
   const cudaFuncAttribute big = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaFuncSetAttribute(k_gabor_tiles<false, false>, big, (int)gabor_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles<true, true>, big, (int)gabor_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles<false, true>, big, (int)gabor_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilD>, big, (int)stencil_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilDS>, big, (int)stencil_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilAdj>, big, (int)stencil_smem_bytes());
@@ -661,6 +733,16 @@ void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int g
 void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                        float2* d_xsave, cudaStream_t s) {
   k_gabor_tiles<true, true><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault, d_xsave);
+}
+void launch_gabor_keep_z(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
+                         cudaStream_t s) {
+  if (nwork > 0)
+    k_gabor_tiles<false, true><<<nwork, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault, nullptr);
+}
+void launch_detect_le(const ScaleDev* d_sd, int dataW, int dataH, const float* d_ch, int chLd, float* d_result,
+                      float* d_ori, int8_t* d_type, int ld, cudaStream_t s) {
+  dim3 b(32, 8), g((dataW + 31) / 32, (dataH + 7) / 8);
+  k_detect_le<<<g, b, 0, s>>>(d_sd, d_ch, chLd, d_result, d_ori, d_type, ld);
 }
 void launch_pyr_f(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s) {
   dim3 b(32, 8), g((maxW + 31) / 32, (maxH + 7) / 8, njobs);

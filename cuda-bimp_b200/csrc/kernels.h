@@ -72,6 +72,13 @@ void launch_pyr_f_adj(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cuda
 // d_xsave + w * kSpecHalf)
 void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                        float2* d_xsave, cudaStream_t s);
+// detection-path tile kernel that also keeps e + i o (ScaleDev::Z) for the
+// line/edge detector; one CTA per work item
+void launch_gabor_keep_z(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
+                         cudaStream_t s);
+// line/edge detection on one scale (d_sd: that scale's descriptor, with Z)
+void launch_detect_le(const ScaleDev* d_sd, int dataW, int dataH, const float* d_ch, int chLd, float* d_result,
+                      float* d_ori, int8_t* d_type, int ld, cudaStream_t s);
 void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, double* d_gparams,
                         cudaStream_t s);
 void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);

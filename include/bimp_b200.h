@@ -160,6 +160,24 @@ int bimp_dense_map(bimp_context* ctx, int scale, int which, float* d_out,
 int bimp_complex_map(bimp_context* ctx, int scale, int orientation, float* d_out,
                      size_t ld, void* stream);
 
+/* Line and edge detection on one scale of the last detection
+ * (detectLE / detectLE_kernel, bimp/src/cuda_bimp.cu:1343-1365,
+ * bimp/include/detection/cuda_bimp.cuh:362-432; the reference defines it but
+ * never calls it).  Per data pixel: where the summed complex response
+ * (d_ch, data_h x data_w with row pitch ch_ld floats; NULL = the sum of the
+ * scale's 8 complex-cell maps) is at least 0.1, the dominant orientation's
+ * odd/even responses and complex cell are tested one pixel across it.
+ * Outputs (data_h x data_w, row pitch ld): d_result = the complex response
+ * at detected lines/edges, else 0; d_ori = the orientation angle there
+ * (o * 0.392699), else 0; d_type = 1 positive line, 2 negative line,
+ * 3 positive edge, 4 negative edge, else 0.  Pixels whose one-pixel step
+ * leaves the data are not detected (the reference reads past the data
+ * there).  Recomputes the scale's even/odd responses (its first call
+ * allocates their buffer); synchronises the stream. */
+int bimp_detect_lines_edges(bimp_context* ctx, int scale, const float* d_ch, size_t ch_ld,
+                            float* d_result, float* d_ori, int8_t* d_type, size_t ld,
+                            void* stream);
+
 /* ---- input preprocessing and colour features ------------------------------
  * getGPUImage size rule, bimp/src/cuda_bimp.cu:156-168: images with fewer
  * than 350 rows (and >= 350 columns) are scaled by 350/rows, otherwise

@@ -591,3 +591,71 @@ def color_features(kp_x, kp_y, kp_size, bgr: np.ndarray) -> np.ndarray:
         with np.errstate(invalid="ignore", divide="ignore"):
             out[i] = (0.5 * cnt) / (found * 1.0)
     return out
+
+
+# ---------------------------------------------------------------------------
+# line and edge detection (detectLE_kernel)
+# ---------------------------------------------------------------------------
+LE_THRESH = 0.1   # bimp/include/detection/cuda_bimp.cuh:392
+
+
+def detect_lines_edges(E: np.ndarray, Od: np.ndarray, Ct: np.ndarray, sc: Scale, ch=None):
+    """detectLE_kernel (bimp/include/detection/cuda_bimp.cuh:362-432) on the
+    data pixels of one scale, from the torus maps E, O, C (8, fftH, fftW).
+
+    ch: summed complex response (dataH, dataW); default sum_o C_o.  Returns
+    (result, ori, type, margin): result = C at detected pixels else 0, ori =
+    float32(o * 0.392699) there else 0, type 1..4 (positive/negative line,
+    positive/negative edge; edges override lines) else 0, and per pixel the
+    smallest gap of any comparison the decision made (threshold, dominant
+    orientation, extrema, zero crossings, complex-cell maximum).  A pixel
+    whose one-pixel step leaves the data is not detected (the reference
+    reads past the data there).
+    """
+    H, W = sc.dataH, sc.dataW
+    C = Ct[:, :H, :W]
+    if ch is None:
+        ch = C.sum(axis=0)
+    res = np.zeros((H, W))
+    ori = np.zeros((H, W), dtype=np.float32)
+    typ = np.zeros((H, W), dtype=np.int8)
+    margin = np.full((H, W), np.inf)
+    for y in range(H):
+        for x in range(W):
+            chv = ch[y, x]
+            m = abs(chv - LE_THRESH)
+            if chv < LE_THRESH:
+                margin[y, x] = m
+                continue
+            c = C[:, y, x]
+            maxori, maxresp = -1, 0.0
+            for o in range(NUM_ORI):
+                if c[o] > maxresp:
+                    maxresp, maxori = c[o], o
+            srt = np.sort(c)
+            m = min(m, srt[-1] - srt[-2], abs(srt[-1]))
+            if maxori < 0:
+                margin[y, x] = m
+                continue
+            th = f32(maxori * 0.392699)
+            ox = _round_half_away(float(np.cos(th, dtype=np.float32)))
+            oy = _round_half_away(float(np.sin(th, dtype=np.float32)))
+            xp, yp, xm, ym = x + ox, y + oy, x - ox, y - oy
+            if not (0 <= xp < W and 0 <= yp < H and 0 <= xm < W and 0 <= ym < H):
+                margin[y, x] = m
+                continue
+            o0, op, om = Od[maxori, y, x], Od[maxori, yp, xp], Od[maxori, ym, xm]
+            e0, ep, em = E[maxori, y, x], E[maxori, yp, xp], E[maxori, ym, xm]
+            c0, cp, cm = C[maxori, y, x], C[maxori, yp, xp], C[maxori, ym, xm]
+            romax, romin, rozc = o0 > op and o0 > om, o0 < op and o0 < om, op * om < 0
+            remax, remin, rezc = e0 > ep and e0 > em, e0 < ep and e0 < em, ep * em < 0
+            m = min(m, abs(o0 - op), abs(o0 - om), abs(e0 - ep), abs(e0 - em), abs(op), abs(om), abs(ep),
+                    abs(em), abs(c0 - cp), abs(c0 - cm))
+            margin[y, x] = m
+            if (romax or romin or remax or remin) and (rezc or rozc) and not (c0 <= cp or c0 <= cm):
+                t = 4 if (rezc and romin) else 3 if (rezc and romax) else 2 if (rozc and remin) else \
+                    1 if (rozc and remax) else 0
+                typ[y, x] = t
+                ori[y, x] = th
+                res[y, x] = c0
+    return res, ori, typ, margin

@@ -339,3 +339,31 @@ def test_color_features_match_oracle():
     assert got.shape == (len(rec), 24)
     assert np.array_equal(np.isnan(got), np.isnan(ref))
     assert np.array_equal(np.nan_to_num(got), np.nan_to_num(ref))
+
+
+@pytest.mark.parametrize("w,h,lam", [(320, 240, [4.0, 5.656854, 8.0]), (512, 512, [4.0, 11.313707])])
+def test_lines_edges_match_oracle(w, h, lam):
+    """bimp_detect_lines_edges against the FP64 restatement of detectLE:
+    identical types and orientations except where a decision of the oracle is
+    within 1e-4 of the map peak of a tie; strengths within 1e-4 of the peak."""
+    img = synth.synth_image(w, h, 12, seed=41 + w)
+    res = O.run(img, lam)
+    cs, rec, n = _run_gpu(img, lam)
+    for i, r in enumerate(res):
+        sc = r["scale"]
+        Ct, E, Od = O.complex_cells(r["data"], sc)
+        ref, ori, typ, margin = O.detect_lines_edges(E, Od, Ct, sc)
+        g_res, g_ori, g_typ = (t.cpu().numpy() for t in cs.lines_edges(i))
+        peak = Ct.max()
+        near = margin < 1e-4 * peak
+        diff = (g_typ != typ) & ~near
+        assert not diff.any(), (i, int(diff.sum()), np.argwhere(diff)[:5])
+        both = (g_typ == typ) & (typ > 0)
+        assert both.sum() > 0.9 * (typ > 0).sum()
+        assert np.array_equal(g_ori[both], ori[both])
+        assert np.abs(g_res[both] - ref[both]).max() <= 1e-4 * peak
+        # the caller's summed map gives the same as the default
+        import torch
+        ch = torch.from_numpy(np.ascontiguousarray(Ct[:, :sc.dataH, :sc.dataW].sum(0), dtype=np.float32)).cuda()
+        g2 = cs.lines_edges(i, ch=ch)[2].cpu().numpy()
+        assert ((g2 != g_typ) & ~near).sum() == 0

@@ -187,3 +187,28 @@ def test_color_features_quirks():
     assert f[16:].sum() == 0 and f[1:8].sum() == 0
     bgr[..., 0] = 0       # open interval: 0 is not in (0, 31.875)
     assert O.color_features([10.0], [10.0], [16.0], bgr)[0][:8].sum() == 0
+
+
+def test_lines_edges_known_answers():
+    """detectLE restatement: a bright 1-pixel line is a positive line, a dark
+    one a negative line; opposite step edges get opposite edge types; all at
+    the dominant orientation 0 (vertical structures)."""
+    sc = O.scale_geometry(128, 96, [4.0])[0]
+
+    def run(img):
+        C, E, Od = O.complex_cells(O.level_image(img, sc), sc)
+        return O.detect_lines_edges(E, Od, C, sc)
+
+    line = np.full((96, 128), 60, np.uint8)
+    line[:, 64] = 200
+    r, o, ty, _ = run(line)
+    assert (ty[20:76, 64] == 1).all() and (o[20:76, 64] == 0).all() and (r[20:76, 64] > 0).all()
+    assert (ty[20:76, 40:60] == 0).all()
+    r, o, ty, _ = run(255 - line)
+    assert (ty[20:76, 64] == 2).all()
+    step = np.full((96, 128), 60, np.uint8)
+    step[:, 64:] = 200
+    t_up = run(step)[2][20:76, 64]
+    t_down = run(255 - step)[2][20:76, 64]
+    assert set(np.unique(t_up)) | set(np.unique(t_down)) == {3, 4}
+    assert (t_up != t_down).all()
