@@ -159,6 +159,21 @@ def algorithmic_bytes(cs) -> dict:
     return {"gabor": gabor, "stencil": stencil, "nms": nms}
 
 
+def fft_flops(cs) -> float:
+    """FFT arithmetic of one tile-kernel launch (5 N log2 N per complex N-point
+    transform): per 128 x 128 tile a forward real transform (64 packed rows
+    and 65 half-spectrum columns) and per orientation the spectrum product,
+    128 column and V row inverse transforms and V^2 magnitudes."""
+    per_fft = 5 * 128 * 7
+    total = 0.0
+    for k in cs.ks:
+        v = 128 - 2 * k["kernel_x"]
+        tiles = -(-(k["data_w"] + 1) // v) * -(-(k["data_h"] + 2) // v)
+        per_tile = (64 + 65) * per_fft + 8 * (2 * 128 * 128 + (128 + v) * per_fft + 3 * v * v)
+        total += tiles * per_tile
+    return total
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -258,6 +273,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     for name in ("stencil", "nms"):
         a_gbs = alg[name] / (stage_ms[name] * 1e-3) / 1e9
         roofline[f"{name}_frac"] = round(a_gbs / peak, 4)
+    # the tile kernel is bound by FP32 FFT arithmetic, not HBM: its FFT
+    # flop rate against the nominal FP32 CUDA-core peak, for context
+    fl = fft_flops(cs)
+    roofline["fp32_context"] = {"fft_gflop_per_launch": round(fl / 1e9, 3),
+                                "tflops": round(fl / (stage_ms["gabor"] * 1e-3) / 1e12, 2),
+                                "nominal_fp32_tflops": 74.4,
+                                "frac_of_nominal": round(fl / (stage_ms["gabor"] * 1e-3) / 74.4e12, 3)}
 
     # -- end to end through the host-buffer C ABI ---------------------------
     e2e = None
