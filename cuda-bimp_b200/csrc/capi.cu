@@ -125,7 +125,7 @@ struct Engine {
   unsigned int* d_fault = nullptr;      // set by the tile kernel if a bounded wait expired
   KpOut* d_outs = nullptr;
   std::vector<PyrJob> h_pyr;                 // grouped by level
-  std::vector<int> pyrFirst, pyrCount, pyrMaxW, pyrMaxH;
+  std::vector<int> pyrFirst, pyrCount, pyrLevels, pyrMaxW, pyrMaxH;   // per launch (up to 3 levels)
   PyrJob* d_pyr = nullptr;
   std::vector<size_t> imgKpOffset;           // internal keypoint buffers (batch)
   float* d_kpInternal = nullptr;
@@ -303,20 +303,24 @@ struct Engine {
       }
     }
     imgRowStart.push_back(static_cast<int>(rows.size()));
-    // pyramid jobs grouped by level
-    pyrFirst.clear(); pyrCount.clear(); pyrMaxW.clear(); pyrMaxH.clear(); h_pyr.clear();
-    for (int l = 1; l <= maxLevel; ++l) {
+    // pyramid jobs: up to 3 levels per launch (levels 1-3 from level 0,
+    // 4-6 from level 3, ...)
+    pyrFirst.clear(); pyrCount.clear(); pyrLevels.clear(); pyrMaxW.clear(); pyrMaxH.clear(); h_pyr.clear();
+    for (int base = 0; base < maxLevel; base += 3) {
+      const int K = std::min(3, maxLevel - base);
       pyrFirst.push_back(static_cast<int>(h_pyr.size()));
       int mw = 0, mh = 0;
       for (int i = 0; i < n; ++i) {
-        PyrJob j;
-        j.sw = lvlW[i][l - 1]; j.sh = lvlH[i][l - 1]; j.sp = lvlP[i][l - 1];
-        j.dw = lvlW[i][l]; j.dh = lvlH[i][l]; j.dp = lvlP[i][l];
-        j.src = nullptr; j.dst = nullptr;
+        PyrJob j{};
+        j.sw = lvlW[i][base]; j.sh = lvlH[i][base]; j.sp = lvlP[i][base];
+        for (int m = 0; m < K; ++m) {
+          j.dw[m] = lvlW[i][base + m + 1]; j.dh[m] = lvlH[i][base + m + 1]; j.dp[m] = lvlP[i][base + m + 1];
+        }
         h_pyr.push_back(j);
-        mw = std::max(mw, j.dw); mh = std::max(mh, j.dh);
+        mw = std::max(mw, j.dw[K - 1]); mh = std::max(mh, j.dh[K - 1]);
       }
       pyrCount.push_back(n);
+      pyrLevels.push_back(K);
       pyrMaxW.push_back(mw);
       pyrMaxH.push_back(mh);
     }
@@ -379,10 +383,11 @@ struct Engine {
         d.nmsMask = reinterpret_cast<unsigned int*>(base + offMask[e2]);
       }
     }
-    for (int l = 1, k = 0; l <= maxLevel; ++l)
+    for (size_t g = 0, k = 0; g < pyrFirst.size(); ++g)
       for (int i = 0; i < n; ++i, ++k) {
-        h_pyr[k].src = lvl[i][l - 1];
-        h_pyr[k].dst = lvl[i][l];
+        const int base = 3 * static_cast<int>(g);
+        h_pyr[k].src = lvl[i][base];
+        for (int m = 0; m < pyrLevels[g]; ++m) h_pyr[k].dst[m] = lvl[i][base + m + 1];
       }
     // TMA tensor maps of the complex-cell maps (the stencil's staging)
     std::vector<TensorMapBlob> maps(sds.size());
@@ -441,7 +446,7 @@ struct Engine {
     switch (which) {
       case 0:
         for (size_t l = 0; l < pyrFirst.size(); ++l)
-          launch_pyr(d_pyr + pyrFirst[l], pyrCount[l], pyrMaxW[l], pyrMaxH[l], s);
+          launch_pyr(d_pyr + pyrFirst[l], pyrCount[l], pyrLevels[l], pyrMaxW[l], pyrMaxH[l], s);
         break;
       case 1:
         if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s);

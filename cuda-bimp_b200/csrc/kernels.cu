@@ -35,27 +35,95 @@ __device__ __forceinline__ int reflect101(int i, int n) {
 
 // dst(y,x) = rint(sum w_i w_j src(r101(2y+i), r101(2x+j)) / 256), w = 1 4 6 4 1.
 // The weighted sum is an exact integer; ties round to even (cvt.rni).
-__global__ void k_pyr_down(const PyrJob* __restrict__ jobs) {
-  const PyrJob j = jobs[blockIdx.z];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= j.dw || y >= j.dh) return;
-  const int w5[5] = {1, 4, 6, 4, 1};
-  int cols[5];
+//
+// K levels in one launch: a CTA owns a T x T tile of the deepest level
+// (T = 8, 16, 32 for K = 3, 2, 1) and the 2x, 4x larger tiles above it; it
+// loads the source region the tile depends on (5-tap support, reflect-101
+// at the level edges) into shared memory and computes each level's region
+// from the one above, writing the part it owns.
+constexpr int pyr_tile(int K) { return 32 >> (K - 1); }
+
+// reflect101 for indices at most one period outside [0, n) (the 5-tap
+// support, n >= 2); the general form for n == 1
+__device__ __forceinline__ int reflect101_near(int i, int n) {
+  if (n == 1) return 0;
+  i = i < 0 ? -i : i;
+  i = i >= n ? 2 * n - 2 - i : i;
+  return i < 0 ? -i : i;
+}
+constexpr int pyr_side(int K, int m) { return m == K ? pyr_tile(K) : 2 * pyr_side(K, m + 1) + 3; }
+constexpr int pyr_smem(int K) {
+  return K == 3 ? pyr_side(3, 0) * pyr_side(3, 0) + pyr_side(3, 1) * pyr_side(3, 1) +
+                      pyr_side(3, 2) * pyr_side(3, 2) + pyr_side(3, 3) * pyr_side(3, 3)
+       : K == 2 ? pyr_side(2, 0) * pyr_side(2, 0) + pyr_side(2, 1) * pyr_side(2, 1) + pyr_side(2, 2) * pyr_side(2, 2)
+                : pyr_side(1, 0) * pyr_side(1, 0) + pyr_side(1, 1) * pyr_side(1, 1);
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ jobs) {
+  __shared__ uint8_t s_lvl[pyr_smem(K)];
+  const PyrJob& j = jobs[blockIdx.z];
+  constexpr int T = pyr_tile(K);
+  const int oy = blockIdx.y * T, ox = blockIdx.x * T;
+  if (oy >= j.dh[K - 1] || ox >= j.dw[K - 1]) return;
+  int loY[K + 1], loX[K + 1], off[K + 1];
+  loY[K] = oy;
+  loX[K] = ox;
 #pragma unroll
-  for (int k = 0; k < 5; ++k) cols[k] = reflect101(2 * x + k - 2, j.sw);
-  int acc = 0;
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const uint8_t* row = j.src + (size_t)reflect101(2 * y + i - 2, j.sh) * j.sp;
-    int h = 0;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) h += w5[k] * row[cols[k]];
-    acc += w5[i] * h;
+  for (int m = K; m >= 1; --m) {
+    loY[m - 1] = 2 * loY[m] - 2;
+    loX[m - 1] = 2 * loX[m] - 2;
   }
-  const int q = acc >> 8;
-  const int v = (acc + 127 + (q & 1)) >> 8;
-  j.dst[(size_t)y * j.dp + x] = (uint8_t)(v > 255 ? 255 : v);
+  off[0] = 0;
+#pragma unroll
+  for (int m = 1; m <= K; ++m) off[m] = off[m - 1] + pyr_side(K, m - 1) * pyr_side(K, m - 1);
+  const int t = threadIdx.x;
+  // source region, clipped to the source level (reflected taps stay inside)
+  {
+    constexpr int S0 = pyr_side(K, 0);
+    for (int idx = t; idx < S0 * S0; idx += blockDim.x) {
+      const int r = idx / S0, c = idx - r * S0;
+      const int gy = loY[0] + r, gx = loX[0] + c;
+      if (gy >= 0 && gy < j.sh && gx >= 0 && gx < j.sw) s_lvl[idx] = j.src[(size_t)gy * j.sp + gx];
+    }
+  }
+  __syncthreads();
+  const int w5[5] = {1, 4, 6, 4, 1};
+#pragma unroll
+  for (int m = 1; m <= K; ++m) {
+    const int Si = pyr_side(K, m - 1), So = pyr_side(K, m);
+    const int Wi = m == 1 ? j.sw : j.dw[m - 2], Hi = m == 1 ? j.sh : j.dh[m - 2];
+    const int Wo = j.dw[m - 1], Ho = j.dh[m - 1];
+    const int own = T << (K - m);
+    const int ownY = oy << (K - m), ownX = ox << (K - m);
+    const uint8_t* in = s_lvl + off[m - 1];
+    uint8_t* outS = s_lvl + off[m];
+    uint8_t* dst = j.dst[m - 1];
+    const int dp = j.dp[m - 1];
+    for (int idx = t; idx < So * So; idx += blockDim.x) {
+      const int r = idx / So, c = idx - r * So;
+      const int y = loY[m] + r, x = loX[m] + c;
+      if (y < 0 || y >= Ho || x < 0 || x >= Wo) continue;
+      int cols[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) cols[k] = reflect101_near(2 * x + k - 2, Wi) - loX[m - 1];
+      int acc = 0;
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const uint8_t* row = in + (reflect101_near(2 * y + i - 2, Hi) - loY[m - 1]) * Si;
+        int h = 0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) h += w5[k] * row[cols[k]];
+        acc += w5[i] * h;
+      }
+      const int q = acc >> 8;
+      int v = (acc + 127 + (q & 1)) >> 8;
+      v = v > 255 ? 255 : v;
+      outS[idx] = (uint8_t)v;
+      if (y >= ownY && y < ownY + own && x >= ownX && x < ownX + own) dst[(size_t)y * dp + x] = (uint8_t)v;
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -721,9 +789,13 @@ cudaError_t configure_kernels() {
   return upload_twiddles();
 }
 
-void launch_pyr(const PyrJob* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s) {
-  dim3 b(32, 8), g((maxW + 31) / 32, (maxH + 7) / 8, njobs);
-  k_pyr_down<<<g, b, 0, s>>>(d_jobs);
+void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s) {
+  if (njobs <= 0 || levels <= 0) return;
+  const int T = 32 >> (levels - 1);
+  dim3 g((maxW + T - 1) / T, (maxH + T - 1) / T, njobs);
+  if (levels == 3) k_pyr_down<3><<<g, 256, 0, s>>>(d_jobs);
+  else if (levels == 2) k_pyr_down<2><<<g, 256, 0, s>>>(d_jobs);
+  else k_pyr_down<1><<<g, 256, 0, s>>>(d_jobs);
 }
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                   cudaStream_t s) {

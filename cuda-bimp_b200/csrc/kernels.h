@@ -11,11 +11,12 @@
 namespace bimp_b200 {
 
 // One pyramid step src (sw x sh, pitch sp) -> dst (dw x dh, pitch dp).
+// Up to three pyrDown levels of one image from one source level.
 struct PyrJob {
   const uint8_t* src;
   int sw, sh, sp;
-  uint8_t* dst;
-  int dw, dh, dp;
+  uint8_t* dst[3];
+  int dw[3], dh[3], dp[3];
 };
 
 // One float pyramid step (same fields; for the transpose, src is the level-l
@@ -40,7 +41,9 @@ cudaError_t configure_kernels();
 size_t gabor_smem_bytes();
 size_t stencil_smem_bytes();
 
-void launch_pyr(const PyrJob* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
+// `levels` (1..3) pyrDown steps per job in one launch; maxW/maxH: largest
+// deepest-level size over the jobs
+void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s);
 // d_fault: word that receives 1 if a bounded device wait expired.
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                   cudaStream_t s);
