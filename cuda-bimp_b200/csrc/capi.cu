@@ -434,7 +434,7 @@ struct Engine {
         outs[i].kp = d_kpInternal + (size_t)i * BIMP_KP_VECTOR_LENGTH * internalKpCap;
         outs[i].ld = internalKpCap;
         outs[i].capacity = internalKpCap;
-        outs[i].pad_ = 0;
+        outs[i].aos = 0;
       }
       BIMP_CUDA(cudaMemcpy(d_outs, outs.data(), sizeof(KpOut) * n, cudaMemcpyHostToDevice));
     }
@@ -628,7 +628,7 @@ int bimp_ctx_scale_info(const bimp_context* c, int s, bimp_scale_info* out) {
 
 static int ctx_run(bimp_context* c, const uint8_t* image, size_t pitch, int width, int height,
                    cudaMemcpyKind kind, float* d_kp, size_t ld, int capacity, int* d_count,
-                   cudaStream_t s) {
+                   cudaStream_t s, int aos = 0) {
   if (!c || !image) return fail(BIMP_ERR_INVALID, "null argument");
   if (width != c->width || height != c->height)
     return fail(BIMP_ERR_INVALID, "image size differs from the context's");
@@ -642,7 +642,7 @@ static int ctx_run(bimp_context* c, const uint8_t* image, size_t pitch, int widt
   o.kp = d_kp;
   o.ld = ld;
   o.capacity = capacity;
-  o.pad_ = 0;
+  o.aos = aos;
   BIMP_CUDA(cudaMemcpyAsync(e.d_outs, &o, sizeof(o), cudaMemcpyHostToDevice, s));
   int rc = e.enqueue(s);
   if (rc != BIMP_OK) return rc;
@@ -682,13 +682,6 @@ static int ensure_host_buffers(bimp_context* c, int capacity) {
     BIMP_CUDA(cudaMalloc(&c->d_kpScratch, sizeof(float) * BIMP_KP_VECTOR_LENGTH * (size_t)capacity));
     c->d_kpScratchCap = capacity;
   }
-  if (c->h_kpCap < capacity) {
-    if (c->h_kp) cudaFreeHost(c->h_kp);
-    c->h_kp = nullptr;
-    c->h_kpCap = 0;
-    BIMP_CUDA(cudaMallocHost(&c->h_kp, sizeof(float) * BIMP_KP_VECTOR_LENGTH * (size_t)capacity));
-    c->h_kpCap = capacity;
-  }
   return BIMP_OK;
 }
 
@@ -701,30 +694,20 @@ int bimp_detect_host(bimp_context* c, const uint8_t* image, size_t pitch, int wi
   const int cap = std::max(capacity, 1);
   int rc = ensure_host_buffers(c, cap);
   if (rc != BIMP_OK) return rc;
+  // the NMS writes cv::KeyPoint-layout records straight into the scratch
   rc = ctx_run(c, image, pitch, width, height, cudaMemcpyHostToDevice, c->d_kpScratch, cap,
-               capacity, nullptr, s);
+               capacity, nullptr, s, 1);
   if (rc != BIMP_OK) return rc;
   BIMP_CUDA(cudaMemcpyAsync(c->h_count, c->eng.d_totals, sizeof(int), cudaMemcpyDeviceToHost, s));
   BIMP_CUDA(cudaMemcpyAsync(c->h_count + 1, c->eng.d_fault, sizeof(int), cudaMemcpyDeviceToHost, s));
   BIMP_CUDA(cudaStreamSynchronize(s));
   const int total = *c->h_count;
-  if (c->h_count[1]) return fail(BIMP_ERR_CUDA, "a bounded device wait expired in the tile kernel");
+  if (c->h_count[1]) return fail(BIMP_ERR_CUDA, "a bounded device wait expired");
   const int n = std::min(total, capacity);
   if (n > 0) {
-    float* hk = reinterpret_cast<float*>(c->h_kp);
-    BIMP_CUDA(cudaMemcpy2DAsync(hk, sizeof(float) * n, c->d_kpScratch, sizeof(float) * cap,
-                                sizeof(float) * n, BIMP_KP_VECTOR_LENGTH, cudaMemcpyDeviceToHost, s));
+    static_assert(sizeof(bimp_keypoint) == 7 * sizeof(float), "record layout");
+    BIMP_CUDA(cudaMemcpyAsync(out, c->d_kpScratch, sizeof(bimp_keypoint) * (size_t)n, cudaMemcpyDeviceToHost, s));
     BIMP_CUDA(cudaStreamSynchronize(s));
-    for (int j = 0; j < n; ++j) {
-      bimp_keypoint& k = out[j];
-      k.x = hk[BIMP_X_ROW * n + j];
-      k.y = hk[BIMP_Y_ROW * n + j];
-      std::memcpy(&k.class_id, &hk[BIMP_LAPLACIAN_ROW * n + j], 4);
-      std::memcpy(&k.octave, &hk[BIMP_OCTAVE_ROW * n + j], 4);
-      k.size = hk[BIMP_SIZE_ROW * n + j];
-      k.angle = hk[BIMP_ANGLE_ROW * n + j];
-      k.response = hk[BIMP_HESSIAN_ROW * n + j];
-    }
   }
   *n_found = total;
   if (total > capacity)

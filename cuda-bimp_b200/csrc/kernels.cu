@@ -619,14 +619,25 @@ k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int
           if (denx != 0.f) xpos += __fdiv_rn(numx, denx);
           if (deny != 0.f) ypos += __fdiv_rn(numy, deny);
           float* kpm = out.kp;
-          const size_t ld = out.ld;
-          kpm[0 * ld + idx] = xpos * pyr;
-          kpm[1 * ld + idx] = ypos * pyr;
-          reinterpret_cast<int*>(kpm)[2 * ld + idx] = 1;
-          reinterpret_cast<int*>(kpm)[3 * ld + idx] = kpOctave;
-          kpm[4 * ld + idx] = kpSize;
-          kpm[5 * ld + idx] = -1.f;
-          kpm[6 * ld + idx] = xv2;
+          if (out.aos) {   // pt.x, pt.y, size, angle, response, octave, class_id
+            float* k = kpm + (size_t)7 * idx;
+            k[0] = xpos * pyr;
+            k[1] = ypos * pyr;
+            k[2] = kpSize;
+            k[3] = -1.f;
+            k[4] = xv2;
+            reinterpret_cast<int*>(k)[5] = kpOctave;
+            reinterpret_cast<int*>(k)[6] = 1;
+          } else {
+            const size_t ld = out.ld;
+            kpm[0 * ld + idx] = xpos * pyr;
+            kpm[1 * ld + idx] = ypos * pyr;
+            reinterpret_cast<int*>(kpm)[2 * ld + idx] = 1;
+            reinterpret_cast<int*>(kpm)[3 * ld + idx] = kpOctave;
+            kpm[4 * ld + idx] = kpSize;
+            kpm[5 * ld + idx] = -1.f;
+            kpm[6 * ld + idx] = xv2;
+          }
         }
       }
       base += __popc(bal);

@@ -30,11 +30,14 @@ struct PyrJobF {
 };
 
 // Keypoint destination of one image: 7 x ld float matrix, `capacity` columns.
+// Keypoint destination of one image: a 7 x ld SURF-layout float matrix
+// (rows X, Y, LAPLACIAN, OCTAVE, SIZE, ANGLE, HESSIAN), or with aos = 1 an
+// array of bimp_keypoint records (7 words each, cv::KeyPoint field order).
 struct KpOut {
   float* kp;
   size_t ld;
   int capacity;
-  int pad_;
+  int aos;
 };
 
 cudaError_t configure_kernels();

@@ -135,7 +135,7 @@ extern "C" int bimp_extract_keypoints_noalloc(const float* d_map, size_t ld, int
   out.kp = d_kp;
   out.ld = kp_ld;
   out.capacity = capacity;
-  out.pad_ = 0;
+  out.aos = 0;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   k_noalloc_setup<<<std::max(1, std::min(64, (nrows + 255) / 256)), 256, 0, st>>>(s, sd, out, nrows);
   dim3 g((width + 255) / 256 < 8 ? (width + 255) / 256 : 8, std::min(height, 1024));
