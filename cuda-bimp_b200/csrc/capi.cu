@@ -493,11 +493,8 @@ struct bimp_context {
   Engine eng;
   int width = 0, height = 0;
   std::vector<ScaleHost> info;
-  // pinned staging for the host path
-  bimp_keypoint* h_kp = nullptr;
-  int h_kpCap = 0;
-  bimp_keypoint* d_aos = nullptr;
-  int d_aosCap = 0;
+  // host path: pinned count/fault words; device scratch the NMS writes
+  // cv::KeyPoint records into before the single copy to the caller's array
   int* h_count = nullptr;   // pinned: [0] keypoint total, [1] device fault word
   float* d_kpScratch = nullptr;
   int d_kpScratchCap = 0;
@@ -597,9 +594,7 @@ int bimp_ctx_destroy(bimp_context* c) {
   if (!c) return BIMP_OK;
   cudaSetDevice(c->eng.device);
   c->eng.release();
-  if (c->h_kp) cudaFreeHost(c->h_kp);
   if (c->h_count) cudaFreeHost(c->h_count);
-  if (c->d_aos) cudaFree(c->d_aos);
   if (c->d_kpScratch) cudaFree(c->d_kpScratch);
   if (c->d_leZ) cudaFree(c->d_leZ);
   if (c->d_leSd) cudaFree(c->d_leSd);

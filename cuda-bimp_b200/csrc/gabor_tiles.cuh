@@ -3,35 +3,91 @@
 //
 // One CTA (512 threads, 16 warps) per tile.  The tile's real input window is
 // read from the pyramid level through the reference's padded-torus index map,
-// transformed once (forward 2D FFT, Hermitian half kept in shared memory),
-// and then for each of the 8 orientations the spectrum is multiplied by that
-// orientation's real Gabor spectrum G_o, inverse transformed as one complex
-// FFT (e + i o) and reduced to |e + i o| on the valid outputs.  The
-// differentiable variant also stores e + i o and the tile's image spectrum
-// for the adjoint.
+// transformed once (forward 2D FFT, Hermitian half), and the full spectrum is
+// written to tensor memory (TMEM): lane p holds column p, 32-bit columns
+// 2 py and 2 py + 1 the real and imaginary parts of row py.  Thread t reads
+// only lane t mod 128, which is the lane its warp may access, so the spectrum
+// product pass of every orientation fetches its 8 values with one tcgen05.ld
+// and no Hermitian lookup.  For each of the 8 orientations the spectrum is
+// multiplied by that orientation's real Gabor spectrum G_o, inverse
+// transformed as one complex FFT (e + i o) and reduced to |e + i o| on the
+// valid outputs.  The differentiable variant also stores e + i o and the
+// tile's image spectrum for the adjoint.
 //
-// G_o (64 KB per orientation, L2-resident) is streamed into a double buffer of
-// 16 KB chunks with TMA bulk copies (cp.async.bulk + mbarrier): chunk c + 2 is
-// issued as soon as every thread has finished with chunk c, so the next
-// orientation's first chunks load during the current orientation's last three
-// passes.  Every mbarrier wait is bounded; on expiry the kernel records a
-// fault in *fault, waits once more (bounded) for its copies and carries on,
-// and the host reports the fault.
+// G_o (64 KB per orientation, L2-resident) is streamed in 16 KB chunks with
+// TMA bulk copies (cp.async.bulk + mbarrier) into a ring of 6 chunk slots:
+// the four chunks of orientation o + 1 are issued as soon as orientation o's
+// spectrum product pass is complete and land during its three remaining
+// passes, so that pass needs no barrier of its own.  Every mbarrier wait is
+// bounded; on expiry the kernel records a fault in *fault, waits once more
+// (bounded) for its copies and carries on, and the host reports the fault.
 //
 // Included inside namespace bimp_b200 by kernels.cu, after the helpers it uses
-// (pad_src, pmod, spectrum_at, c_w128).
+// (pad_src, pmod, c_w128).
 #pragma once
 
 constexpr int kGChunkRows = 32;                          // rows of G per chunk
 constexpr int kGChunkFloats = kGChunkRows * kTile;       // 4096 floats = 16 KB
+constexpr int kGSlots = 6;                               // G ring: 1.5 orientations
 constexpr int kSmemW = kTile * kTile * 8;                // work buffer 128 x 128 complex
-constexpr int kSmemXh = kTile * kXhCols * 8;             // Hermitian half spectrum
-constexpr int kSmemG = 2 * kGChunkFloats * 4;            // G double buffer
+constexpr int kSmemXh = kTile * kXhCols * 8;             // Hermitian half spectrum (adjoint kernel)
+constexpr int kSmemG = kGSlots * kGChunkFloats * 4;      // G chunk ring
 constexpr int kSmemTw = 8 * 17 * 8;                      // twiddles w128^(n1*k2)
 constexpr int kSmemMaps = 2 * kTile * 2;                 // int16 row / column maps
-constexpr int kSmemBars = 2 * 8;                         // two mbarriers
-constexpr int kGaborSmem = kSmemW + kSmemXh + kSmemG + kSmemTw + kSmemMaps + kSmemBars;
+constexpr int kSmemBars = kGSlots * 8 + 8;               // ring mbarriers + the TMEM base address
+constexpr int kGaborSmem = kSmemW + kSmemG + kSmemTw + kSmemMaps + kSmemBars;
 static_assert(kGaborSmem <= 232448, "tile kernel exceeds the 227 KB shared-memory limit");
+// During the forward transform the Hermitian half lives in rows 64..127 of
+// the work buffer (slots 0..63, 64 complex per row) and in ring slot 4 (the
+// Nyquist slot 64): orientation 0's chunks occupy slots 0..3 at that time.
+constexpr int kNyqSlot = 4;
+static_assert(kNyqSlot >= 4 && kNyqSlot < kGSlots, "Nyquist scratch must not hold orientation 0's chunks");
+
+// Tensor memory: the tile's full spectrum, 128 lanes x 256 32-bit columns.
+constexpr uint32_t kTmemCols = 2 * kTile;
+
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Whole warp: allocate kTmemCols columns, base address written to dst_smem.
+__device__ __forceinline__ void tmem_alloc_warp(uint32_t dst_smem) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
+               "n"(kTmemCols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_warp(uint32_t taddr) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "n"(kTmemCols) : "memory");
+}
+// Whole warp: each thread stores 8 complex (16 columns from taddr's column)
+// into its own lane and waits for the store to complete.
+__device__ __forceinline__ void tmem_store8(uint32_t taddr, const float2 (&v)[8]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16};\n"
+      "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
+      "r"(__float_as_uint(v[0].x)), "r"(__float_as_uint(v[0].y)), "r"(__float_as_uint(v[1].x)),
+      "r"(__float_as_uint(v[1].y)), "r"(__float_as_uint(v[2].x)), "r"(__float_as_uint(v[2].y)),
+      "r"(__float_as_uint(v[3].x)), "r"(__float_as_uint(v[3].y)), "r"(__float_as_uint(v[4].x)),
+      "r"(__float_as_uint(v[4].y)), "r"(__float_as_uint(v[5].x)), "r"(__float_as_uint(v[5].y)),
+      "r"(__float_as_uint(v[6].x)), "r"(__float_as_uint(v[6].y)), "r"(__float_as_uint(v[7].x)),
+      "r"(__float_as_uint(v[7].y))
+      : "memory");
+}
+// Whole warp: each thread loads 8 complex from its own lane; the values are
+// complete when the statement returns.
+__device__ __forceinline__ void tmem_load8(uint32_t taddr, float2 (&v)[8]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
+}
 
 // |z| as s * rsqrt(s), s = |z|^2 (hardware reciprocal square root, relative
 // error a few 1e-7); exactly 0 for z = 0.
@@ -97,14 +153,22 @@ __device__ __forceinline__ float level_value(const ScaleDev* sd, int r, int c) {
   }
 }
 
+// Element (row, slot) of the Hermitian half during the forward transform:
+// slots 0..63 at Xh64[row * 64 + slot], the Nyquist slot 64 at Nyq[row].
+__device__ __forceinline__ float2* xh_ptr(float2* Xh64, float2* Nyq, int row, int slot) {
+  return slot < 64 ? Xh64 + row * 64 + slot : Nyq + row;
+}
+
 // Index maps of the tile's input window and its forward 2D FFT.
 // rmap/cmap: window row/col -> level row/col through the padded torus.
-// On return Xh holds the Hermitian half X[py][slot] (py = permuted ky,
-// slot = kx 0..64), including the DC of the removed 0.5 offset.  Uses the
-// first 64 rows of W as scratch.  Ends with a barrier.
+// On return the Hermitian half X[py][slot] (py = permuted ky, slot = kx
+// 0..64), including the DC of the removed 0.5 offset, is in Xh64 / Nyq
+// (see xh_ptr).  Uses the first 64 rows of W as scratch.  Ends with a
+// barrier.
 template <bool FLT>
-__device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0, int C0, float2* W, float2* Xh,
-                                                      const float2* tw, short* rmap, short* cmap, int t) {
+__device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0, int C0, float2* W, float2* Xh64,
+                                                      float2* Nyq, const float2* tw, short* rmap, short* cmap,
+                                                      int t) {
   const int kX = sd->kX;
   if (t < kTile) {
     rmap[t] = (short)pad_src(pmod(R0 - kX + t, sd->fftH), sd->dataH, kX);
@@ -150,33 +214,37 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
     const int nk = (128 - kx) & 127;
     const float2 Z = W[widx(r, 8 * (kx & 15) + (kx >> 4))];
     const float2 Zn = W[widx(r, 8 * (nk & 15) + (nk >> 4))];
-    Xh[r * kXhCols + s] = make_float2(0.5f * (Z.x + Zn.x), 0.5f * (Z.y - Zn.y));
-    Xh[(r + 64) * kXhCols + s] = make_float2(0.5f * (Z.y + Zn.y), 0.5f * (Zn.x - Z.x));
+    *xh_ptr(Xh64, Nyq, r, s) = make_float2(0.5f * (Z.x + Zn.x), 0.5f * (Z.y - Zn.y));
+    *xh_ptr(Xh64, Nyq, r + 64, s) = make_float2(0.5f * (Z.y + Zn.y), 0.5f * (Zn.x - Z.x));
   }
   __syncthreads();
   // F3: y-dim pass A on the 65 half columns
   for (int j = t; j < 8 * kXhCols; j += kTileThreads) {
     const int n1 = j / kXhCols, s = j - n1 * kXhCols;
+    float2* col = xh_ptr(Xh64, Nyq, 0, s);
+    const int st = s < 64 ? 64 : 1;
     float2 v[16];
 #pragma unroll
-    for (int m = 0; m < 16; ++m) v[m] = Xh[(n1 + 8 * m) * kXhCols + s];
+    for (int m = 0; m < 16; ++m) v[m] = col[(n1 + 8 * m) * st];
     dft16<false>(v);
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) Xh[(n1 + 8 * k2) * kXhCols + s] = c_mul(v[k2], tw[n1 * 17 + k2]);
+    for (int k2 = 0; k2 < 16; ++k2) col[(n1 + 8 * k2) * st] = c_mul(v[k2], tw[n1 * 17 + k2]);
   }
   __syncthreads();
-  // F4: y-dim pass B -> Xh rows in permuted ky order
+  // F4: y-dim pass B -> rows in permuted ky order
   for (int j = t; j < 16 * kXhCols; j += kTileThreads) {
     const int k2 = j / kXhCols, s = j - k2 * kXhCols;
+    float2* col = xh_ptr(Xh64, Nyq, 0, s);
+    const int st = s < 64 ? 64 : 1;
     float2 v[8];
 #pragma unroll
-    for (int n1 = 0; n1 < 8; ++n1) v[n1] = Xh[(8 * k2 + n1) * kXhCols + s];
+    for (int n1 = 0; n1 < 8; ++n1) v[n1] = col[(8 * k2 + n1) * st];
     dft8<false>(v);
 #pragma unroll
-    for (int k1 = 0; k1 < 8; ++k1) Xh[(8 * k2 + k1) * kXhCols + s] = v[k1];
+    for (int k1 = 0; k1 < 8; ++k1) col[(8 * k2 + k1) * st] = v[k1];
   }
   __syncthreads();
-  if (t == 0) Xh[0].x += 0.5f * (float)(kTile * kTile);   // DC of the removed 0.5 offset
+  if (t == 0) Xh64[0].x += 0.5f * (float)(kTile * kTile);   // DC of the removed 0.5 offset
   __syncthreads();
 }
 
@@ -187,14 +255,15 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
   extern __shared__ float4 smem4[];
   char* base = reinterpret_cast<char*>(smem4);
   float2* W = reinterpret_cast<float2*>(base);
-  float2* Xh = reinterpret_cast<float2*>(base + kSmemW);
-  float* Gbuf = reinterpret_cast<float*>(base + kSmemW + kSmemXh);
-  float2* tw = reinterpret_cast<float2*>(base + kSmemW + kSmemXh + kSmemG);
-  short* rmap = reinterpret_cast<short*>(base + kSmemW + kSmemXh + kSmemG + kSmemTw);
+  float* Gbuf = reinterpret_cast<float*>(base + kSmemW);
+  float2* tw = reinterpret_cast<float2*>(base + kSmemW + kSmemG);
+  short* rmap = reinterpret_cast<short*>(base + kSmemW + kSmemG + kSmemTw);
   short* cmap = rmap + kTile;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kSmemW + kSmemXh + kSmemG + kSmemTw + kSmemMaps);
-  const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
-  const uint32_t gdst0 = smem_u32(Gbuf), gdst1 = smem_u32(Gbuf + kGChunkFloats);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kSmemW + kSmemG + kSmemTw + kSmemMaps);
+  uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(bars + kGSlots);
+  float2* Xh64 = W + 64 * kTile;                                             // forward transform only
+  float2* Nyq = reinterpret_cast<float2*>(Gbuf + kNyqSlot * kGChunkFloats);  // forward transform only
+  const uint32_t bar0 = smem_u32(&bars[0]), gdst0 = smem_u32(Gbuf);
   const int t = threadIdx.x;
 
   if (t < 8 * 17) {
@@ -202,24 +271,30 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     tw[t] = k2 < 16 ? c_w128[(n1 * k2) & 127] : make_float2(0.f, 0.f);
   }
   if (t == 0) {
-    mbar_init(bar0);
-    mbar_init(bar1);
+    for (int i = 0; i < kGSlots; ++i) mbar_init(bar0 + 8 * i);
     fence_mbar_init();
   }
+  if ((t >> 5) == 0) tmem_alloc_warp(smem_u32(tmemSlot));
+  tmem_fence_before();
   __syncthreads();
+  tmem_fence_after();
+  // this thread's lane (t mod 128) of the spectrum; (warp mod 4) * 32 is the
+  // lane block the warp may access
+  const uint32_t tlane = *tmemSlot + ((uint32_t)((t >> 5) & 3) << 21);
 
-  uint32_t gc = 0;       // G chunks consumed by this CTA (identical in every thread)
+  uint32_t ph = 0;       // per ring slot: parity of its next fill (identical in every thread)
   bool fault = false;
   // Where this thread's column p of the full spectrum lives in the
-  // Hermitian half Xh (the same for every tile and orientation): the half
-  // holds kx = 0..64; the other columns are conj(X(-k)), read from row
-  // -ky.  Resolved once, so that the spectrum product pass has no branch.
-  const int pI1 = t & 127;
+  // Hermitian half (the same for every tile): the half holds kx = 0..64; the
+  // other columns are conj(X(-k)), read from row -ky.
+  const int pI1 = t & 127, h = t >> 7;
   const int pa = pI1 >> 3, pb = pI1 & 7;
   const bool pNyq = pb == 4 && pa == 0;
   const bool pConj = pb >= 4 && !pNyq;
   const int pSlot = pb < 4 ? 4 * pa + pb : (pNyq ? 64 : (pa > 0 ? 4 * (16 - pa) + (7 - pb) : 8 - pb));
   const float pSign = pConj ? -1.f : 1.f;
+  const float2* pSrc = pNyq ? Nyq : Xh64 + pSlot;
+  const int pStride = pNyq ? 1 : 64;
 
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const TileWork item = work[w];
@@ -230,19 +305,37 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     const float* __restrict__ G0 = sd->G;
 
     __syncthreads();   // previous tile finished with every buffer
-    if (t == 0) {      // first two chunks of this tile's orientation 0
+    if (t == 0) {      // orientation 0's four chunks into slots 0..3
       fence_proxy_async();
-      bulk_load((gc & 1) ? gdst1 : gdst0, G0, kGChunkFloats * 4, (gc & 1) ? bar1 : bar0);
-      bulk_load(((gc + 1) & 1) ? gdst1 : gdst0, G0 + kGChunkFloats, kGChunkFloats * 4,
-                ((gc + 1) & 1) ? bar1 : bar0);
+      for (int c = 0; c < 4; ++c) bulk_load(gdst0 + c * kGChunkFloats * 4, G0 + c * kGChunkFloats, kGChunkFloats * 4,
+                                            bar0 + 8 * c);
     }
-    tile_forward_spectrum<FLT>(sd, R0, C0, W, Xh, tw, rmap, cmap, t);
+    tile_forward_spectrum<FLT>(sd, R0, C0, W, Xh64, Nyq, tw, rmap, cmap, t);
+    // full spectrum into TMEM: this thread writes the rows py = 8 k2 + k1,
+    // k2 = h + 4 q, that it reads in every orientation's product pass
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+      const int k2 = h + 4 * q;
+      float2 x[8];
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) {
+        // row of -ky in the permuted order (ky = 16 k1 + k2 for py = 8 k2 + k1)
+        const int row = pConj ? (k2 > 0 ? 8 * (16 - k2) + (7 - k1) : (8 - k1) & 7) : 8 * k2 + k1;
+        x[k1] = pSrc[row * pStride];
+        x[k1].y *= pSign;
+      }
+      tmem_store8(tlane + 16 * k2, x);
+    }
     if constexpr (SAVE_Z) {   // the adjoint keeps the tile's image spectrum (Hermitian half)
       if (xsave) {
         float2* __restrict__ xs = xsave + (size_t)w * kSpecHalf;
-        for (int j = t; j < kSpecHalf; j += kTileThreads) xs[j] = Xh[j];
+        for (int j = t; j < kSpecHalf; j += kTileThreads) {
+          const int r = j / kXhCols, sl = j - r * kXhCols;
+          xs[j] = *xh_ptr(Xh64, Nyq, r, sl);
+        }
       }
     }
+    __syncthreads();   // the Hermitian half in W / slot 4 is dead from here
 
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     // tiles holding window column 0 or column dataW of a map with fftW == dataW
@@ -254,34 +347,30 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     const long long cStride = sd->cStride;
     for (int o = 0; o < kNumOri; ++o) {
       float* __restrict__ Cout = C0p + (size_t)o * cStride;
-      // I1: y-dim pass B' with the spectrum product Z = X * G, one 16 KB
-      // chunk of G (rows py in [32q, 32q+32)) per quarter q
+      // I1: y-dim pass B' with the spectrum product Z = X * G; quarter q
+      // uses chunk 4 o + q (G rows py in [32 q, 32 q + 32))
 #pragma unroll 1
       for (int q = 0; q < 4; ++q) {
-        const uint32_t buf = gc & 1;
-        if (!mbar_wait(buf ? bar1 : bar0, (gc >> 1) & 1)) fault = true;
-        const float* Gq = Gbuf + buf * kGChunkFloats;
-        const int p = pI1, k2 = (t >> 7) + 4 * q;
+        const int k2 = h + 4 * q;
+        const int slot = (4 * o + q) % kGSlots;
         float2 v[8];
+        tmem_load8(tlane + 16 * k2, v);
+        if (!mbar_wait(bar0 + 8 * slot, (ph >> slot) & 1)) fault = true;
+        ph ^= 1u << slot;
+        const float* Gq = Gbuf + slot * kGChunkFloats + 8 * h * kTile + pI1;
 #pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) {
-          const int py = 8 * k2 + k1;
-          // row of -ky in the permuted order (ky = 16 k1 + k2 for py = 8 k2 + k1)
-          const int row = pConj ? (k2 > 0 ? 8 * (16 - k2) + (7 - k1) : (8 - k1) & 7) : py;
-          float2 x = Xh[row * kXhCols + pSlot];
-          x.y *= pSign;
-          v[k1] = c_scale(x, Gq[(py - kGChunkRows * q) * kTile + p]);
-        }
+        for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], Gq[k1 * kTile]);
         dft8<true>(v);
 #pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, p)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
-        __syncthreads();   // chunk buffer free, and (q == 3) the pass is complete
-        const int next = 4 * o + q + 2;
-        if (t == 0 && next < 4 * kNumOri) {
-          fence_proxy_async();
-          bulk_load(buf ? gdst1 : gdst0, G0 + (size_t)next * kGChunkFloats, kGChunkFloats * 4, buf ? bar1 : bar0);
+        for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, pI1)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
+      }
+      __syncthreads();   // W complete; every slot of orientation o consumed
+      if (t == 0 && o + 1 < kNumOri) {   // orientation o + 1's chunks land during I2..I4
+        fence_proxy_async();
+        for (int j = 0; j < 4; ++j) {
+          const int c = 4 * (o + 1) + j, sl = c % kGSlots;
+          bulk_load(gdst0 + sl * kGChunkFloats * 4, G0 + (size_t)c * kGChunkFloats, kGChunkFloats * 4, bar0 + 8 * sl);
         }
-        ++gc;
       }
       // I2: y-dim pass A' -> natural y
 #pragma unroll
@@ -358,7 +447,10 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     // a wait expired: record it, then give the copies still in flight a
     // second bounded chance to land before the CTA releases its memory
     if (t == 0) atomicOr(fault_word, 1u);
-    mbar_wait(bar0, ((gc + 1) >> 1) & 1);
-    mbar_wait(bar1, (gc >> 1) & 1);
+    for (int i = 0; i < kGSlots; ++i) mbar_wait(bar0 + 8 * i, ((ph >> i) & 1) ^ 1);
   }
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  if ((t >> 5) == 0) tmem_dealloc_warp(*tmemSlot);
 }

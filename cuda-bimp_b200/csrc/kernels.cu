@@ -142,19 +142,6 @@ __device__ __forceinline__ int pad_src(int t, int nData, int kHalf) {
   return t < nData ? t : (t < nData + kHalf ? nData - 1 : 0);
 }
 
-// X[ky][kx] of the tile spectrum at permuted row position py and permuted
-// column position p, from the Hermitian half Xh[py][slot].
-__device__ __forceinline__ float2 spectrum_at(const float2* __restrict__ Xh, int py, int p) {
-  const int a = p >> 3, b = p & 7;
-  if (b < 4) return Xh[py * kXhCols + 4 * a + b];
-  if (b == 4 && a == 0) return Xh[py * kXhCols + 64];
-  const int slot = a > 0 ? 4 * (16 - a) + (7 - b) : (8 - b);
-  const int c = py >> 3, d = py & 7;
-  const int npy = c > 0 ? 8 * (16 - c) + (7 - d) : ((8 - d) & 7);
-  const float2 v = Xh[npy * kXhCols + slot];
-  return make_float2(v.x, -v.y);
-}
-
 #include "gabor_tiles.cuh"
 
 // ---------------------------------------------------------------------------
