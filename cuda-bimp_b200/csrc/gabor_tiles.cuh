@@ -32,7 +32,7 @@ constexpr int kGSlots = 6;                               // G ring: 1.5 orientat
 constexpr int kSmemW = kTile * kTile * 8;                // work buffer 128 x 128 complex
 constexpr int kSmemXh = kTile * kXhCols * 8;             // Hermitian half spectrum (adjoint kernel)
 constexpr int kSmemG = kGSlots * kGChunkFloats * 4;      // G chunk ring
-constexpr int kSmemTw = 8 * 17 * 8;                      // twiddles w128^(n1*k2)
+constexpr int kSmemTw = 8 * 17 * 8;                      // twiddles w128^(n1*k2) (1 for n1 k2 = 0: not applied)
 constexpr int kSmemMaps = 2 * kTile * 2;                 // int16 row / column maps
 constexpr int kSmemBars = kGSlots * 8 + 8;               // ring mbarriers + the TMEM base address
 constexpr int kGaborSmem = kSmemW + kSmemG + kSmemTw + kSmemMaps + kSmemBars;
@@ -191,7 +191,7 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
     }
     dft16<false>(v);
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) W[widx(r, n1 + 8 * k2)] = c_mul(v[k2], tw[n1 * 17 + k2]);
+    for (int k2 = 0; k2 < 16; ++k2) W[widx(r, n1 + 8 * k2)] = k2 ? c_mul(v[k2], tw[n1 * 17 + k2]) : v[0];
   }
   __syncthreads();
   // F2: x-dim pass B
@@ -228,7 +228,7 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
     for (int m = 0; m < 16; ++m) v[m] = col[(n1 + 8 * m) * st];
     dft16<false>(v);
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) col[(n1 + 8 * k2) * st] = c_mul(v[k2], tw[n1 * 17 + k2]);
+    for (int k2 = 0; k2 < 16; ++k2) col[(n1 + 8 * k2) * st] = k2 ? c_mul(v[k2], tw[n1 * 17 + k2]) : v[0];
   }
   __syncthreads();
   // F4: y-dim pass B -> rows in permuted ky order
@@ -362,7 +362,7 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], Gq[k1 * kTile]);
         dft8<true>(v);
 #pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, pI1)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
+        for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, pI1)] = n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0];
       }
       __syncthreads();   // W complete; every slot of orientation o consumed
       if (t == 0 && o + 1 < kNumOri) {   // orientation o + 1's chunks land during I2..I4
@@ -393,7 +393,7 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
         dft8<true>(v);
 #pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = c_mulc(v[n1], tw[n1 * 17 + k2]);
+        for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0];
       }
       __syncthreads();
       // I4: x-dim pass A' -> natural x; complex magnitude of valid outputs

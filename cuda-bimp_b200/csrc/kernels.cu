@@ -256,7 +256,7 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
   float dmax = -INFINITY;
   // no bounds test needed when every pixel of the block is >= 8 from the edges
   const bool inner = x0 >= kHalo && x0 + kStX <= W - kHalo && y0 >= kHalo && y0 + kStY <= H - kHalo;
-#pragma unroll 1
+#pragma unroll
   for (int i = 0; i < kStY / (NT / 32); ++i) {
     const int ly = ly0 + (NT / 32) * i;
     const int y = y0 + ly;
@@ -281,16 +281,18 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
 }
 
 // Persistent, warp-specialised stencil kernel: one CTA per SM walks the block
-// list.  A producer warp stages block k + 1's complex-cell window (8
-// orientations x 48 rows x 48 floats: the 32 x 32 block plus an 8-pixel halo)
-// as one TMA tensor box into the free one of two buffers, with the block's
-// parameters, while 16 consumer warps compute block k from the other.  Full
-// barriers (TMA bytes) and empty barriers (one arrival per consumer warp)
-// order the two sides; there is no CTA-wide barrier in the loop.  Every wait
-// is bounded; on expiry the kernel sets *fault and stops.
+// list.  A producer warp stages the complex-cell windows (8 orientations x 48
+// rows x 48 floats: a 32 x 32 block plus an 8-pixel halo) as one TMA tensor
+// box each, with the block's parameters, into a ring of kStBufs buffers, so
+// that up to kStBufs - 1 windows are in flight while 16 consumer warps
+// compute the oldest.  Full barriers (TMA bytes) and empty barriers (one
+// arrival per consumer warp) order the two sides; there is no CTA-wide
+// barrier in the loop.  Every wait is bounded; on expiry the kernel sets
+// *fault and stops.
 constexpr int kStConsumers = 512;                    // 16 compute warps
 constexpr int kStThreads = kStConsumers + 32;        // + the producer warp
 constexpr int kStBuf = kNumOri * kStH * kStW;        // floats per staging buffer
+constexpr int kStBufs = 2;                           // staging ring depth (3 measured no faster)
 
 // Everything a consumer needs about its block, written by the producer.
 struct StencilBlk {
@@ -356,31 +358,32 @@ template <int MODE>
 __global__ void __launch_bounds__(kStThreads, 1)
 k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int nwork,
           unsigned int* __restrict__ fault_word) {
-  extern __shared__ float4 s_c4[];   // 2 buffers of kNumOri x kStH x kStW floats (+128 B for alignment)
-  // TMA box destinations are 128-byte aligned
-  float* s_buf = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(s_c4) + 127) & ~uintptr_t(127));
-  __shared__ StencilBlk blk[2];
-  __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
+  extern __shared__ float4 s_c4[];   // kStBufs buffers of kNumOri x kStH x kStW floats (+128 B for alignment)
+  // TMA box destinations are 128-byte aligned.  The offset is added to the
+  // shared-memory pointer itself (not through an integer round trip), so
+  // that the compiler keeps every access to the window a shared-memory load.
+  float* s_buf = reinterpret_cast<float*>(s_c4) + ((128u - (smem_u32(s_c4) & 127u)) & 127u) / 4u;
+  __shared__ StencilBlk blk[kStBufs];
+  __shared__ __align__(8) uint64_t s_full[kStBufs], s_empty[kStBufs];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   if ((int)blockIdx.x >= nwork) return;
-  const uint32_t full0 = smem_u32(&s_full[0]), full1 = smem_u32(&s_full[1]);
-  const uint32_t empty0 = smem_u32(&s_empty[0]), empty1 = smem_u32(&s_empty[1]);
+  const uint32_t full0 = smem_u32(&s_full[0]), empty0 = smem_u32(&s_empty[0]);
   if (t == 0) {
-    mbar_init_count(full0, 1);
-    mbar_init_count(full1, 1);
-    mbar_init_count(empty0, kStConsumers / 32);
-    mbar_init_count(empty1, kStConsumers / 32);
+    for (int i = 0; i < kStBufs; ++i) {
+      mbar_init_count(full0 + 8 * i, 1);
+      mbar_init_count(empty0 + 8 * i, kStConsumers / 32);
+    }
     fence_mbar_init();
   }
   __syncthreads();
   const int nk = (nwork - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;   // blocks of this CTA
   if (warp == kStConsumers / 32) {
-    // producer warp
+    // producer warp: block k goes to buffer k mod kStBufs, its use k / kStBufs
     int issued = 0;
     bool expired = false;
     for (int k = 0; k < nk; ++k) {
-      const int b = k & 1, u = k >> 1;
-      if (u >= 1 && !mbar_wait(b ? empty1 : empty0, (u - 1) & 1)) {   // consumers released use u - 1
+      const int b = k % kStBufs, u = k / kStBufs;
+      if (u >= 1 && !mbar_wait(empty0 + 8 * b, (u - 1) & 1)) {   // consumers released use u - 1
         expired = true;
         break;
       }
@@ -390,22 +393,22 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
       block_origin(sd, item.y, x0, y0);
       stencil_record(sd, x0, y0, blk[b], lane);
       __syncwarp();
-      if (lane == 0) stencil_stage_tma(sd, x0, y0, s_buf + b * kStBuf, b ? full1 : full0);
+      if (lane == 0) stencil_stage_tma(sd, x0, y0, s_buf + b * kStBuf, full0 + 8 * b);
       __syncwarp();
       issued = k + 1;
     }
     if (expired && lane == 0) atomicOr(fault_word, 2u);
-    // before the CTA can end, the last copies into each buffer must land
+    // before the CTA can end, the last copy into each buffer must land
     if (lane == 0) {
-      if (issued >= 1) mbar_wait(((issued - 1) & 1) ? full1 : full0, ((issued - 1) >> 1) & 1);
-      if (issued >= 2) mbar_wait(((issued - 2) & 1) ? full1 : full0, ((issued - 2) >> 1) & 1);
+      for (int k = issued - 1; k >= 0 && k >= issued - kStBufs; --k)
+        mbar_wait(full0 + 8 * (k % kStBufs), (k / kStBufs) & 1);
     }
     return;
   }
   // consumer warps
   for (int k = 0; k < nk; ++k) {
-    const int b = k & 1, u = k >> 1;
-    if (!mbar_wait(b ? full1 : full0, u & 1)) {
+    const int b = k % kStBufs, u = k / kStBufs;
+    if (!mbar_wait(full0 + 8 * b, u & 1)) {
       if (lane == 0) atomicOr(fault_word, 2u);
       break;
     }
@@ -423,7 +426,7 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
     for (int m = 16; m > 0; m >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
     if (lane == 0 && dmax > -INFINITY) atomicMax(B.maxKey, float_key(dmax));
     __syncwarp();
-    if (lane == 0) mbar_arrive(b ? empty1 : empty0);   // this warp is done with buffer b and blk[b]
+    if (lane == 0) mbar_arrive(empty0 + 8 * b);   // this warp is done with buffer b and blk[b]
   }
 }
 
@@ -719,7 +722,7 @@ cudaError_t upload_twiddles() {
 }
 
 size_t gabor_smem_bytes() { return kGaborSmem; }
-size_t stencil_smem_bytes() { return sizeof(float) * 2 * kStBuf + 128; }
+size_t stencil_smem_bytes() { return sizeof(float) * kStBufs * kStBuf + 128; }
 
 namespace {
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
