@@ -18,7 +18,11 @@
 // TMA bulk copies (cp.async.bulk + mbarrier) into a ring of 6 chunk slots:
 // the four chunks of orientation o + 1 are issued as soon as orientation o's
 // spectrum product pass is complete and land during its three remaining
-// passes, so that pass needs no barrier of its own.  Every mbarrier wait is
+// passes, so that pass needs no barrier of its own.  The product pass writes
+// its y-pass output to TMEM as well (lane p = column p), where the second
+// y-pass reads it back; the product pass therefore uses no shared memory,
+// and warps that finish an orientation's last pass start the next
+// orientation's product pass without waiting at a barrier.  Every mbarrier wait is
 // bounded; on expiry the kernel records a fault in *fault, waits once more
 // (bounded) for its copies and carries on, and the host reports the fault.
 //
@@ -43,8 +47,12 @@ static_assert(kGaborSmem <= 232448, "tile kernel exceeds the 227 KB shared-memor
 constexpr int kNyqSlot = 4;
 static_assert(kNyqSlot >= 4 && kNyqSlot < kGSlots, "Nyquist scratch must not hold orientation 0's chunks");
 
-// Tensor memory: the tile's full spectrum, 128 lanes x 256 32-bit columns.
-constexpr uint32_t kTmemCols = 2 * kTile;
+// Tensor memory, 128 lanes x 512 32-bit columns: the tile's full spectrum
+// (columns [0, 256): lane p, columns 2 py, 2 py + 1 = X[py][p]) and the
+// output of the first inverse y-pass (columns [256, 512): lane p, columns
+// 256 + 2 (16 n1 + k2) + {0, 1} = row 8 k2 + n1 of column p).
+constexpr uint32_t kTmemCols = 4 * kTile;
+constexpr uint32_t kTmemY = 2 * kTile;
 
 __device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -72,6 +80,31 @@ __device__ __forceinline__ void tmem_store8(uint32_t taddr, const float2 (&v)[8]
       "r"(__float_as_uint(v[6].x)), "r"(__float_as_uint(v[6].y)), "r"(__float_as_uint(v[7].x)),
       "r"(__float_as_uint(v[7].y))
       : "memory");
+}
+// Whole warp: each thread stores one complex (2 columns) into its own lane;
+// completion is awaited with tmem_wait_st.
+__device__ __forceinline__ void tmem_store1(uint32_t taddr, float2 v) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(__float_as_uint(v.x)),
+               "r"(__float_as_uint(v.y))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+// Whole warp: each thread loads 16 complex (32 columns) from its own lane;
+// the values are complete when the statement returns.
+__device__ __forceinline__ void tmem_load16(uint32_t taddr, float2 (&v)[16]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
 }
 // Whole warp: each thread loads 8 complex from its own lane; the values are
 // complete when the statement returns.
@@ -335,7 +368,9 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         }
       }
     }
+    tmem_fence_before();
     __syncthreads();   // the Hermitian half in W / slot 4 is dead from here
+    tmem_fence_after();
 
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     // tiles holding window column 0 or column dataW of a map with fftW == dataW
@@ -362,9 +397,15 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], Gq[k1 * kTile]);
         dft8<true>(v);
 #pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) W[widx(8 * k2 + n1, pI1)] = n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0];
+        for (int n1 = 0; n1 < 8; ++n1)
+          tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0]);
       }
-      __syncthreads();   // W complete; every slot of orientation o consumed
+      tmem_wait_st();
+      tmem_fence_before();
+      // the y-pass output is complete, every slot of orientation o is
+      // consumed, and (previous orientation) no thread still reads W
+      __syncthreads();
+      tmem_fence_after();
       if (t == 0 && o + 1 < kNumOri) {   // orientation o + 1's chunks land during I2..I4
         fence_proxy_async();
         for (int j = 0; j < 4; ++j) {
@@ -376,15 +417,16 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
 #pragma unroll
       for (int it = 0; it < 2; ++it) {
         const int j = t + it * kTileThreads;
-        const int p = j & 127, n1 = j >> 7;
+        const int p = j & 127, n1 = j >> 7;   // p = this thread's lane
         float2 v[16];
-#pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(8 * k2 + n1, p)];
+        tmem_load16(tlane + kTmemY + 32 * n1, v);
         dft16<true>(v);
 #pragma unroll
         for (int n2 = 0; n2 < 16; ++n2) W[widx(n1 + 8 * n2, p)] = v[n2];
       }
-      __syncthreads();
+      tmem_fence_before();
+      __syncthreads();   // W holds the y-transformed tile; the TMEM y-pass area is free
+      tmem_fence_after();
       // I3: x-dim pass B' on the rows holding valid outputs
       for (int j = t; j < V * 16; j += kTileThreads) {
         const int y = kX + (j >> 4), k2 = j & 15;
@@ -440,7 +482,8 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
           }
         }
       }
-      __syncthreads();
+      // no barrier here: the next orientation's I1 touches only TMEM and the
+      // G ring, so warps done with I4 start it while the others finish
     }
   }
   if (fault) {
