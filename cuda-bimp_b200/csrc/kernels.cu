@@ -303,32 +303,63 @@ struct StencilBlk {
   unsigned int* maxKey;
 };
 
-__device__ __forceinline__ void block_origin(const ScaleDev* sd, int blk, int& x0, int& y0) {
-  const int nbx = (sd->dataW + kStX - 1) / kStX;
-  const int by = blk / nbx;
-  x0 = (blk - by * nbx) * kStX;
-  y0 = by * kStY;
+// One block's record as the producer lanes hold it in registers between
+// fetching it from global memory and writing it to shared memory: lanes
+// 0..7 the offsets of orientation `lane`, lane 8 the block's scalars, lane 0
+// also the tensor map.  Fetching the next block's record one block ahead
+// hides the dependent global loads (work item -> descriptor -> fields).
+struct StencilPre {
+  int x0, y0, W, H;
+  int e1, e2, i1, i2, h1, h2;
+  int pattern, pitch;
+  float gain, wT, wR;
+  float *D, *S, *T, *R;
+  unsigned int *bits, *maxKey;
+  const void* cMap;
+};
+
+__device__ __forceinline__ StencilPre stencil_fetch(const ScaleDev* __restrict__ sds, const int2* __restrict__ work,
+                                                    int idx, int lane) {
+  StencilPre r;
+  const int2 item = work[idx];
+  const ScaleDev* sd = sds + item.x;
+  r.W = sd->dataW;
+  r.H = sd->dataH;
+  const int nbx = (r.W + kStX - 1) / kStX;
+  const int by = item.y / nbx;
+  r.x0 = (item.y - by * nbx) * kStX;
+  r.y0 = by * kStY;
+  if (lane < kNumOri) {
+    r.e1 = sd->es1[lane]; r.e2 = sd->es2[lane]; r.i1 = sd->in1[lane]; r.i2 = sd->in2[lane];
+    r.h1 = sd->ih1[lane]; r.h2 = sd->ih2[lane];
+  }
+  if (lane == kNumOri) {
+    r.pattern = sd->pattern; r.pitch = sd->dPitch;
+    r.gain = sd->radialGain; r.wT = sd->wTan; r.wR = sd->wRad;
+    r.D = sd->D; r.S = sd->S; r.T = sd->T; r.R = sd->R; r.bits = sd->bits; r.maxKey = sd->maxKey;
+  }
+  if (lane == 0) r.cMap = sd->cMap;
+  return r;
 }
 
-// Lane `lane` (< 8: orientation lane) of the producer fills the block record.
-__device__ __forceinline__ void stencil_record(const ScaleDev* sd, int x0, int y0, StencilBlk& B, int lane) {
-  const int W = sd->dataW, H = sd->dataH;
+// Lane `lane` (< 8: orientation lane) of the producer writes the block record.
+__device__ __forceinline__ void stencil_put(const StencilPre& r, StencilBlk& B, int lane) {
+  const int W = r.W, H = r.H;
   if (lane < kNumOri) {
     const int o = lane;
     StencilPar& P = B.P;
-    const int e1 = sd->es1[o], e2 = sd->es2[o], i1 = sd->in1[o], i2 = sd->in2[o];
-    P.e1[o] = e1; P.e2[o] = e2; P.i1[o] = i1; P.i2[o] = i2;
-    P.h1[o] = sd->ih1[o]; P.h2[o] = sd->ih2[o];
-    P.exlo[o] = 2 * abs(e2); P.exhi[o] = W - 2 * abs(e2);
-    P.eylo[o] = 2 * abs(e1); P.eyhi[o] = H - 2 * abs(e1);
-    P.ixlo[o] = 2 * abs(i2); P.ixhi[o] = W - 2 * abs(i2);
-    P.iylo[o] = 2 * abs(i1); P.iyhi[o] = H - 2 * abs(i1);
+    P.e1[o] = r.e1; P.e2[o] = r.e2; P.i1[o] = r.i1; P.i2[o] = r.i2;
+    P.h1[o] = r.h1; P.h2[o] = r.h2;
+    P.exlo[o] = 2 * abs(r.e2); P.exhi[o] = W - 2 * abs(r.e2);
+    P.eylo[o] = 2 * abs(r.e1); P.eyhi[o] = H - 2 * abs(r.e1);
+    P.ixlo[o] = 2 * abs(r.i2); P.ixhi[o] = W - 2 * abs(r.i2);
+    P.iylo[o] = 2 * abs(r.i1); P.iyhi[o] = H - 2 * abs(r.i1);
   } else if (lane == kNumOri) {
-    B.x0 = x0; B.y0 = y0; B.W = W; B.H = H; B.pattern = sd->pattern;
-    B.gain = sd->radialGain; B.wT = sd->wTan; B.wR = sd->wRad;
-    B.out.D = sd->D; B.out.S = sd->S; B.out.T = sd->T; B.out.R = sd->R; B.out.bits = sd->bits;
-    B.out.pitch = sd->dPitch;
-    B.maxKey = sd->maxKey;
+    B.x0 = r.x0; B.y0 = r.y0; B.W = W; B.H = H; B.pattern = r.pattern;
+    B.gain = r.gain; B.wT = r.wT; B.wR = r.wR;
+    B.out.D = r.D; B.out.S = r.S; B.out.T = r.T; B.out.R = r.R; B.out.bits = r.bits;
+    B.out.pitch = r.pitch;
+    B.maxKey = r.maxKey;
   }
 }
 
@@ -336,14 +367,14 @@ __device__ __forceinline__ void stencil_record(const ScaleDev* sd, int x0, int y
 // x0 - 8, y0 - 8) through the entry's tensor map.  x0 - 8 is a multiple of 4
 // floats (16 bytes); parts of the box outside the maps read as zero.  The
 // arrive releases the block record written before it.
-__device__ __forceinline__ void stencil_stage_tma(const ScaleDev* sd, int x0, int y0, float* buf, uint32_t bar) {
+__device__ __forceinline__ void stencil_stage_tma(const void* cMap, int x0, int y0, float* buf, uint32_t bar) {
   fence_proxy_async();   // the buffer was last read through the generic proxy
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((uint32_t)(kStBuf * 4))
                : "memory");
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
           "r"(smem_u32(buf)),
-      "l"(sd->cMap), "r"(x0 - kHalo), "r"(y0 - kHalo), "r"(0), "r"(bar)
+      "l"(cMap), "r"(x0 - kHalo), "r"(y0 - kHalo), "r"(0), "r"(bar)
       : "memory");
 }
 
@@ -381,21 +412,19 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
     // producer warp: block k goes to buffer k mod kStBufs, its use k / kStBufs
     int issued = 0;
     bool expired = false;
+    StencilPre cur = stencil_fetch(sds, work, blockIdx.x, lane);
     for (int k = 0; k < nk; ++k) {
       const int b = k % kStBufs, u = k / kStBufs;
       if (u >= 1 && !mbar_wait(empty0 + 8 * b, (u - 1) & 1)) {   // consumers released use u - 1
         expired = true;
         break;
       }
-      const int2 item = work[blockIdx.x + k * gridDim.x];
-      const ScaleDev* sd = sds + item.x;
-      int x0, y0;
-      block_origin(sd, item.y, x0, y0);
-      stencil_record(sd, x0, y0, blk[b], lane);
+      stencil_put(cur, blk[b], lane);
       __syncwarp();
-      if (lane == 0) stencil_stage_tma(sd, x0, y0, s_buf + b * kStBuf, full0 + 8 * b);
+      if (lane == 0) stencil_stage_tma(cur.cMap, cur.x0, cur.y0, s_buf + b * kStBuf, full0 + 8 * b);
       __syncwarp();
       issued = k + 1;
+      if (k + 1 < nk) cur = stencil_fetch(sds, work, blockIdx.x + (k + 1) * gridDim.x, lane);
     }
     if (expired && lane == 0) atomicOr(fault_word, 2u);
     // before the CTA can end, the last copy into each buffer must land
