@@ -182,7 +182,7 @@ struct bimp_adjoint {
         d.image = i;
         const int entry = static_cast<int>(sds.size());
         for (int tI = 0; tI < d.tilesX * d.tilesY; ++tI) tiles.push_back({entry, tI});
-        const int nbx = (s.dataW + 31) / 32, nby = (s.dataH + 31) / 32;
+        const int nbx = (s.dataW + 31) / 32, nby = (s.dataH + kStencilBlockH - 1) / kStencilBlockH;
         for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
         const int nbx2 = (s.dataW + 1 + 31) / 32, nby2 = (s.dataH + 2 + 31) / 32;   // window + row dataH + 1
         for (int b = 0; b < nbx2 * nby2; ++b) stenB.push_back(make_int2(entry, b));

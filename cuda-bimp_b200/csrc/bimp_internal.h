@@ -21,6 +21,9 @@ constexpr int kTileThreads = 512;
 constexpr int kMaxHalf = 56;               // largest supported kernel half size
 constexpr int kSpecFloats = kTile * kTile; // one orientation's real spectrum
 constexpr int kSpecHalf = kTile * kXhCols;  // Hermitian half of a tile spectrum
+// Forward stencil blocks: 32 columns x kStencilBlockH rows of D per block
+// (the host's block lists and the kernel share this).
+constexpr int kStencilBlockH = 32;
 
 // Per (image, scale) descriptor read by every kernel.  Plain old data.
 struct ScaleDev {

@@ -291,7 +291,7 @@ struct Engine {
         const int entry = static_cast<int>(sds.size());
         d.rowBase = static_cast<int>(rows.size());
         for (int tIdx = 0; tIdx < d.tilesX * d.tilesY; ++tIdx) tiles.push_back({entry, tIdx});
-        const int nbx = (s.dataW + 31) / 32, nby = (s.dataH + 31) / 32;
+        const int nbx = (s.dataW + 31) / 32, nby = (s.dataH + kStencilBlockH - 1) / kStencilBlockH;
         for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
         const int yEnd = std::min(s.dataH - s.off - 1, s.dataH - 2);
         for (int y = s.off + 1; y <= yEnd; ++y) rows.push_back(make_int2(entry, y - s.off - 1));

@@ -147,8 +147,9 @@ __device__ __forceinline__ int pad_src(int t, int nData, int kHalf) {
 // ---------------------------------------------------------------------------
 // stencil: end-stopping, inhibition, summed keypoint map
 // ---------------------------------------------------------------------------
-constexpr int kStX = 32, kStY = 32, kHalo = 8;
-constexpr int kStW = kStX + 2 * kHalo, kStH = kStY + 2 * kHalo;
+constexpr int kStX = 32, kStY = 32, kHalo = 8;   // kStY: the adjoint's stencil blocks
+constexpr int kFwY = kStencilBlockH;               // forward stencil block rows
+constexpr int kStW = kStX + 2 * kHalo, kStH = kFwY + 2 * kHalo;
 
 __device__ __forceinline__ unsigned int float_key(float f) {
   const unsigned int b = __float_as_uint(f);
@@ -255,9 +256,9 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
   const int x = x0 + lx;
   float dmax = -INFINITY;
   // no bounds test needed when every pixel of the block is >= 8 from the edges
-  const bool inner = x0 >= kHalo && x0 + kStX <= W - kHalo && y0 >= kHalo && y0 + kStY <= H - kHalo;
+  const bool inner = x0 >= kHalo && x0 + kStX <= W - kHalo && y0 >= kHalo && y0 + kFwY <= H - kHalo;
 #pragma unroll
-  for (int i = 0; i < kStY / (NT / 32); ++i) {
+  for (int i = 0; i < kFwY / (NT / 32); ++i) {
     const int ly = ly0 + (NT / 32) * i;
     const int y = y0 + ly;
     if (x >= W || y >= H) continue;
@@ -291,6 +292,7 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
 // *fault and stops.
 constexpr int kStConsumers = 512;                    // 16 compute warps
 constexpr int kStThreads = kStConsumers + 32;        // + the producer warp
+constexpr int kStCtasPerSm = 1;                      // resident CTAs per SM (2 with 16-row blocks: no faster)
 constexpr int kStBuf = kNumOri * kStH * kStW;        // floats per staging buffer
 constexpr int kStBufs = 2;                           // staging ring depth (3 measured no faster)
 
@@ -328,7 +330,7 @@ __device__ __forceinline__ StencilPre stencil_fetch(const ScaleDev* __restrict__
   const int nbx = (r.W + kStX - 1) / kStX;
   const int by = item.y / nbx;
   r.x0 = (item.y - by * nbx) * kStX;
-  r.y0 = by * kStY;
+  r.y0 = by * kFwY;
   if (lane < kNumOri) {
     r.e1 = sd->es1[lane]; r.e2 = sd->es2[lane]; r.i1 = sd->in1[lane]; r.i2 = sd->in2[lane];
     r.h1 = sd->ih1[lane]; r.h2 = sd->ih2[lane];
@@ -386,7 +388,7 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kStThreads, 1)
+__global__ void __launch_bounds__(kStThreads, kStCtasPerSm)
 k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int nwork,
           unsigned int* __restrict__ fault_word) {
   extern __shared__ float4 s_c4[];   // kStBufs buffers of kNumOri x kStH x kStW floats (+128 B for alignment)
@@ -870,7 +872,7 @@ void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, i
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigned int* d_fault, cudaStream_t s,
                     int mode) {
   if (nwork <= 0) return;
-  const int grid = std::min(nwork, num_sms());
+  const int grid = std::min(nwork, kStCtasPerSm * num_sms());
   if (mode == kStencilDS)
     k_stencil<kStencilDS><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
   else if (mode == kStencilAdj)
