@@ -503,6 +503,14 @@ struct bimp_context {
   float2* d_leZ = nullptr;
   ScaleDev* d_leSd = nullptr;
   TileWork* d_leTiles = nullptr;
+  // the detection's fixed launch sequence (max reset, pyramid, tile kernel,
+  // stencil, NMS), captured once at creation and launched into the caller's
+  // stream after each call's input copies; null if the capture failed
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  // the output descriptor last copied to the device (skipped when unchanged)
+  KpOut lastOut{};
+  bool outSet = false;
 };
 
 struct bimp_batch {
@@ -528,6 +536,29 @@ int capture_batch(bimp_batch* b) {
   if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
   if (e != cudaSuccess) return fail(BIMP_ERR_CUDA, std::string("batch graph setup: ") + cudaGetErrorString(e));
   return BIMP_OK;
+}
+// Captures a context's launch sequence into its graph.  On any failure the
+// context keeps no graph and launches the same kernels directly.
+void capture_ctx(bimp_context* c) {
+  cudaStream_t cs = nullptr;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    const int rc = c->eng.enqueue(cs);
+    const cudaError_t e = cudaStreamEndCapture(cs, &g);
+    cudaGraphExec_t x = nullptr;
+    if (rc == BIMP_OK && e == cudaSuccess && g && cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+      c->graph = g;
+      c->exec = x;
+      g = nullptr;
+    }
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  cudaStreamDestroy(cs);
 }
 }  // namespace
 
@@ -586,6 +617,7 @@ int bimp_ctx_create(bimp_context** ctx, int width, int height, const float* lamb
     delete c;
     return fail(BIMP_ERR_NOMEM, "cudaMallocHost failed");
   }
+  capture_ctx(c);
   *ctx = c;
   return BIMP_OK;
 }
@@ -593,6 +625,8 @@ int bimp_ctx_create(bimp_context** ctx, int width, int height, const float* lamb
 int bimp_ctx_destroy(bimp_context* c) {
   if (!c) return BIMP_OK;
   cudaSetDevice(c->eng.device);
+  if (c->exec) cudaGraphExecDestroy(c->exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
   c->eng.release();
   if (c->h_count) cudaFreeHost(c->h_count);
   if (c->d_kpScratch) cudaFree(c->d_kpScratch);
@@ -638,9 +672,21 @@ static int ctx_run(bimp_context* c, const uint8_t* image, size_t pitch, int widt
   o.ld = ld;
   o.capacity = capacity;
   o.aos = aos;
-  BIMP_CUDA(cudaMemcpyAsync(e.d_outs, &o, sizeof(o), cudaMemcpyHostToDevice, s));
-  int rc = e.enqueue(s);
-  if (rc != BIMP_OK) return rc;
+  if (!c->outSet || std::memcmp(&o, &c->lastOut, sizeof(o)) != 0) {
+    BIMP_CUDA(cudaMemcpyAsync(e.d_outs, &o, sizeof(o), cudaMemcpyHostToDevice, s));
+    c->lastOut = o;
+    c->outSet = true;
+  }
+  // the captured sequence, unless the caller's stream is itself being
+  // captured (then the kernels go straight into the caller's capture)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BIMP_CUDA(cudaStreamIsCapturing(s, &cap));
+  if (c->exec && cap == cudaStreamCaptureStatusNone) {
+    BIMP_CUDA(cudaGraphLaunch(c->exec, s));
+  } else {
+    const int rc = e.enqueue(s);
+    if (rc != BIMP_OK) return rc;
+  }
   if (d_count) BIMP_CUDA(cudaMemcpyAsync(d_count, e.d_totals, sizeof(int), cudaMemcpyDeviceToDevice, s));
   return BIMP_OK;
 }
