@@ -608,62 +608,78 @@ k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int
   const int kpOctave = sd->kpOctave;
   const unsigned int* __restrict__ mask = sd->nmsMask ? sd->nmsMask + (size_t)item.y * sd->nmsChunks : nullptr;
   const int nch = (xEnd - off - 1 + 31) / 32;
-  // chunks with a keypoint: 32 decision words per load when they are stored
-  for (int c0 = 0; c0 < nch; c0 += 32) {
-    unsigned int words = 0, live;
-    if (mask) {
-      words = c0 + lane < nch ? mask[c0 + lane] : 0u;
-      live = __ballot_sync(0xffffffffu, words != 0u);
+  // One keypoint record: subpixel position from the parabolas through the
+  // 3 samples per axis (cuda_bimp.cuh:114-132), cv::KeyPoint fields.
+  auto emit = [&](int x, int idx) {
+    const float* r1 = D + (size_t)y * dp;
+    const float xv1 = r1[x - 1], xv2 = r1[x], xv3 = r1[x + 1];
+    const float yv1 = r1[x - dp], yv3 = r1[x + dp];
+    float xpos = (float)x, ypos = (float)y;
+    const float denx = xv1 + xv3 - 2.f * xv2;
+    const float deny = yv1 + yv3 - 2.f * xv2;
+    const float numx = 0.5f * (xv1 - xv3);
+    const float numy = 0.5f * (yv1 - yv3);
+    if (denx != 0.f) xpos += __fdiv_rn(numx, denx);
+    if (deny != 0.f) ypos += __fdiv_rn(numy, deny);
+    float* kpm = out.kp;
+    if (out.aos) {   // pt.x, pt.y, size, angle, response, octave, class_id
+      float* k = kpm + (size_t)7 * idx;
+      k[0] = xpos * pyr;
+      k[1] = ypos * pyr;
+      k[2] = kpSize;
+      k[3] = -1.f;
+      k[4] = xv2;
+      reinterpret_cast<int*>(k)[5] = kpOctave;
+      reinterpret_cast<int*>(k)[6] = 1;
     } else {
-      live = nch - c0 >= 32 ? 0xffffffffu : (1u << (nch - c0)) - 1u;
+      const size_t ld = out.ld;
+      kpm[0 * ld + idx] = xpos * pyr;
+      kpm[1 * ld + idx] = ypos * pyr;
+      reinterpret_cast<int*>(kpm)[2 * ld + idx] = 1;
+      reinterpret_cast<int*>(kpm)[3 * ld + idx] = kpOctave;
+      kpm[4 * ld + idx] = kpSize;
+      kpm[5 * ld + idx] = -1.f;
+      kpm[6 * ld + idx] = xv2;
     }
-    while (live) {
-      const int cc = __ffs(live) - 1;
-      live &= live - 1u;
-      const int c = c0 + cc;
-      const int x = off + 1 + 32 * c + lane;
-      const unsigned int bal = mask ? __shfl_sync(0xffffffffu, words, cc)
-                                    : __ballot_sync(0xffffffffu, x < xEnd && is_keypoint(D, dp, x, y, thr));
-      const bool kp = (bal >> lane) & 1u;
-      if (kp) {
-        const int idx = base + __popc(bal & ((1u << lane) - 1u));
-        if (idx < out.capacity) {
-          const float* r1 = D + (size_t)y * dp;
-          const float xv1 = r1[x - 1], xv2 = r1[x], xv3 = r1[x + 1];
-          const float yv1 = r1[x - dp], yv3 = r1[x + dp];
-          float xpos = (float)x, ypos = (float)y;
-          // cuda_bimp.cuh:114-132 (parabola through the 3 samples per axis)
-          const float denx = xv1 + xv3 - 2.f * xv2;
-          const float deny = yv1 + yv3 - 2.f * xv2;
-          const float numx = 0.5f * (xv1 - xv3);
-          const float numy = 0.5f * (yv1 - yv3);
-          if (denx != 0.f) xpos += __fdiv_rn(numx, denx);
-          if (deny != 0.f) ypos += __fdiv_rn(numy, deny);
-          float* kpm = out.kp;
-          if (out.aos) {   // pt.x, pt.y, size, angle, response, octave, class_id
-            float* k = kpm + (size_t)7 * idx;
-            k[0] = xpos * pyr;
-            k[1] = ypos * pyr;
-            k[2] = kpSize;
-            k[3] = -1.f;
-            k[4] = xv2;
-            reinterpret_cast<int*>(k)[5] = kpOctave;
-            reinterpret_cast<int*>(k)[6] = 1;
-          } else {
-            const size_t ld = out.ld;
-            kpm[0 * ld + idx] = xpos * pyr;
-            kpm[1 * ld + idx] = ypos * pyr;
-            reinterpret_cast<int*>(kpm)[2 * ld + idx] = 1;
-            reinterpret_cast<int*>(kpm)[3 * ld + idx] = kpOctave;
-            kpm[4 * ld + idx] = kpSize;
-            kpm[5 * ld + idx] = -1.f;
-            kpm[6 * ld + idx] = xv2;
-          }
-        }
+  };
+  if (mask) {
+    // 32 decision words per round, one per lane: each lane writes its word's
+    // keypoints at the word's place in the row (a warp prefix sum of the
+    // word popcounts keeps x order), so a dense row costs as many steps as
+    // its densest word has bits, not one step per chunk with a keypoint
+    for (int c0 = 0; c0 < nch; c0 += 32) {
+      unsigned int word = c0 + lane < nch ? mask[c0 + lane] : 0u;
+      const int pc = __popc(word);
+      int incl = pc;
+#pragma unroll
+      for (int m = 1; m < 32; m <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, m);
+        if (lane >= m) incl += u;
       }
-      base += __popc(bal);
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      int idx = base + incl - pc;
+      while (word) {
+        const int bit = __ffs(word) - 1;
+        word &= word - 1u;
+        if (idx < out.capacity) emit(off + 1 + 32 * (c0 + lane) + bit, idx);
+        ++idx;
+      }
+      base += total;
       if (base >= out.capacity) return;
     }
+    return;
+  }
+  // no stored decisions: test each chunk's pixels (one ballot per chunk)
+  for (int c = 0; c < nch; ++c) {
+    const int x = off + 1 + 32 * c + lane;
+    const unsigned int bal = __ballot_sync(0xffffffffu, x < xEnd && is_keypoint(D, dp, x, y, thr));
+    if (!bal) continue;
+    if ((bal >> lane) & 1u) {
+      const int idx = base + __popc(bal & ((1u << lane) - 1u));
+      if (idx < out.capacity) emit(x, idx);
+    }
+    base += __popc(bal);
+    if (base >= out.capacity) return;
   }
 }
 
