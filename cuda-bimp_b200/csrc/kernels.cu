@@ -59,9 +59,16 @@ constexpr int pyr_smem(int K) {
                 : pyr_side(1, 0) * pyr_side(1, 0) + pyr_side(1, 1) * pyr_side(1, 1);
 }
 
+// Largest horizontal-pass buffer of a K-level launch (rows of the level
+// above x columns of the level computed).
+constexpr int pyr_hbuf(int K) {
+  return K == 3 ? pyr_side(3, 0) * pyr_side(3, 1) : K == 2 ? pyr_side(2, 0) * pyr_side(2, 1) : pyr_side(1, 0) * pyr_side(1, 1);
+}
+
 template <int K>
 __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ jobs) {
   __shared__ uint8_t s_lvl[pyr_smem(K)];
+  __shared__ uint16_t s_h[pyr_hbuf(K)];
   const PyrJob& j = jobs[blockIdx.z];
   constexpr int T = pyr_tile(K);
   const int oy = blockIdx.y * T, ox = blockIdx.x * T;
@@ -78,13 +85,24 @@ __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ job
 #pragma unroll
   for (int m = 1; m <= K; ++m) off[m] = off[m - 1] + pyr_side(K, m - 1) * pyr_side(K, m - 1);
   const int t = threadIdx.x;
-  // source region, clipped to the source level (reflected taps stay inside)
+  // source region as aligned 4-byte words (rows are 16-byte aligned in the
+  // level buffers).  Bytes outside the level (negative coordinates, or
+  // between the width and the pitch) are never used: reflect-101 keeps every
+  // tap inside the level.
   {
     constexpr int S0 = pyr_side(K, 0);
-    for (int idx = t; idx < S0 * S0; idx += blockDim.x) {
-      const int r = idx / S0, c = idx - r * S0;
-      const int gy = loY[0] + r, gx = loX[0] + c;
-      if (gy >= 0 && gy < j.sh && gx >= 0 && gx < j.sw) s_lvl[idx] = j.src[(size_t)gy * j.sp + gx];
+    constexpr int WPR = (S0 + 3) / 4 + 1;   // words per region row
+    const int a = loX[0] & ~3;
+    for (int idx = t; idx < S0 * WPR; idx += blockDim.x) {
+      const int r = idx / WPR, w = a + 4 * (idx - r * WPR);
+      const int gy = loY[0] + r;
+      if (gy < 0 || gy >= j.sh || w < 0 || w >= j.sp) continue;
+      const uint32_t v = *reinterpret_cast<const uint32_t*>(j.src + (size_t)gy * j.sp + w);
+#pragma unroll
+      for (int bt = 0; bt < 4; ++bt) {
+        const int c = w + bt - loX[0];
+        if (c >= 0 && c < S0) s_lvl[r * S0 + c] = (uint8_t)(v >> (8 * bt));
+      }
     }
   }
   __syncthreads();
@@ -100,22 +118,53 @@ __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ job
     uint8_t* outS = s_lvl + off[m];
     uint8_t* dst = j.dst[m - 1];
     const int dp = j.dp[m - 1];
+    // A region wholly inside the level above needs no reflection: output
+    // column c of the region takes input columns 2 c .. 2 c + 4, row r rows
+    // 2 r .. 2 r + 4.
+    const bool inner = loX[m - 1] >= 0 && loY[m - 1] >= 0 && loX[m - 1] + Si <= Wi && loY[m - 1] + Si <= Hi;
+    if (inner) {
+      for (int idx = t; idx < Si * So; idx += blockDim.x) {
+        const int r = idx / So, c = idx - r * So;
+        const uint8_t* a = in + r * Si + 2 * c;
+        s_h[idx] = (uint16_t)(a[0] + 4 * a[1] + 6 * a[2] + 4 * a[3] + a[4]);
+      }
+      __syncthreads();
+      for (int idx = t; idx < So * So; idx += blockDim.x) {
+        const int r = idx / So, c = idx - r * So;
+        const uint16_t* a = s_h + 2 * r * So + c;
+        const int acc = a[0] + 4 * a[So] + 6 * a[2 * So] + 4 * a[3 * So] + a[4 * So];
+        const int q = acc >> 8;
+        int v = (acc + 127 + (q & 1)) >> 8;
+        v = v > 255 ? 255 : v;
+        outS[idx] = (uint8_t)v;
+        const int y = loY[m] + r, x = loX[m] + c;
+        if (y >= ownY && y < ownY + own && x >= ownX && x < ownX + own && y < Ho && x < Wo)
+          dst[(size_t)y * dp + x] = (uint8_t)v;
+      }
+      __syncthreads();
+      continue;
+    }
+    // horizontal pass: every region row inside the level above, every
+    // output column inside this level (exact integer sums)
+    for (int idx = t; idx < Si * So; idx += blockDim.x) {
+      const int r = idx / So, c = idx - r * So;
+      const int gy = loY[m - 1] + r, x = loX[m] + c;
+      if (gy < 0 || gy >= Hi || x < 0 || x >= Wo) continue;
+      const uint8_t* row = in + r * Si;
+      int h = 0;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) h += w5[k] * row[reflect101_near(2 * x + k - 2, Wi) - loX[m - 1]];
+      s_h[r * So + c] = (uint16_t)h;
+    }
+    __syncthreads();
+    // vertical pass, rounding to nearest with ties to even
     for (int idx = t; idx < So * So; idx += blockDim.x) {
       const int r = idx / So, c = idx - r * So;
       const int y = loY[m] + r, x = loX[m] + c;
       if (y < 0 || y >= Ho || x < 0 || x >= Wo) continue;
-      int cols[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) cols[k] = reflect101_near(2 * x + k - 2, Wi) - loX[m - 1];
       int acc = 0;
 #pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        const uint8_t* row = in + (reflect101_near(2 * y + i - 2, Hi) - loY[m - 1]) * Si;
-        int h = 0;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) h += w5[k] * row[cols[k]];
-        acc += w5[i] * h;
-      }
+      for (int i = 0; i < 5; ++i) acc += w5[i] * (int)s_h[(reflect101_near(2 * y + i - 2, Hi) - loY[m - 1]) * So + c];
       const int q = acc >> 8;
       int v = (acc + 127 + (q & 1)) >> 8;
       v = v > 255 ? 255 : v;
