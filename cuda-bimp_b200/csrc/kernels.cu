@@ -297,37 +297,49 @@ struct StencilOut {
   int pitch;
 };
 
-template <int PAT, int MODE, int NT>
-__device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, const StencilPar& P, int x0, int y0,
-                                               int W, int H, float gain, float wT, float wR, const StencilOut& out) {
+// The rows of one thread (ly0, ly0 + NT/32, ...).  CHECK = false: every
+// pixel of the block is inside the map and at least 8 from its edges, so
+// the rows run as straight-line code whose loads and sums interleave.
+template <bool CHECK, int PAT, int MODE, int NT>
+__device__ __forceinline__ float stencil_rows(const float* __restrict__ s_c, const StencilPar& P, int x0, int y0,
+                                              int W, int H, float gain, float wT, float wR, const StencilOut& out) {
   const int t = threadIdx.x;
   const int lx = t & 31, ly0 = t >> 5;
   const int x = x0 + lx;
-  float dmax = -INFINITY;
-  // no bounds test needed when every pixel of the block is >= 8 from the edges
-  const bool inner = x0 >= kHalo && x0 + kStX <= W - kHalo && y0 >= kHalo && y0 + kFwY <= H - kHalo;
+  constexpr int kRows = kFwY / (NT / 32);
+  float D[kRows], S[kRows], T[kRows], R[kRows];
+  unsigned int b[kRows];
 #pragma unroll
-  for (int i = 0; i < kFwY / (NT / 32); ++i) {
+  for (int i = 0; i < kRows; ++i) {
     const int ly = ly0 + (NT / 32) * i;
-    const int y = y0 + ly;
-    if (x >= W || y >= H) continue;
-    float D, S, T, R;
-    unsigned int b;
-    if (inner)
-      stencil_pixel<false, PAT, MODE>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S, T, R, b);
-    else
-      stencil_pixel<true, PAT, MODE>(s_c, P, x, y, ly + kHalo, lx + kHalo, gain, wT, wR, D, S, T, R, b);
+    stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i], R[i],
+                                    b[i]);
+  }
+  float dmax = -INFINITY;
+#pragma unroll
+  for (int i = 0; i < kRows; ++i) {
+    const int y = y0 + ly0 + (NT / 32) * i;
+    if (CHECK && (x >= W || y >= H)) continue;
     const size_t k = (size_t)y * out.pitch + x;
-    out.D[k] = D;
-    if constexpr (MODE == kStencilDS) out.S[k] = S;
+    out.D[k] = D[i];
+    if constexpr (MODE == kStencilDS) out.S[k] = S[i];
     if constexpr (MODE == kStencilAdj) {
-      out.T[k] = T;
-      out.R[k] = R;
-      out.bits[k] = b;
+      out.T[k] = T[i];
+      out.R[k] = R[i];
+      out.bits[k] = b[i];
     }
-    dmax = fmaxf(dmax, D);
+    dmax = fmaxf(dmax, D[i]);
   }
   return dmax;
+}
+
+template <int PAT, int MODE, int NT>
+__device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, const StencilPar& P, int x0, int y0,
+                                               int W, int H, float gain, float wT, float wR, const StencilOut& out) {
+  // no bounds test needed when every pixel of the block is >= 8 from the edges
+  const bool inner = x0 >= kHalo && x0 + kStX <= W - kHalo && y0 >= kHalo && y0 + kFwY <= H - kHalo;
+  return inner ? stencil_rows<false, PAT, MODE, NT>(s_c, P, x0, y0, W, H, gain, wT, wR, out)
+               : stencil_rows<true, PAT, MODE, NT>(s_c, P, x0, y0, W, H, gain, wT, wR, out);
 }
 
 // Persistent, warp-specialised stencil kernel: one CTA per SM walks the block
