@@ -263,11 +263,14 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
           const int gy = R0 + y - kX, gx = C0 + x - kX;
           ok[u] = y >= kX && y < kX + V && x >= kX && x < kX + V && gy < cRows && gx < cCols;
           const size_t k = ok[u] ? (size_t)o * cStride + (size_t)gy * cPitch + gx : 0;
-          m[u] = ok[u] ? __ldg(sd->C + k) : 0.f;
           gc[u] = ok[u] ? __ldg(sd->gC + k) : 0.f;
           if (ok[u] && wrapW && gx == 0 && gy >= 1) gc[u] += __ldg(sd->gWrap + o * (sd->dataH + 1) + gy - 1);
           z[u] = ok[u] ? __ldg(sd->Z + k) : make_float2(0.f, 0.f);
         }
+        // |z| as the forward computed it (the forward stored C = cmag(z)),
+        // recomputed instead of read back
+#pragma unroll
+        for (int u = 0; u < 4; ++u) m[u] = ok[u] ? cmag(z[u]) : 0.f;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int j = j0 + u * kTileThreads;
