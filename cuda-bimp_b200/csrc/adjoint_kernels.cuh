@@ -73,7 +73,8 @@ __device__ __forceinline__ void block_add_double(double v, double* dst) {
   }
 }
 
-// Over the 32x32 block: sum M * D into loss[0], and -sum M * T, -sum M * R
+// Over one forward stencil block (32 x kStencilBlockH pixels, the forward
+// stencil's block list): sum M * D into loss[0], and -sum M * T, -sum M * R
 // (dL/dw_tan and dL/dw_rad: D = D0 - w_tan T - w_rad R) into gparams[2..3].
 __global__ void __launch_bounds__(256) k_masked_loss(const ScaleDev* __restrict__ sds, const int2* __restrict__ work,
                                                      double* __restrict__ loss, double* __restrict__ gparams) {
@@ -84,8 +85,8 @@ __global__ void __launch_bounds__(256) k_masked_loss(const ScaleDev* __restrict_
   const int by = item.y / nbx, bx = item.y - by * nbx;
   double acc = 0.0, accT = 0.0, accR = 0.0;
   const int x = bx * kStX + (threadIdx.x & 31);
-  for (int i = threadIdx.x >> 5; i < kStY; i += 8) {
-    const int y = by * kStY + i;
+  for (int i = threadIdx.x >> 5; i < kStencilBlockH; i += 8) {
+    const int y = by * kStencilBlockH + i;
     if (x < W && y < H) {
       const double m = sd->M[(size_t)y * W + x];
       const size_t k = (size_t)y * sd->dPitch + x;
