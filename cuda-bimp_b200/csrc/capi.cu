@@ -508,9 +508,12 @@ struct bimp_context {
   // stream after each call's input copies; null if the capture failed
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  // the output descriptor last copied to the device (skipped when unchanged)
+  // the output descriptor last written on the device (not rewritten when
+  // unchanged, unless the context was ever used in a caller's stream
+  // capture: a replay of that graph rewrites it behind this record)
   KpOut lastOut{};
   bool outSet = false;
+  bool captured = false;
 };
 
 struct bimp_batch {
@@ -672,15 +675,20 @@ static int ctx_run(bimp_context* c, const uint8_t* image, size_t pitch, int widt
   o.ld = ld;
   o.capacity = capacity;
   o.aos = aos;
-  if (!c->outSet || std::memcmp(&o, &c->lastOut, sizeof(o)) != 0) {
-    BIMP_CUDA(cudaMemcpyAsync(e.d_outs, &o, sizeof(o), cudaMemcpyHostToDevice, s));
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BIMP_CUDA(cudaStreamIsCapturing(s, &cap));
+  // the destination descriptor: rewritten when it changes, and always when
+  // the caller's stream is being captured (a replay must not depend on
+  // what later calls leave in the device copy)
+  if (cap != cudaStreamCaptureStatusNone) c->captured = true;
+  if (c->captured || !c->outSet || std::memcmp(&o, &c->lastOut, sizeof(o)) != 0) {
+    launch_set_out(e.d_outs, o, s);
+    BIMP_CUDA(cudaGetLastError());
     c->lastOut = o;
     c->outSet = true;
   }
   // the captured sequence, unless the caller's stream is itself being
   // captured (then the kernels go straight into the caller's capture)
-  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-  BIMP_CUDA(cudaStreamIsCapturing(s, &cap));
   if (c->exec && cap == cudaStreamCaptureStatusNone) {
     BIMP_CUDA(cudaGraphLaunch(c->exec, s));
   } else {

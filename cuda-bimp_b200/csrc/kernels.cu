@@ -898,6 +898,12 @@ cudaError_t configure_kernels() {
   return upload_twiddles();
 }
 
+// The keypoint destination descriptor of a context, written in stream order
+// from a kernel argument (no host memory involved, so the write is also
+// valid inside a stream capture).
+__global__ void k_set_out(KpOut* __restrict__ d, KpOut v) { *d = v; }
+void launch_set_out(KpOut* d, const KpOut& v, cudaStream_t s) { k_set_out<<<1, 1, 0, s>>>(d, v); }
+
 void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s) {
   if (njobs <= 0 || levels <= 0) return;
   const int T = 32 >> (levels - 1);

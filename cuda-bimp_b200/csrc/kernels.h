@@ -46,6 +46,7 @@ size_t stencil_smem_bytes();
 
 // `levels` (1..3) pyrDown steps per job in one launch; maxW/maxH: largest
 // deepest-level size over the jobs
+void launch_set_out(KpOut* d, const KpOut& v, cudaStream_t s);
 void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s);
 // d_fault: word that receives 1 if a bounded device wait expired.
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,

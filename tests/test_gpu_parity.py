@@ -367,3 +367,50 @@ def test_lines_edges_match_oracle(w, h, lam):
         ch = torch.from_numpy(np.ascontiguousarray(Ct[:, :sc.dataH, :sc.dataW].sum(0), dtype=np.float32)).cuda()
         g2 = cs.lines_edges(i, ch=ch)[2].cpu().numpy()
         assert ((g2 != g_typ) & ~near).sum() == 0
+
+
+def test_async_detection_captured_in_a_caller_graph():
+    """bimp_detect_device_async recorded into the caller's own CUDA graph and
+    replayed writes the same keypoints as a direct call, also when direct
+    calls into another keypoint matrix run before and after the replay (the
+    context's keypoint destination is rewritten in stream order)."""
+    import ctypes as C
+
+    import torch
+    from bimp_b200 import _lib as L
+    imgs, lam = synth.workload("vga")
+    cs = api.CudaStuff(640, 480, lam)
+    ref, n_ref = api.getKeypoints(imgs[0], cs, return_count=True)
+    ref = ref.clone()
+    img = torch.from_numpy(imgs[0]).cuda().contiguous()
+    cap = 8192
+    lib = L.lib()
+
+    def call(out, count, stream):
+        L.check(lib.bimp_detect_device_async(cs.handle, C.c_void_p(img.data_ptr()), img.stride(0), 640, 480,
+                                             C.c_void_p(out.data_ptr()), out.stride(0), cap,
+                                             C.c_void_p(count.data_ptr()), C.c_void_p(stream.cuda_stream)),
+                "bimp_detect_device_async")
+
+    kp = torch.zeros((7, cap), dtype=torch.float32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    other = torch.zeros_like(kp)
+    cnt2 = torch.zeros_like(cnt)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g, stream=s):
+        call(kp, cnt, s)
+    call(other, cnt2, torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    assert int(cnt2.item()) == n_ref <= cap
+    assert torch.equal(other[:, :n_ref], ref[:, :n_ref])
+    g.replay()
+    torch.cuda.synchronize()
+    assert int(cnt.item()) == n_ref
+    assert torch.equal(kp[:, :n_ref], ref[:, :n_ref])
+    other.zero_()
+    call(other, cnt2, torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    assert torch.equal(other[:, :n_ref], ref[:, :n_ref])
+    del g
