@@ -497,7 +497,17 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
     }
     return;
   }
-  // consumer warps
+  // consumer warps.  The map max is kept per lane across the blocks of one
+  // scale and goes out as one atomic per warp when the scale changes (not
+  // one per block: consecutive blocks share their scale's max word).
+  unsigned int* runKey = nullptr;
+  float runMax = -INFINITY;
+  auto flush = [&]() {
+    float m = runMax;
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, sh));
+    if (lane == 0 && runKey && m > -INFINITY) atomicMax(runKey, float_key(m));
+  };
   for (int k = 0; k < nk; ++k) {
     const int b = k % kStBufs, u = k / kStBufs;
     if (!mbar_wait(full0 + 8 * b, u & 1)) {
@@ -506,6 +516,11 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
     }
     const StencilBlk& B = blk[b];
     const float* s_c = s_buf + b * kStBuf;
+    if (B.maxKey != runKey) {
+      flush();
+      runKey = B.maxKey;
+      runMax = -INFINITY;
+    }
     float dmax;
     if (B.pattern == 1)
       dmax = stencil_block<1, MODE, kStConsumers>(s_c, B.P, B.x0, B.y0, B.W, B.H, B.gain, B.wT, B.wR, B.out);
@@ -513,13 +528,11 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
       dmax = stencil_block<2, MODE, kStConsumers>(s_c, B.P, B.x0, B.y0, B.W, B.H, B.gain, B.wT, B.wR, B.out);
     else
       dmax = stencil_block<0, MODE, kStConsumers>(s_c, B.P, B.x0, B.y0, B.W, B.H, B.gain, B.wT, B.wR, B.out);
-    // map max: one atomic per warp
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
-    if (lane == 0 && dmax > -INFINITY) atomicMax(B.maxKey, float_key(dmax));
+    runMax = fmaxf(runMax, dmax);
     __syncwarp();
     if (lane == 0) mbar_arrive(empty0 + 8 * b);   // this warp is done with buffer b and blk[b]
   }
+  flush();
 }
 
 // ---------------------------------------------------------------------------
