@@ -355,7 +355,7 @@ constexpr int kStConsumers = 512;                    // 16 compute warps
 constexpr int kStThreads = kStConsumers + 32;        // + the producer warp
 constexpr int kStCtasPerSm = 1;                      // resident CTAs per SM (2 with 16-row blocks: no faster)
 constexpr int kStBuf = kNumOri * kStH * kStW;        // floats per staging buffer
-constexpr int kStBufs = 2;                           // staging ring depth (3 measured no faster)
+constexpr int kStBufs = 3;                           // staging ring depth
 
 // Everything a consumer needs about its block, written by the producer.
 struct StencilBlk {
