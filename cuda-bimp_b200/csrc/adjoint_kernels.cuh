@@ -73,26 +73,32 @@ __device__ __forceinline__ void block_add_double(double v, double* dst) {
   }
 }
 
-// Over one forward stencil block (32 x kStencilBlockH pixels, the forward
-// stencil's block list): sum M * D into loss[0], and -sum M * T, -sum M * R
-// (dL/dw_tan and dL/dw_rad: D = D0 - w_tan T - w_rad R) into gparams[2..3].
+// Over the forward stencil blocks (32 x kStencilBlockH pixels, the forward
+// stencil's block list), a persistent grid: sum M * D into loss[0], and
+// -sum M * T, -sum M * R (dL/dw_tan and dL/dw_rad: D = D0 - w_tan T -
+// w_rad R) into gparams[2..3].  Each CTA accumulates its blocks in registers
+// and adds once per quantity (a per-block atomic on the same three words
+// serialises).
 __global__ void __launch_bounds__(256) k_masked_loss(const ScaleDev* __restrict__ sds, const int2* __restrict__ work,
-                                                     double* __restrict__ loss, double* __restrict__ gparams) {
-  const int2 item = work[blockIdx.x];
-  const ScaleDev* sd = sds + item.x;
-  const int W = sd->dataW, H = sd->dataH;
-  const int nbx = (W + kStX - 1) / kStX;
-  const int by = item.y / nbx, bx = item.y - by * nbx;
+                                                     int nwork, double* __restrict__ loss,
+                                                     double* __restrict__ gparams) {
   double acc = 0.0, accT = 0.0, accR = 0.0;
-  const int x = bx * kStX + (threadIdx.x & 31);
-  for (int i = threadIdx.x >> 5; i < kStencilBlockH; i += 8) {
-    const int y = by * kStencilBlockH + i;
-    if (x < W && y < H) {
-      const double m = sd->M[(size_t)y * W + x];
-      const size_t k = (size_t)y * sd->dPitch + x;
-      acc += m * (double)sd->D[k];
-      accT += m * (double)sd->T[k];
-      accR += m * (double)sd->R[k];
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const int2 item = work[w];
+    const ScaleDev* sd = sds + item.x;
+    const int W = sd->dataW, H = sd->dataH;
+    const int nbx = (W + kStX - 1) / kStX;
+    const int by = item.y / nbx, bx = item.y - by * nbx;
+    const int x = bx * kStX + (threadIdx.x & 31);
+    for (int i = threadIdx.x >> 5; i < kStencilBlockH; i += 8) {
+      const int y = by * kStencilBlockH + i;
+      if (x < W && y < H) {
+        const double m = sd->M[(size_t)y * W + x];
+        const size_t k = (size_t)y * sd->dPitch + x;
+        acc += m * (double)sd->D[k];
+        accT += m * (double)sd->T[k];
+        accR += m * (double)sd->R[k];
+      }
     }
   }
   block_add_double(acc, loss);

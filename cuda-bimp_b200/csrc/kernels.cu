@@ -954,7 +954,7 @@ void launch_pyr_f_adj(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cuda
 }
 void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, double* d_gparams,
                         cudaStream_t s) {
-  if (nwork > 0) k_masked_loss<<<nwork, 256, 0, s>>>(d_sd, d_work, d_loss, d_gparams);
+  if (nwork > 0) k_masked_loss<<<std::min(nwork, 4 * num_sms()), 256, 0, s>>>(d_sd, d_work, nwork, d_loss, d_gparams);
 }
 void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s) {
   if (nwork > 0) k_stencil_bwd<<<nwork, kStBwThreads, 0, s>>>(d_sd, d_work);

@@ -42,6 +42,8 @@ struct KpOut {
 
 cudaError_t configure_kernels();
 size_t gabor_smem_bytes();
+// SM count of the current device (cached per device).
+int num_sms();
 size_t stencil_smem_bytes();
 
 // `levels` (1..3) pyrDown steps per job in one launch; maxW/maxH: largest
