@@ -139,8 +139,10 @@ int bimp_detect_device_async(bimp_context* ctx, const uint8_t* d_image, size_t p
 /* Context(cv::Mat&) + Context::getKeypointsAndDownload(),
  * bimp/include/detection/bimp.hpp:35,38, bimp/src/bimp.cpp:7-20,89-92,
  * for an already-grey image: host uint8 image in, host cv::KeyPoint-layout
- * records out (utils.cpp:130-150 downloadKeypoints).  Copies go through the
- * context's pinned staging buffers on `stream`; the call synchronises. */
+ * records out (utils.cpp:130-150 downloadKeypoints).  The records are
+ * written on the device in this layout and copied once into `out` after the
+ * count is known (pinned memory keeps the copies asynchronous); the call
+ * synchronises `stream`. */
 int bimp_detect_host(bimp_context* ctx, const uint8_t* image, size_t pitch,
                      int width, int height, bimp_keypoint* out, int capacity,
                      int* n_found, void* stream);

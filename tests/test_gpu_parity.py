@@ -152,6 +152,24 @@ def test_detect_host_matches_device():
     assert np.array_equal(dev, host)
 
 
+def test_detect_host_sequence_of_counts():
+    """One context, host path, images whose keypoint counts rise and fall
+    (including none): every call equals the device path."""
+    imgs, lam = synth.workload("vga")
+    base = imgs[0]
+    half = base.copy()
+    half[:, : base.shape[1] // 2] = 128   # about half the keypoints
+    seq = [base, np.full_like(base, 128), base[:, ::-1].copy(), base[::-1].copy(), half, base, np.full_like(base, 7),
+           base]
+    cs = api.CudaStuff(base.shape[1], base.shape[0], lam)
+    for img in seq:
+        kp, n = api.getKeypoints(img, cs, capacity=100000, return_count=True)
+        dev = api.keypoint_matrix_to_records(kp)
+        host, n2, rc = api.detect_host(cs, img, capacity=100000)
+        assert rc == 0 and n2 == n
+        assert np.array_equal(dev, host)
+
+
 def test_repeatable_bitwise():
     imgs, lam = synth.workload("vga")
     img = imgs[0]
