@@ -344,23 +344,41 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
         const float4* __restrict__ cA = sd->bwA + (size_t)o * kSpecHalf;
         const float2* __restrict__ cB = sd->bwB + (size_t)o * kSpecHalf;
         float sa = 0.f, sr = 0.f;
-        for (int j = t; j < kSpecHalf; j += kTileThreads) {
+        // entry (py, sl) of the half layout, j = py * kXhCols + sl
+        auto entry = [&](int py, int sl, int p, int np, int wp) {
+          const int j = py * kXhCols + sl;
           const float4 c4 = __ldg(cA + j);   // G(k), G(-k), dGa(k), dGr(k)
           const float2 c2 = __ldg(cB + j);   // dGa(-k), dGr(-k)
           const float2 X = __ldg(Xs + j);
-          const int py = j / kXhCols, sl = j - py * kXhCols;
-          const int kx = sl < 64 ? (sl >> 2) + 16 * (sl & 3) : 64;
           const int ky = 16 * (py & 7) + (py >> 3);
-          const int p = perm128d(kx);
-          const int np = perm128d((kTile - kx) & 127), npy = perm128d((kTile - ky) & 127);
-          const float2 A1 = W[widx(py, p)], A2 = W[widx(npy, np)];
-          const float2 b = Bh[j];
-          Bh[j] = make_float2(fmaf(0.5f * c4.x, A1.x, fmaf(0.5f * c4.y, A2.x, b.x)),
-                              fmaf(0.5f * c4.x, A1.y, fmaf(-0.5f * c4.y, A2.y, b.y)));
+          const int npy = perm128d((kTile - ky) & 127);
+          const float2 A1 = W[wp], A2 = W[widx(npy, np)];
+          const float2 bb = Bh[j];
+          Bh[j] = make_float2(fmaf(0.5f * c4.x, A1.x, fmaf(0.5f * c4.y, A2.x, bb.x)),
+                              fmaf(0.5f * c4.x, A1.y, fmaf(-0.5f * c4.y, A2.y, bb.y)));
           const float re1 = A1.x * X.x + A1.y * X.y;   // Re(conj(A(k)) X(k))
           const float re2 = A2.x * X.x - A2.y * X.y;   // Re(conj(A(-k)) conj(X(k)))
           sa = fmaf(c4.z, re1, fmaf(c2.x, re2, sa));
           sr = fmaf(c4.w, re1, fmaf(c2.y, re2, sr));
+        };
+        // slots 0..63: thread t owns slot sl = t mod 64 and the rows
+        // py = t / 64 + 8 r (r = 0..15), so its column terms are fixed and
+        // widx(py, p) = 128 py + (phys(p) ^ 8 (py & 1)) with py & 1 fixed
+        {
+          const int sl = t & 63, pr = t >> 6;
+          const int kx = (sl >> 2) + 16 * (sl & 3);
+          const int p = perm128d(kx), np = perm128d((kTile - kx) & 127);
+          const int pp = phys(p) ^ ((pr & 1) << 3);
+#pragma unroll 4
+          for (int r = 0; r < 16; ++r) {
+            const int py = pr + 8 * r;
+            entry(py, sl, p, np, py * kTile + pp);
+          }
+        }
+        // the Nyquist slot 64 (kx = 64): one row per thread of the first 128
+        if (t < kTile) {
+          const int p = perm128d(64);
+          entry(t, 64, p, p, widx(t, p));
         }
         accA += sa;
         accR += sr;
