@@ -377,6 +377,14 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     const bool wrapTile = sd->wrapW != 0 && (C0 == 0 || C0 + V >= cCols);
     // window positions x in [kX, xHi) are this tile's valid outputs
     const int xHi = min(kX + V, cCols - C0 + kX);
+    // I4's thread keeps column group n1 = t mod 8 for the whole tile: bit n2
+    // of xMask says whether its output x = n1 + 8 n2 is in [kX, xHi)
+    unsigned int xMask = 0;
+#pragma unroll
+    for (int n2 = 0; n2 < 16; ++n2) {
+      const int x = (t & 7) + 8 * n2;
+      xMask |= (x >= kX && x < xHi ? 1u : 0u) << n2;
+    }
     float* __restrict__ C0p = sd->C;
     float2* __restrict__ Z0p = sd->Z;
     const long long cStride = sd->cStride;
@@ -453,7 +461,7 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
 #pragma unroll
             for (int n2 = 0; n2 < 16; ++n2) {
               const int x = n1 + 8 * n2;
-              if (x >= kX && x < xHi) {
+              if ((xMask >> n2) & 1u) {
                 dstx[x] = cmag(v[n2]);
                 if constexpr (SAVE_Z) Z0p[(size_t)o * cStride + (size_t)gy * cPitch + (C0 - kX) + x] = v[n2];
               }
