@@ -122,13 +122,14 @@ __device__ __forceinline__ void tmem_load8(uint32_t taddr, float2 (&v)[8]) {
   for (int i = 0; i < 8; ++i) v[i] = make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1]));
 }
 
-// |z| as s * rsqrt(s), s = |z|^2 (hardware reciprocal square root, relative
-// error a few 1e-7); exactly 0 for z = 0.
+// |z| as s * rsqrt(max(s, 1e-30)), s = |z|^2 (hardware reciprocal square
+// root, relative error a few 1e-7): exactly 0 for z = 0, and below 1e-15
+// (where the max applies) the value stays below |z|.
 __device__ __forceinline__ float cmag(float2 z) {
   const float s = fmaf(z.x, z.x, z.y * z.y);
   float r;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(s));
-  return s > 0.f ? s * r : 0.f;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(fmaxf(s, 1e-30f)));
+  return s * r;
 }
 
 // Float levels hold X (a float image, X = u8/255 for the uint8 content);
