@@ -401,6 +401,7 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         tmem_load8(tlane + 16 * k2, v);
         if (!mbar_wait(bar0 + 8 * slot, (ph >> slot) & 1)) fault = true;
         ph ^= 1u << slot;
+        __syncwarp();   // the warp-collective TMEM stores below need a converged warp
         const float* Gq = Gbuf + slot * kGChunkFloats + 8 * h * kTile + pI1;
 #pragma unroll
         for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], Gq[k1 * kTile]);
