@@ -123,6 +123,8 @@ _PROTOS = [
     ("bimp_batch_counts", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("bimp_batch_keypoints_device", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
                                               C.POINTER(C.c_size_t)]),
+    ("bimp_batch_scale_info", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(ScaleInfo)]),
+    ("bimp_batch_dense_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("bimp_batch_detect_host", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
                                          C.POINTER(C.POINTER(KeyPointC)), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int), C.c_void_p]),

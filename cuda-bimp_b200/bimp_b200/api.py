@@ -397,6 +397,22 @@ class Batch:
                                           _stream_ptr(stream)), "batch_counts")
         return self._counts
 
+    def scale_info(self, i: int, scale: int) -> dict:
+        """Geometry of image i at one scale (bimp_batch_scale_info)."""
+        si = L.ScaleInfo()
+        L.check(L.lib().bimp_batch_scale_info(self._h, int(i), int(scale), C.byref(si)), "batch_scale_info")
+        return {f: getattr(si, f) for f, _ in L.ScaleInfo._fields_}
+
+    def dense_map(self, i: int, scale: int):
+        """Summed keypoint map D of image i, scale `scale` from the last run
+        (bimp_batch_dense_map)."""
+        torch = _torch()
+        k = self.scale_info(i, scale)
+        out = torch.empty((k["data_h"], k["data_w"]), dtype=torch.float32, device="cuda")
+        L.check(L.lib().bimp_batch_dense_map(self._h, int(i), int(scale), C.c_void_p(out.data_ptr()),
+                                             out.stride(0), _stream_ptr()), "batch_dense_map")
+        return out
+
     def keypoints(self, i: int):
         torch = _torch()
         ptr = C.c_void_p()

@@ -1017,6 +1017,34 @@ int bimp_batch_counts(bimp_batch* b, int* d_counts, void* stream) {
   return BIMP_OK;
 }
 
+int bimp_batch_scale_info(const bimp_batch* b, int i, int scale, bimp_scale_info* out) {
+  if (!b || !out || i < 0 || i >= b->eng.nImages || scale < 0 || scale >= b->eng.nScales)
+    return fail(BIMP_ERR_INVALID, "bad batch scale index");
+  const ScaleHost& h = b->eng.geo[i][scale];
+  out->lambda_full = h.lambda2;
+  out->lambda_level = h.lambda;
+  out->pyrstep = h.pyrstep;
+  out->kernel_w = h.kW;
+  out->kernel_x = h.kX;
+  out->data_w = h.dataW;
+  out->data_h = h.dataH;
+  out->fft_w = h.fftW;
+  out->fft_h = h.fftH;
+  out->margin = h.off;
+  return BIMP_OK;
+}
+
+int bimp_batch_dense_map(bimp_batch* b, int i, int scale, float* d_out, size_t ld, void* stream) {
+  if (!b || !d_out || i < 0 || i >= b->eng.nImages || scale < 0 || scale >= b->eng.nScales)
+    return fail(BIMP_ERR_INVALID, "bad batch dense-map arguments");
+  const ScaleDev& d = b->eng.h_sd[(size_t)i * b->eng.nScales + scale];
+  if (ld < (size_t)d.dataW) return fail(BIMP_ERR_INVALID, "ld smaller than data width");
+  BIMP_CUDA(cudaSetDevice(b->eng.device));
+  BIMP_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), d.D, d.dPitch * sizeof(float), d.dataW * sizeof(float),
+                              d.dataH, cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)));
+  return BIMP_OK;
+}
+
 int bimp_batch_keypoints_device(bimp_batch* b, int i, const float** d_kp, size_t* ld) {
   if (!b || i < 0 || i >= b->eng.nImages || !d_kp || !ld)
     return fail(BIMP_ERR_INVALID, "bad batch keypoint arguments");

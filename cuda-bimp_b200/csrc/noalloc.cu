@@ -1,14 +1,14 @@
 // Keypoint extraction from one summed keypoint map with no memory allocation.
 //
-// Callers that cannot allocate device memory while they run -- code that is
-// being captured into a CUDA graph, real-time loops that must not hit the
-// allocator, or hosts whose device memory is owned by a pool the library may
-// not touch -- still need the threshold / non-maximum-suppression /
-// compaction step.  This entry point runs it with all of its scratch (the
-// scale descriptor, the per-row candidate counts and offsets, the maximum of
-// the map) in one file-scope device array of fixed size, and calls no
-// cudaMalloc, cudaFree or allocating library routine.  The caller passes the
-// map and the keypoint destination.
+// Some callers cannot allocate device memory while they run: real-time loops
+// that must never enter the allocator (an allocation can block on a device
+// synchronisation), or hosts whose device memory all belongs to a pool that
+// the library may not touch.  They still need the threshold /
+// non-maximum-suppression / compaction step.  This entry point runs it with
+// all of its scratch (the scale descriptor, the per-row candidate counts and
+// offsets, the maximum of the map) in one file-scope device array of fixed
+// size, and calls no cudaMalloc, cudaFree or allocating library routine.  The
+// caller passes the map and the keypoint destination.
 //
 // The array is shared by every call on a device and keeps the previous call's
 // contents; each call first clears what has to start at zero.  Two calls
@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -97,6 +98,8 @@ extern "C" int bimp_extract_keypoints_noalloc(const float* d_map, size_t ld, int
   if (!d_map || !d_count || width < 3 || height < 3 || ld < (size_t)width || capacity < 0 ||
       (capacity > 0 && (!d_kp || kp_ld < (size_t)capacity)) || !(lambda_level > 0.f) || !(pyrstep > 0.f))
     return na_fail(BIMP_ERR_INVALID, "bad arguments");
+  // the kernels take the map's row pitch as an int
+  if (ld > (size_t)INT_MAX) return na_fail(BIMP_ERR_INVALID, "map row pitch above INT_MAX floats");
   const int off = static_cast<int>(lambda_level);
   const int yEnd = std::min(height - off - 1, height - 2);
   const int nrows = std::max(0, yEnd - off);

@@ -205,16 +205,22 @@ int bimp_color_features(const float* d_kp, size_t kp_ld, int n, const uint8_t* d
 /* ---- keypoint extraction without allocation ------------------------------
  * No counterpart in the reference (its extraction, cuda_gpu_keypoints,
  * allocates GpuMats and thrust/NPP temporaries on every call).  For callers
- * that must not allocate device memory while they run: work being captured
- * into a CUDA graph, real-time loops kept away from the allocator, or hosts
- * whose device memory belongs to a pool the library may not touch.
+ * that cannot allocate device memory while they run: real-time loops that
+ * must never enter the allocator (an allocation can block on a device
+ * synchronisation), or hosts whose device memory all belongs to a pool the
+ * library may not touch.
  *
  * Threshold (thresh_ratio * max of the map), strict 8-neighbour maxima,
  * margin (int)lambda_level and parabolic subpixel refinement on one summed
- * keypoint map `d_map` (height x width floats, row pitch `ld` floats), records
- * written to the 7 x kp_ld device matrix `d_kp` in (y, x) order, the total to
- * the device int `d_count`.  Identical results to the extraction step of
+ * keypoint map `d_map` (height x width floats, row pitch `ld` floats, at
+ * most INT_MAX), records written to the 7 x kp_ld device matrix `d_kp` in
+ * (y, x) order.  Identical results to the extraction step of
  * bimp_detect_device for the same map.
+ *
+ * `*d_count` (device int, stream-ordered) receives the TRUE total, which can
+ * exceed `capacity`: only the first min(total, capacity) records, in (y, x)
+ * order, are written.  The count is known only on the device, so this call
+ * cannot return BIMP_ERR_CAPACITY: compare *d_count with `capacity` yourself.
  *
  * All scratch lives in one fixed device array of about 260 KB per device
  * (held until the process exits); maps with more than 16384 candidate rows

@@ -74,6 +74,16 @@ int bimp_batch_counts(bimp_batch* batch, int* d_counts, void* stream);
  * first min(count, ld) columns are written. */
 int bimp_batch_keypoints_device(bimp_batch* batch, int i, const float** d_kp, size_t* ld);
 
+/* Geometry of image i at one scale (as bimp_ctx_scale_info for a context of
+ * that image's size). */
+int bimp_batch_scale_info(const bimp_batch* batch, int i, int scale, bimp_scale_info* out);
+
+/* Summed keypoint map D of image i, scale `scale` from the last run
+ * (Context::getResponses, bimp/src/bimp.cpp:94-104, for one image of the
+ * batch): data_h x data_w floats to device memory `d_out` (row pitch `ld`
+ * floats) on `stream`. */
+int bimp_batch_dense_map(bimp_batch* batch, int i, int scale, float* d_out, size_t ld, void* stream);
+
 /* Host images in, host keypoints out: uploads every image, replays the
  * graph, downloads totals and records.  n_found[i] receives each image's
  * total; returns BIMP_ERR_CAPACITY if any exceeded its capacity. */

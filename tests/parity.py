@@ -106,3 +106,48 @@ def compare_keypoints(rec: np.ndarray, oracle_result, tie_eps: float = TIE_EPS) 
                 continue
             report["extra"].append((s, key))
     return report
+
+
+def decision_margin(D, thresh_ratio: float = 0.104) -> np.ndarray:
+    """Per-pixel distance of the keypoint decision (strict 8-neighbour
+    maximum, and above thresh_ratio * max) from flipping, from a summed
+    keypoint map."""
+    H, W = D.shape
+    P = np.pad(D, 1, mode="reflect")
+    dil = np.full(D.shape, -np.inf)
+    for dy in (-1, 0, 1):
+        for dx in (-1, 0, 1):
+            if dy or dx:
+                dil = np.maximum(dil, P[1 + dy:1 + dy + H, 1 + dx:1 + dx + W])
+    loc = D - dil
+    dth = D - np.float32(np.float64(D.max()) * thresh_ratio)
+    return np.minimum(np.abs(loc), np.abs(dth))
+
+
+def check_against_c_restatement(cb, ref: np.ndarray, lambdas, rec: np.ndarray, dense_maps,
+                                tie_frac: float = 1e-4) -> dict:
+    """Records `rec` and per-scale summed keypoint maps of one image against
+    the FP32 C restatement `cb` (oracle.cbimp.CBimp) and its records `ref`
+    from cb.detect on the same image: maps within MAP_TOL of the peak;
+    keypoint (scale, x, y) sets equal except where the restatement's decision
+    is within tie_frac of the map peak of a tie (at most max(2, n/1000) such
+    pixels per scale).  Returns the worst map error and the symmetric
+    difference per scale."""
+    out = {"map_err": 0.0, "symdiff": [], "keypoints": 0}
+    lam = sorted(float(np.float32(x)) for x in lambdas)
+    for s, info in enumerate(cb.scales):
+        D = cb.dense_map(s)
+        out["map_err"] = max(out["map_err"], peak_rel_error(dense_maps[s], D))
+        pyr = 2 ** info["level"]
+        size = np.float32(np.float32(np.float32(lam[s]) / np.float32(pyr)) * np.float32(pyr))
+        a = {(int(np.rint(k["x"] / pyr)), int(np.rint(k["y"] / pyr))) for k in ref[ref["size"] == size]}
+        b = {(int(np.rint(k["x"] / pyr)), int(np.rint(k["y"] / pyr))) for k in rec[rec["size"] == size]}
+        marg = decision_margin(D)
+        peak = np.abs(D).max()
+        for (x, y) in a ^ b:
+            assert marg[y, x] < tie_frac * peak, (s, x, y, marg[y, x] / peak)
+        assert len(a ^ b) <= max(2, len(a) // 1000), (s, len(a ^ b), len(a))
+        out["symdiff"].append(len(a ^ b))
+        out["keypoints"] += len(a)
+    assert out["map_err"] <= MAP_TOL, out["map_err"]
+    return out

@@ -104,3 +104,21 @@ def test_adjoint_is_repeatable():
     assert (g1 - g2).abs().max().item() <= 1e-5 * scale and (g1 - g3).abs().max().item() <= 1e-5 * scale
     assert torch.allclose(p1, p2, rtol=1e-6) and torch.allclose(p1, p3, rtol=1e-6)
     adj.close()
+
+
+def test_adjoint_all_16_workload_images():
+    """All 16 images of the 512x512 adjoint workload, 6 scales: branch-matched
+    error (the 1e-3 bar) and, for the record, the error against the FP64
+    reference's own branch."""
+    imgs, lam = synth.workload("adjoint")
+    err = _check(*_run(512, 512, 16, lam, seed=37, imgs=np.stack(imgs)))
+    print(f"16 images: branch-matched {err:.3e}")
+
+
+def test_adjoint_uhd_crop_with_12_scales():
+    """A 1024x1024 crop of a 3840x2160 frame (uint8 / 255) with the 12-scale
+    bank: six pyramid levels down to 32x32, where the coarse scales' kernels
+    are wider than their torus (the taps wrap and add)."""
+    frame = synth.uhd_frames(1, 1004)[0]
+    crop = np.ascontiguousarray(frame[568:1592, 1408:2432]).astype(np.float32) / np.float32(255.0)
+    _check(*_run(1024, 1024, 1, synth.bank(12), seed=43, imgs=crop[None]))

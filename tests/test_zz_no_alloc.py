@@ -1,9 +1,10 @@
 """The allocation-free keypoint extraction entry point.
 
 bimp_extract_keypoints_noalloc serves callers that cannot allocate device
-memory while they run (work captured into a CUDA graph, real-time loops kept
-away from the allocator, device memory owned by an external pool): its
-scratch lives in a fixed file-scope device array.  Its records must equal the
+memory while they run (real-time loops that must never enter the allocator,
+whose calls can block on a device synchronisation, or hosts whose device
+memory all belongs to an external pool): its scratch lives in a fixed
+file-scope device array.  Its records must equal the
 extraction step of the existing bimp_detect_device entry point on the same
 summed keypoint map, on consecutive calls that reuse the shared scratch.
 
