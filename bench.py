@@ -194,6 +194,14 @@ def profiled_traffic():
     return float(m.group(1)) if m else None
 
 
+def headline_config(lam, world: int) -> dict:
+    """The workload both arms report (the same dict in both lines)."""
+    return {"workload": "plain BIMP, one 1920x1080 uint8 image per step (1/f^2 noise + 150 polygons)",
+            "scales": 8, "orientations": 8, "lambdas": [round(x, 6) for x in lam],
+            "input_pool": f"{POOL} distinct 1080p images (133 MB > L2), rotated per step",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
     import torch.distributed as dist
@@ -268,7 +276,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     achieved = alg["gabor"] / (stage_ms["gabor"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": "k_gabor_tiles", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "traffic": profiled_traffic(), "algorithmic_bytes": alg["gabor"],
+                "traffic": profiled_traffic(), "traffic_source": "profiles/gabor_tiles_hd.md (one ncu capture "
+                "of this launch; not measured in this run)", "algorithmic_bytes": alg["gabor"],
                 "avg_launch_ms": round(stage_ms["gabor"], 4)}
     for name in ("stencil", "nms"):
         a_gbs = alg[name] / (stage_ms[name] * 1e-3) / 1e9
@@ -282,37 +291,70 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                 "frac_of_nominal": round(fl / (stage_ms["gabor"] * 1e-3) / 74.4e12, 3)}
 
     # -- end to end through the host-buffer C ABI ---------------------------
+    # Pinned host frames in, host cv::KeyPoint records out, every copy inside
+    # the timed region.  Headline: the pipelined entry point (frames in
+    # flight, bimp_pipeline_push/pop); beside it the one-frame-per-call
+    # bimp_detect_host.  Timed by the host clock from the first push to the
+    # last pop (which returns only after that frame's copies are done).
     e2e = None
     if not args.no_e2e:
         pinned = [torch.from_numpy(im).pin_memory() for im in pool_np[:8]]
+        arrs = [t.numpy() for t in pinned]
         outs = (L.KeyPointC * cap)()
         n = C.c_int()
         d2h = []
+        depth = 3
+        pl = api.Pipeline(W_HD, H_HD, lam, depth=depth, capacity=cap)
 
-        def detect_host(img):
-            a = img.numpy()
+        def pop():
+            rc = lib.bimp_pipeline_pop(pl._h, outs, cap, C.byref(n))
+            if rc not in (0, L.BIMP_ERR_CAPACITY):
+                L.check(rc, "bimp_pipeline_pop")
+            d2h.append(8 + 28 * min(n.value, cap))
+
+        def push(a):
+            L.check(lib.bimp_pipeline_push(pl._h, C.c_void_p(a.ctypes.data), a.strides[0], W_HD, H_HD),
+                    "bimp_pipeline_push")
+
+        def stream_frames(k):
+            for i in range(k):
+                if lib.bimp_pipeline_in_flight(pl._h) == depth:
+                    pop()
+                push(arrs[i % 8])
+            while lib.bimp_pipeline_in_flight(pl._h):
+                pop()
+
+        stream_frames(max(3, args.warmup))
+        d2h.clear()
+        k_e2e = max(10, min(args.steps, 1000))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        stream_frames(k_e2e)
+        ms_e2e = max_ms((time.perf_counter() - t0) * 1e3)
+        pl.close()
+        e2e = {"value": round(world * k_e2e * W_HD * H_HD / (ms_e2e * 1e-3) / 1e6, 2), "unit": UNIT,
+               "h2d_bytes_per_step": W_HD * H_HD, "d2h_bytes_per_step": int(np.mean(d2h)),
+               "steps": k_e2e, "api": f"bimp_pipeline_push / bimp_pipeline_pop, {depth} frames in flight",
+               "host_memory": "pinned frames in, caller's records array out"}
+
+        def detect_host(a):
             rc = lib.bimp_detect_host(cs.handle, C.c_void_p(a.ctypes.data), a.strides[0], W_HD, H_HD, outs, cap,
                                       C.byref(n), sp)
             if rc not in (0, L.BIMP_ERR_CAPACITY):
                 L.check(rc, "bimp_detect_host")
-            d2h.append(4 + 28 * min(n.value, cap))
 
-        for i in range(max(3, args.warmup)):
-            detect_host(pinned[i % 8])
-        d2h.clear()
-        k_e2e = max(10, min(args.steps, 500))
+        for i in range(3):
+            detect_host(arrs[i % 8])
         barrier()
         torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
+        t0 = time.perf_counter()
         for i in range(k_e2e):
-            detect_host(pinned[i % 8])
-        b.record(stream)
-        torch.cuda.synchronize()
-        ms_e2e = max_ms(a.elapsed_time(b))
-        e2e = {"value": round(world * k_e2e * W_HD * H_HD / (ms_e2e * 1e-3) / 1e6, 2), "unit": UNIT,
-               "h2d_bytes_per_step": W_HD * H_HD, "d2h_bytes_per_step": int(np.mean(d2h)),
-               "steps": k_e2e, "api": "bimp_detect_host"}
+            detect_host(arrs[i % 8])
+        ms_sync = max_ms((time.perf_counter() - t0) * 1e3)
+        e2e["per_call_api"] = {"api": "bimp_detect_host (one frame per call, synchronous)",
+                               "value": round(world * k_e2e * W_HD * H_HD / (ms_sync * 1e-3) / 1e6, 2),
+                               "ms_per_frame": round(ms_sync / k_e2e, 4)}
 
     # -- batched mixed sizes vs the same images one by one -----------------
     batched = None
@@ -383,11 +425,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "plain BIMP, one 1920x1080 uint8 image per step (1/f^2 noise + 150 polygons)",
-                       "scales": 8, "orientations": 8, "lambdas": [round(x, 6) for x in lam],
-                       "input_pool": f"{POOL} distinct 1080p images resident in HBM (133 MB > L2), "
-                                     "rotated per step; each step also streams ~200 MB of maps",
-                       "keypoints_last_step": n_kp, "parallelism": f"replicas x{world}"},
+            "config": headline_config(lam, world), "keypoints_last_step": n_kp,
             "roofline": roofline, "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
             "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "adjoint": adjoint,
             "gpu_launches": cs_launches(cs) * args.steps, "clocks": clk,
@@ -598,34 +636,34 @@ def cpu_port_baseline(images_np, lam, images: int, warmup: int = 1) -> dict:
 def run_reference(args, rank: int, world: int):
     """The reference's pipeline on the host cores: the reference itself needs
     OpenCV-CUDA 3.x, Boost, CUDA-samples headers and texture references
-    (removed in CUDA 12), so its FP32 C restatement stands in for it."""
+    (removed in CUDA 12), so its FP32 C restatement stands in for it.  Same
+    64-image pool, bank and config as the GPU arm; each step is one whole
+    1080p image, at most 30 steps so that the run stays within minutes."""
     if rank != 0:
         return
     from bimp_b200 import synth
     from oracle.cbimp import CBimp, max_threads
     lam = synth.bank(8)
-    pool_np = hd_pool(0, 8)
+    pool_np = hd_pool(0)
     with CBimp(W_HD, H_HD, lam) as cb:
         for i in range(args.warmup):
-            cb.detect(pool_np[i % 8])
+            cb.detect(pool_np[i % POOL])
         t0 = time.perf_counter()
         n_kp = 0
         for i in range(args.steps):
-            n_kp = cb.detect(pool_np[i % 8])[1]
+            n_kp = cb.detect(pool_np[i % POOL])[1]
         dt = time.perf_counter() - t0
     value = args.steps * W_HD * H_HD / dt / 1e6
     cores = max_threads()
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "plain BIMP, one 1920x1080 uint8 image per step (1/f^2 noise + 150 polygons)",
-                       "scales": 8, "orientations": 8, "lambdas": [round(x, 6) for x in lam],
-                       "keypoints_last_step": n_kp},
+            "config": headline_config(lam, world), "keypoints_last_step": n_kp,
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} whole 1080p images after {args.warmup} warm-up; FP32 C "
-                                       "restatement of the reference pipeline, OpenMP over all host threads "
-                                       "(the reference needs OpenCV-CUDA 3.x and CUDA<=11 texture references "
-                                       "and cannot be built here)"},
+                             "sample": f"{args.steps} whole 1080p images of the {POOL}-image pool after "
+                                       f"{args.warmup} warm-up; FP32 C restatement of the reference pipeline, "
+                                       "OpenMP over all host threads (the reference needs OpenCV-CUDA 3.x and "
+                                       "CUDA<=11 texture references and cannot be built here)"},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -662,10 +700,9 @@ def main():
         print(json.dumps({"adjoint": out}), flush=True)
         return
     if args.impl == "reference":
-        # each step is a whole 1080p image on the CPU (~1 s): keep the run
+        # each step is a whole 1080p image on the CPU (~0.3 s): keep the run
         # within a few minutes
         args.steps = min(args.steps, 30)
-        args.warmup = min(args.warmup, 3)
         run_reference(args, rank, world)
         return
     if world > 1:

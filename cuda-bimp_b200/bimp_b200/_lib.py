@@ -73,6 +73,12 @@ _PROTOS = [
     ("bimp_ctx_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.POINTER(C.c_float), C.c_int,
                                   C.POINTER(Params)]),
     ("bimp_ctx_destroy", C.c_int, [C.c_void_p]),
+    ("bimp_ctx_create_for_input", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.POINTER(C.c_float), C.c_int, C.POINTER(Params)]),
+    ("bimp_device_alloc", C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
+    ("bimp_device_free", C.c_int, [C.c_void_p]),
+    ("bimp_copy_2d", C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t,
+                               C.c_void_p]),
     ("bimp_ctx_num_scales", C.c_int, [C.c_void_p]),
     ("bimp_ctx_scale_info", C.c_int, [C.c_void_p, C.c_int, C.POINTER(ScaleInfo)]),
     ("bimp_detect_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p,
@@ -81,6 +87,12 @@ _PROTOS = [
                                            C.c_void_p, C.c_size_t, C.c_int, C.c_void_p, C.c_void_p]),
     ("bimp_detect_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int,
                                    C.POINTER(KeyPointC), C.c_int, C.POINTER(C.c_int), C.c_void_p]),
+    ("bimp_pipeline_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.POINTER(C.c_float), C.c_int,
+                                       C.POINTER(Params), C.c_int, C.c_int]),
+    ("bimp_pipeline_destroy", C.c_int, [C.c_void_p]),
+    ("bimp_pipeline_push", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int]),
+    ("bimp_pipeline_pop", C.c_int, [C.c_void_p, C.POINTER(KeyPointC), C.c_int, C.POINTER(C.c_int)]),
+    ("bimp_pipeline_in_flight", C.c_int, [C.c_void_p]),
     ("bimp_dense_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("bimp_complex_map", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("bimp_detect_lines_edges", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,

@@ -96,14 +96,20 @@ def _params(params) -> L.Params | None:
 class CudaStuff:
     """bimp::cuda::CudaStuff: filter bank + buffers for one image size."""
 
-    def __init__(self, width: int, height: int, lambdas, params=None):
+    def __init__(self, width: int, height: int, lambdas, params=None, input_size=None):
+        """input_size (default (width, height)): the size of the images a
+        detection takes; a larger input is filtered on the top-left window of
+        each pyramid level (bimp_ctx_create_for_input), as the reference's
+        Context does for upscaled small images."""
         lam = (C.c_float * len(lambdas))(*[float(x) for x in lambdas])
         h = C.c_void_p()
         p = _params(params)
-        L.check(L.lib().bimp_ctx_create(C.byref(h), int(width), int(height), lam, len(lambdas),
-                                        C.byref(p) if p is not None else None), "CudaStuff")
+        iw, ih = (int(width), int(height)) if input_size is None else (int(input_size[0]), int(input_size[1]))
+        L.check(L.lib().bimp_ctx_create_for_input(C.byref(h), int(width), int(height), iw, ih, lam, len(lambdas),
+                                                  C.byref(p) if p is not None else None), "CudaStuff")
         self._h = h
         self.width, self.height = int(width), int(height)
+        self.input_width, self.input_height = iw, ih
         self.ks = [self.scale_info(i) for i in range(L.lib().bimp_ctx_num_scales(h))]
 
     @property
@@ -219,6 +225,11 @@ def uploadKeypoints(points) -> "object":
     return kp[:, :n]
 
 
+# cv::KeyPoint field order of the host records (bimp_keypoint)
+_HOST_RECORD = np.dtype([("x", "<f4"), ("y", "<f4"), ("size", "<f4"), ("angle", "<f4"), ("response", "<f4"),
+                         ("octave", "<i4"), ("class_id", "<i4")])
+
+
 def detect_host(cs: CudaStuff, image: np.ndarray, capacity: int = KP_MAX_POINTS):
     """Host image in, host records out through bimp_detect_host.
 
@@ -231,11 +242,31 @@ def detect_host(cs: CudaStuff, image: np.ndarray, capacity: int = KP_MAX_POINTS)
     if rc not in (L.BIMP_OK, L.BIMP_ERR_CAPACITY):
         L.check(rc, "detect_host")
     m = min(n.value, capacity)
-    rec = np.frombuffer(out, dtype=np.dtype([("x", "<f4"), ("y", "<f4"), ("size", "<f4"),
-                                             ("angle", "<f4"), ("response", "<f4"),
-                                             ("octave", "<i4"), ("class_id", "<i4")]),
-                        count=m).copy()
+    rec = np.frombuffer(out, dtype=_HOST_RECORD, count=m).copy()
     return rec, n.value, rc
+
+
+def min_size_dims(width: int, height: int) -> tuple:
+    """getGPUImage's size rule (bimp_min_size_dims): (out_w, out_h)."""
+    ow, oh = C.c_int(), C.c_int()
+    L.check(L.lib().bimp_min_size_dims(int(width), int(height), C.byref(ow), C.byref(oh), None), "min_size_dims")
+    return ow.value, oh.value
+
+
+def gpu_image_device(image: np.ndarray, grayscale: bool = True):
+    """getGPUImage (cuda_bimp.cu:156-180) keeping the result on the device:
+    uint8 CUDA tensor (h, w) for grey output, (h, w * 3) for BGR."""
+    torch = _torch()
+    img = np.ascontiguousarray(image, dtype=np.uint8)
+    h, w = img.shape[:2]
+    cn = 1 if img.ndim == 2 else img.shape[2]
+    ow, oh = min_size_dims(w, h)
+    ocn = 1 if (grayscale or cn == 1) else cn
+    src = torch.from_numpy(img.reshape(h, w * cn)).cuda()
+    dst = torch.empty((oh, ow * ocn), dtype=torch.uint8, device="cuda")
+    L.check(L.lib().bimp_gpu_image(C.c_void_p(src.data_ptr()), src.stride(0), w, h, cn, int(bool(grayscale)),
+                                   C.c_void_p(dst.data_ptr()), dst.stride(0), _stream_ptr()), "gpu_image")
+    return dst
 
 
 def gpu_image(image: np.ndarray, grayscale: bool = True) -> np.ndarray:
@@ -287,20 +318,26 @@ def keypoint_matrix_to_records(kp) -> np.ndarray:
 
 
 class Context:
-    """bimp::Context (bimp.hpp:19-51, bimp.cpp:7-129) for grey uint8 images.
+    """bimp::Context (bimp.hpp:19-51, bimp.cpp:7-129) for grey or BGR uint8
+    images.
 
-    The bank is makeLambdasLog(4, 64, 2) as in bimp.cpp:8.
+    As in the reference: the bank is makeLambdasLog(4, 64, 2) (bimp.cpp:8);
+    the image goes through getGPUImage (grey; upscaled when a side is below
+    350 pixels; the colour image is kept for the colour histogram);
+    CudaStuff is built from the image's own size (bimp.cpp:7-8), so an
+    upscaled image is filtered on the top-left window of each pyramid level;
+    width()/height() are the uploaded image's.
     """
 
     def __init__(self, image, lambdas=None, params=None):
         img = np.asarray(image)
-        if img.ndim != 2:
-            raise ValueError("Context expects a grey uint8 image")
+        if img.dtype != np.uint8 or img.ndim not in (2, 3) or (img.ndim == 3 and img.shape[2] != 3):
+            raise ValueError("Context expects a grey or BGR uint8 image")
         self.lambdas = list(lambdas) if lambdas is not None else makeLambdasLog(4, 64, 2)
-        self.cuda_data = CudaStuff(img.shape[1], img.shape[0], self.lambdas, params)
-        self.current_image = _as_gpu_u8(img)
+        h, w = img.shape[:2]
+        self.cuda_data = CudaStuff(w, h, self.lambdas, params, input_size=min_size_dims(w, h))
         self.current_keypoints = None
-        self.has_changed_keypoints = True
+        self.loadImage(img)
 
     def width(self) -> int:
         return int(self.current_image.shape[1])
@@ -309,7 +346,19 @@ class Context:
         return int(self.current_image.shape[0])
 
     def loadImage(self, new_image):
-        self.current_image = _as_gpu_u8(new_image)
+        """A host image (numpy, through getGPUImage) or a grey uint8 CUDA
+        tensor of the uploaded size (loadImage(GpuMat))."""
+        torch = _torch()
+        if isinstance(new_image, torch.Tensor):
+            grey, colour = _as_gpu_u8(new_image), None
+        else:
+            img = np.asarray(new_image)
+            grey = gpu_image_device(img, grayscale=True)
+            colour = gpu_image_device(img, grayscale=False) if img.ndim == 3 else None
+        if tuple(grey.shape) != (self.cuda_data.input_height, self.cuda_data.input_width):
+            raise ValueError("loadImage: size differs from the context's")
+        self.current_image = grey
+        self.current_image_color = colour
         self.has_changed_keypoints = True
 
     def getKeypoints(self):
@@ -322,12 +371,77 @@ class Context:
         return downloadKeypoints(self.getKeypoints())
 
     def getResponses(self) -> list:
-        """Per-scale summed keypoint map D and single-stopped map S."""
+        """Per-scale geometry with the summed keypoint map D and the
+        single-stopped map S."""
         self.getKeypoints()
         out = []
         for i, k in enumerate(self.cuda_data.ks):
             out.append(dict(k, D=self.cuda_data.dense_map(i, 0), S=self.cuda_data.dense_map(i, 1)))
         return out
+
+    def getColorFeatures(self) -> np.ndarray:
+        """24-bin colour histograms of the current keypoints (n x 24)."""
+        if self.current_image_color is None:
+            raise ValueError("the image has no colour")
+        h, w3 = self.current_image_color.shape
+        img = self.current_image_color.cpu().numpy().reshape(h, w3 // 3, 3)
+        return color_features(self.getKeypoints(), img)
+
+
+class Pipeline:
+    """Host frames in flight (bimp_pipeline_*): push() enqueues a uint8 host
+    frame and returns at once, pop() returns the oldest frame's records as a
+    structured array (the layout of detect_host).  Up to `depth` frames are
+    in flight, so one frame's copies overlap another's kernels.  A pushed
+    frame's memory must stay unchanged until it is popped (this class keeps a
+    reference to it)."""
+
+    def __init__(self, width: int, height: int, lambdas, depth: int = 3, capacity: int = KP_MAX_POINTS,
+                 params=None):
+        lam = (C.c_float * len(lambdas))(*[float(x) for x in lambdas])
+        p = _params(params)
+        h = C.c_void_p()
+        L.check(L.lib().bimp_pipeline_create(C.byref(h), int(width), int(height), lam, len(lambdas),
+                                             C.byref(p) if p is not None else None, int(depth), int(capacity)),
+                "Pipeline")
+        self._h = h
+        self.width, self.height, self.depth, self.capacity = int(width), int(height), int(depth), int(capacity)
+        self._frames = []
+        self._out = (L.KeyPointC * self.capacity)()
+
+    def in_flight(self) -> int:
+        return int(L.lib().bimp_pipeline_in_flight(self._h))
+
+    def push(self, image: np.ndarray):
+        img = np.asarray(image)
+        if img.dtype != np.uint8 or img.shape != (self.height, self.width) or img.strides[1] != 1:
+            raise ValueError("expected a uint8 host image of the pipeline's size (rows contiguous)")
+        L.check(L.lib().bimp_pipeline_push(self._h, C.c_void_p(img.ctypes.data), img.strides[0], self.width,
+                                           self.height), "pipeline_push")
+        self._frames.append(img)
+
+    def pop(self, capacity: int | None = None):
+        """(records, total, status) of the oldest frame in flight."""
+        cap = self.capacity if capacity is None else int(capacity)
+        n = C.c_int(0)
+        rc = L.lib().bimp_pipeline_pop(self._h, self._out, cap, C.byref(n))
+        if rc not in (L.BIMP_OK, L.BIMP_ERR_CAPACITY):
+            L.check(rc, "pipeline_pop")
+        self._frames.pop(0)
+        m = min(n.value, cap, self.capacity)
+        rec = np.frombuffer(self._out, dtype=_HOST_RECORD, count=m).copy()
+        return rec, n.value, rc
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            L.lib().bimp_pipeline_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:
@@ -452,6 +566,7 @@ class Adjoint:
         L.check(L.lib().bimp_adjoint_create(C.byref(h), int(width), int(height), int(n_images), lam, len(lambdas),
                                             C.byref(p) if p is not None else None), "Adjoint")
         self._h = h
+        self.params = p if p is not None else default_params()
         self.width, self.height, self.n = int(width), int(height), int(n_images)
         self.layout = []
         for s in range(L.lib().bimp_adjoint_num_scales(h)):

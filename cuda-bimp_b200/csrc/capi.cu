@@ -101,7 +101,8 @@ struct Engine {
   std::vector<ScaleHost> bank;          // geometry of the first image size + taps
   int nScales = 0;
   int nImages = 0;
-  std::vector<int> widths, heights;
+  std::vector<int> widths, heights;         // geometry sizes (CudaStuff's width x height)
+  std::vector<int> inWidths, inHeights;     // input image sizes (>= the geometry sizes)
   std::vector<std::vector<ScaleHost>> geo;   // per image per scale geometry
   // device memory
   char* d_mem = nullptr;
@@ -117,12 +118,13 @@ struct Engine {
   int nSten = 0;
   int2* d_rows = nullptr;
   int nRows = 0;
-  int* d_counts = nullptr;
-  int* d_offsets = nullptr;
-  int* d_imgRowStart = nullptr;
+  NmsCta* d_nmsCtas = nullptr;          // the NMS kernel's row groups (one image each)
+  int nNmsCtas = 0;
+  unsigned long long* d_nmsStatus = nullptr;   // the NMS CTAs' published prefixes (zeroed per detection)
+  size_t resetBytes = 0;                // d_maxKeys .. end of d_nmsStatus, zeroed per detection
   int* d_totals = nullptr;
   unsigned int* d_maxKeys = nullptr;
-  unsigned int* d_fault = nullptr;      // set by the tile kernel if a bounded wait expired
+  unsigned int* d_fault = nullptr;      // set by the tile kernel, the stencil or the NMS if a bounded wait expired
   KpOut* d_outs = nullptr;
   std::vector<PyrJob> h_pyr;                 // grouped by level
   std::vector<int> pyrFirst, pyrCount, pyrLevels, pyrMaxW, pyrMaxH;   // per launch (up to 3 levels)
@@ -184,20 +186,27 @@ struct Engine {
     return BIMP_OK;
   }
 
+  // inW/inH (null: the geometry sizes) are the sizes of the images a
+  // detection takes: each pyramid level of the input is computed in full,
+  // and each scale filters the top-left dataW x dataH window of its level.
   int build(int dev, const int* w, const int* h, int n, const float* lambdas, int nl,
-            const bimp_params& p, int internalKpCap) {
+            const bimp_params& p, int internalKpCap, const int* inW = nullptr, const int* inH = nullptr) {
     device = dev;
     params = p;
     nImages = n;
     widths.assign(w, w + n);
     heights.assign(h, h + n);
+    inWidths.assign(inW ? inW : w, (inW ? inW : w) + n);
+    inHeights.assign(inH ? inH : h, (inH ? inH : h) + n);
     std::vector<float> lam(lambdas, lambdas + nl);
     std::string err;
     geo.resize(n);
     for (int i = 0; i < n; ++i) {
       if (w[i] < 2 || h[i] < 2) return fail(BIMP_ERR_INVALID, "image size must be at least 2x2");
-      if (w[i] > 32767 || h[i] > 32767)   // tile index maps are int16
+      if (w[i] > 32767 || h[i] > 32767 || inWidths[i] > 32767 || inHeights[i] > 32767)   // int16 tile index maps
         return fail(BIMP_ERR_UNSUPPORTED, "image sides above 32767 pixels are not supported");
+      if (inWidths[i] < w[i] || inHeights[i] < h[i])
+        return fail(BIMP_ERR_INVALID, "input image smaller than the context's size");
       if (!build_scales(w[i], h[i], lam, p, geo[i], err)) return fail(BIMP_ERR_INVALID, err);
       if (i == 0) bank = geo[0];
       for (auto& s : geo[i]) {        // taps and spectra are shared with image 0
@@ -220,7 +229,7 @@ struct Engine {
     int maxLevel = 0;
     for (auto& s : bank) maxLevel = std::max(maxLevel, s.level);
     for (int i = 0; i < n; ++i) {
-      int cw = w[i], ch = h[i];
+      int cw = inWidths[i], ch = inHeights[i];
       for (int l = 0; l <= maxLevel; ++l) {
         if (l > 0) { cw = (cw + 1) / 2; ch = (ch + 1) / 2; }
         const int pitch = static_cast<int>(align_up(cw, 16));
@@ -303,6 +312,15 @@ struct Engine {
       }
     }
     imgRowStart.push_back(static_cast<int>(rows.size()));
+    // NMS row groups: consecutive candidate rows of one image, kNmsRowsPerCta per CTA
+    std::vector<NmsCta> nmsCtas;
+    for (int i = 0; i < n; ++i) {
+      const int first = static_cast<int>(nmsCtas.size());
+      for (int r = imgRowStart[i]; r < imgRowStart[i + 1]; r += kNmsRowsPerCta)
+        nmsCtas.push_back({r, std::min(kNmsRowsPerCta, imgRowStart[i + 1] - r), first, i, 0});
+      if (static_cast<int>(nmsCtas.size()) > first) nmsCtas.back().last = 1;
+    }
+    nNmsCtas = static_cast<int>(nmsCtas.size());
     // pyramid jobs: up to 3 levels per launch (levels 1-3 from level 0,
     // 4-6 from level 3, ...)
     pyrFirst.clear(); pyrCount.clear(); pyrLevels.clear(); pyrMaxW.clear(); pyrMaxH.clear(); h_pyr.clear();
@@ -342,11 +360,13 @@ struct Engine {
     const size_t offTiles = a.reserve(sizeof(TileWork) * std::max<size_t>(1, (size_t)tileCap));
     const size_t offSten = a.reserve(sizeof(int2) * std::max<size_t>(1, sten.size()));
     const size_t offRows = a.reserve(sizeof(int2) * std::max<size_t>(1, rows.size()));
-    const size_t offCounts = a.reserve(sizeof(int) * std::max<size_t>(1, rows.size()));
-    const size_t offOffsets = a.reserve(sizeof(int) * std::max<size_t>(1, rows.size()));
-    const size_t offImgRow = a.reserve(sizeof(int) * imgRowStart.size());
+    const size_t offNmsCtas = a.reserve(sizeof(NmsCta) * std::max<size_t>(1, nmsCtas.size()));
     const size_t offTotals = a.reserve(sizeof(int) * n);
-    const size_t offMax = a.reserve(sizeof(unsigned int) * (sds.size() + 1));
+    // per-detection reset region: the map maxima, the fault word, the NMS
+    // status words (8-byte aligned), cleared by one memset
+    const size_t maxBytes = align_up(sizeof(unsigned int) * (sds.size() + 1), 8);
+    const size_t offMax = a.reserve(maxBytes + sizeof(unsigned long long) * std::max<size_t>(1, nmsCtas.size()));
+    resetBytes = maxBytes + sizeof(unsigned long long) * std::max<size_t>(1, nmsCtas.size());
     const size_t offOuts = a.reserve(sizeof(KpOut) * n);
     const size_t offPyr = a.reserve(sizeof(PyrJob) * std::max<size_t>(1, h_pyr.size()));
     const size_t offMaps = a.reserve(kTensorMapBytes * sds.size());
@@ -401,11 +421,10 @@ struct Engine {
     d_tiles = reinterpret_cast<TileWork*>(base + offTiles);
     d_sten = reinterpret_cast<int2*>(base + offSten);
     d_rows = reinterpret_cast<int2*>(base + offRows);
-    d_counts = reinterpret_cast<int*>(base + offCounts);
-    d_offsets = reinterpret_cast<int*>(base + offOffsets);
-    d_imgRowStart = reinterpret_cast<int*>(base + offImgRow);
+    d_nmsCtas = reinterpret_cast<NmsCta*>(base + offNmsCtas);
     d_totals = reinterpret_cast<int*>(base + offTotals);
     d_maxKeys = reinterpret_cast<unsigned int*>(base + offMax);
+    d_nmsStatus = reinterpret_cast<unsigned long long*>(base + offMax + maxBytes);
     d_fault = d_maxKeys + sds.size();
     d_outs = reinterpret_cast<KpOut*>(base + offOuts);
     d_pyr = reinterpret_cast<PyrJob*>(base + offPyr);
@@ -424,8 +443,10 @@ struct Engine {
       BIMP_CUDA(cudaMemcpy(d_sten, sten.data(), sizeof(int2) * sten.size(), cudaMemcpyHostToDevice));
     if (!rows.empty())
       BIMP_CUDA(cudaMemcpy(d_rows, rows.data(), sizeof(int2) * rows.size(), cudaMemcpyHostToDevice));
-    BIMP_CUDA(cudaMemcpy(d_imgRowStart, imgRowStart.data(), sizeof(int) * imgRowStart.size(),
-                         cudaMemcpyHostToDevice));
+    if (!nmsCtas.empty())
+      BIMP_CUDA(cudaMemcpy(d_nmsCtas, nmsCtas.data(), sizeof(NmsCta) * nmsCtas.size(), cudaMemcpyHostToDevice));
+    // images without candidate rows keep a total of zero
+    BIMP_CUDA(cudaMemset(d_totals, 0, sizeof(int) * n));
     if (!h_pyr.empty())
       BIMP_CUDA(cudaMemcpy(d_pyr, h_pyr.data(), sizeof(PyrJob) * h_pyr.size(), cudaMemcpyHostToDevice));
     if (internalKpCap > 0) {
@@ -438,7 +459,7 @@ struct Engine {
       }
       BIMP_CUDA(cudaMemcpy(d_outs, outs.data(), sizeof(KpOut) * n, cudaMemcpyHostToDevice));
     }
-    BIMP_CUDA(cudaMemset(d_maxKeys, 0, sizeof(unsigned int) * (sds.size() + 1)));
+    BIMP_CUDA(cudaMemset(d_maxKeys, 0, resetBytes));
     return BIMP_OK;
   }
 
@@ -455,7 +476,7 @@ struct Engine {
         if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD);
         break;
       case 3:
-        launch_nms(d_sd, d_rows, nRows, d_counts, d_offsets, d_imgRowStart, nImages, d_totals, d_outs, s);
+        launch_nms_fused(d_sd, d_rows, d_nmsCtas, nNmsCtas, d_nmsStatus, d_totals, d_outs, d_fault, s);
         break;
       default:
         return fail(BIMP_ERR_INVALID, "unknown stage");
@@ -465,14 +486,14 @@ struct Engine {
   }
 
   int kernel_launches() const {
-    return static_cast<int>(pyrFirst.size()) + (nTiles > 0) + (nSten > 0) + 1 + 2 * (nRows > 0);
+    return static_cast<int>(pyrFirst.size()) + (nTiles > 0) + (nSten > 0) + (nNmsCtas > 0);
   }
 
   // Everything after the level-0 images are in place.
   int enqueue(cudaStream_t s) {
     int rc = stage(0, s);
     if (rc != BIMP_OK) return rc;
-    BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, sizeof(unsigned int) * (h_sd.size() + 1), s));
+    BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, resetBytes, s));
     for (int k = 1; k <= 3; ++k) {
       rc = stage(k, s);
       if (rc != BIMP_OK) return rc;
@@ -491,13 +512,20 @@ struct Engine {
 // ---------------------------------------------------------------------------
 struct bimp_context {
   Engine eng;
-  int width = 0, height = 0;
+  int width = 0, height = 0;         // geometry (CudaStuff) size
+  int inWidth = 0, inHeight = 0;     // size of the images a detection takes
   std::vector<ScaleHost> info;
   // host path: pinned count/fault words; device scratch the NMS writes
   // cv::KeyPoint records into before the single copy to the caller's array
   int* h_count = nullptr;   // pinned: [0] keypoint total, [1] device fault word
   float* d_kpScratch = nullptr;
   int d_kpScratchCap = 0;
+  // pinned host staging of the records, and how many records go back with
+  // the count before the first synchronisation (the last call's count plus
+  // a margin), so that one synchronisation usually serves a whole call
+  bimp_keypoint* h_stage = nullptr;
+  int h_stageCap = 0;
+  int specRecords = 1024;
   // line/edge detection, allocated on first use: e + i o of one scale, that
   // scale's descriptor and tile list
   float2* d_leZ = nullptr;
@@ -523,6 +551,17 @@ struct bimp_batch {
   cudaStream_t capStream = nullptr;
   int* h_totals = nullptr;   // pinned: n_images totals, then the device fault word
   std::vector<bimp_keypoint> tmp;
+};
+
+// Host frames in flight: `depth` contexts of one image size, each with its
+// own stream, used round robin, so that one frame's copies overlap another
+// frame's kernels.
+struct bimp_pipeline {
+  std::vector<bimp_context*> ctx;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> done;
+  std::vector<int> spec;
+  int depth = 0, capacity = 0, head = 0, inFlight = 0, device = 0;
 };
 
 namespace {
@@ -593,12 +632,14 @@ int bimp_make_lambdas_lin(float start, float end, int num, float* out, int cap, 
 
 int bimp_snap_transform_size(int n) { return snap_transform_size(n); }
 
-int bimp_ctx_create(bimp_context** ctx, int width, int height, const float* lambdas, int n_lambdas,
-                    const bimp_params* params) {
+int bimp_ctx_create_for_input(bimp_context** ctx, int width, int height, int input_width, int input_height,
+                              const float* lambdas, int n_lambdas, const bimp_params* params) {
   if (!ctx) return fail(BIMP_ERR_INVALID, "ctx is null");
   *ctx = nullptr;
   if (!lambdas || n_lambdas <= 0) return fail(BIMP_ERR_INVALID, "empty wavelength list");
   if (width < 2 || height < 2) return fail(BIMP_ERR_INVALID, "image size must be at least 2x2");
+  if (input_width < width || input_height < height)
+    return fail(BIMP_ERR_INVALID, "input image smaller than the context's size");
   int dev = 0;
   BIMP_CUDA(cudaGetDevice(&dev));
   int rc = ensure_device_configured(dev);
@@ -606,8 +647,10 @@ int bimp_ctx_create(bimp_context** ctx, int width, int height, const float* lamb
   bimp_context* c = new bimp_context();
   c->width = width;
   c->height = height;
+  c->inWidth = input_width;
+  c->inHeight = input_height;
   const bimp_params p = params ? *params : default_params();
-  rc = c->eng.build(dev, &width, &height, 1, lambdas, n_lambdas, p, 0);
+  rc = c->eng.build(dev, &width, &height, 1, lambdas, n_lambdas, p, 0, &input_width, &input_height);
   if (rc != BIMP_OK) {
     c->eng.release();
     delete c;
@@ -625,6 +668,11 @@ int bimp_ctx_create(bimp_context** ctx, int width, int height, const float* lamb
   return BIMP_OK;
 }
 
+int bimp_ctx_create(bimp_context** ctx, int width, int height, const float* lambdas, int n_lambdas,
+                    const bimp_params* params) {
+  return bimp_ctx_create_for_input(ctx, width, height, width, height, lambdas, n_lambdas, params);
+}
+
 int bimp_ctx_destroy(bimp_context* c) {
   if (!c) return BIMP_OK;
   cudaSetDevice(c->eng.device);
@@ -633,6 +681,7 @@ int bimp_ctx_destroy(bimp_context* c) {
   c->eng.release();
   if (c->h_count) cudaFreeHost(c->h_count);
   if (c->d_kpScratch) cudaFree(c->d_kpScratch);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
   if (c->d_leZ) cudaFree(c->d_leZ);
   if (c->d_leSd) cudaFree(c->d_leSd);
   if (c->d_leTiles) cudaFree(c->d_leTiles);
@@ -662,7 +711,7 @@ static int ctx_run(bimp_context* c, const uint8_t* image, size_t pitch, int widt
                    cudaMemcpyKind kind, float* d_kp, size_t ld, int capacity, int* d_count,
                    cudaStream_t s, int aos = 0) {
   if (!c || !image) return fail(BIMP_ERR_INVALID, "null argument");
-  if (width != c->width || height != c->height)
+  if (width != c->inWidth || height != c->inHeight)
     return fail(BIMP_ERR_INVALID, "image size differs from the context's");
   if (pitch < (size_t)width) return fail(BIMP_ERR_INVALID, "pitch smaller than width");
   if (capacity < 0) return fail(BIMP_ERR_INVALID, "negative capacity");
@@ -731,6 +780,56 @@ static int ensure_host_buffers(bimp_context* c, int capacity) {
     BIMP_CUDA(cudaMalloc(&c->d_kpScratch, sizeof(float) * BIMP_KP_VECTOR_LENGTH * (size_t)capacity));
     c->d_kpScratchCap = capacity;
   }
+  if (c->h_stageCap < capacity) {
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    c->h_stageCap = 0;
+    BIMP_CUDA(cudaMallocHost(&c->h_stage, sizeof(bimp_keypoint) * (size_t)capacity));
+    c->h_stageCap = capacity;
+  }
+  return BIMP_OK;
+}
+
+// Host path, first half: the image copy, the detection (records written as
+// cv::KeyPoint-layout structs into the device scratch), and the copies back
+// of the count, the fault word and the first *spec records into the pinned
+// staging, all on stream s.  Nothing waits.
+static int host_enqueue(bimp_context* c, const uint8_t* image, size_t pitch, int width, int height, int capacity,
+                        cudaStream_t s, int* spec) {
+  BIMP_CUDA(cudaSetDevice(c->eng.device));
+  const int cap = std::max(capacity, 1);
+  int rc = ensure_host_buffers(c, cap);
+  if (rc != BIMP_OK) return rc;
+  rc = ctx_run(c, image, pitch, width, height, cudaMemcpyHostToDevice, c->d_kpScratch, cap, capacity, nullptr, s, 1);
+  if (rc != BIMP_OK) return rc;
+  BIMP_CUDA(cudaMemcpyAsync(c->h_count, c->eng.d_totals, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIMP_CUDA(cudaMemcpyAsync(c->h_count + 1, c->eng.d_fault, sizeof(int), cudaMemcpyDeviceToHost, s));
+  *spec = std::min(capacity, c->specRecords);
+  if (*spec > 0)
+    BIMP_CUDA(cudaMemcpyAsync(c->h_stage, c->d_kpScratch, sizeof(bimp_keypoint) * (size_t)*spec,
+                              cudaMemcpyDeviceToHost, s));
+  return BIMP_OK;
+}
+
+// Host path, second half, once stream s has finished the first: the records
+// beyond the speculative copy (rare: a count well above the previous call's)
+// come back with one more copy and synchronisation, then everything is
+// copied from the staging into the caller's array.
+static int host_finish(bimp_context* c, int spec, bimp_keypoint* out, int capacity, int* n_found, cudaStream_t s) {
+  const int total = c->h_count[0];
+  *n_found = total;
+  if (c->h_count[1]) return fail(BIMP_ERR_CUDA, "a bounded device wait expired");
+  const int n = std::min(total, capacity);
+  if (n > spec) {
+    BIMP_CUDA(cudaMemcpyAsync(c->h_stage + spec, reinterpret_cast<const bimp_keypoint*>(c->d_kpScratch) + spec,
+                              sizeof(bimp_keypoint) * (size_t)(n - spec), cudaMemcpyDeviceToHost, s));
+    BIMP_CUDA(cudaStreamSynchronize(s));
+  }
+  static_assert(sizeof(bimp_keypoint) == 7 * sizeof(float), "record layout");
+  if (n > 0) std::memcpy(out, c->h_stage, sizeof(bimp_keypoint) * (size_t)n);
+  c->specRecords = std::max(256, std::min(std::max(capacity, 1), n + n / 8 + 256));
+  if (total > capacity)
+    return fail(BIMP_ERR_CAPACITY, "keypoints exceed capacity (" + std::to_string(total) + ")");
   return BIMP_OK;
 }
 
@@ -739,29 +838,11 @@ int bimp_detect_host(bimp_context* c, const uint8_t* image, size_t pitch, int wi
   if (!c || !n_found || capacity < 0 || (capacity > 0 && !out))
     return fail(BIMP_ERR_INVALID, "null argument");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  BIMP_CUDA(cudaSetDevice(c->eng.device));
-  const int cap = std::max(capacity, 1);
-  int rc = ensure_host_buffers(c, cap);
+  int spec = 0;
+  const int rc = host_enqueue(c, image, pitch, width, height, capacity, s, &spec);
   if (rc != BIMP_OK) return rc;
-  // the NMS writes cv::KeyPoint-layout records straight into the scratch
-  rc = ctx_run(c, image, pitch, width, height, cudaMemcpyHostToDevice, c->d_kpScratch, cap,
-               capacity, nullptr, s, 1);
-  if (rc != BIMP_OK) return rc;
-  BIMP_CUDA(cudaMemcpyAsync(c->h_count, c->eng.d_totals, sizeof(int), cudaMemcpyDeviceToHost, s));
-  BIMP_CUDA(cudaMemcpyAsync(c->h_count + 1, c->eng.d_fault, sizeof(int), cudaMemcpyDeviceToHost, s));
   BIMP_CUDA(cudaStreamSynchronize(s));
-  const int total = *c->h_count;
-  if (c->h_count[1]) return fail(BIMP_ERR_CUDA, "a bounded device wait expired");
-  const int n = std::min(total, capacity);
-  if (n > 0) {
-    static_assert(sizeof(bimp_keypoint) == 7 * sizeof(float), "record layout");
-    BIMP_CUDA(cudaMemcpyAsync(out, c->d_kpScratch, sizeof(bimp_keypoint) * (size_t)n, cudaMemcpyDeviceToHost, s));
-    BIMP_CUDA(cudaStreamSynchronize(s));
-  }
-  *n_found = total;
-  if (total > capacity)
-    return fail(BIMP_ERR_CAPACITY, "keypoints exceed capacity (" + std::to_string(total) + ")");
-  return BIMP_OK;
+  return host_finish(c, spec, out, capacity, n_found, s);
 }
 
 int bimp_dense_map(bimp_context* c, int scale, int which, float* d_out, size_t ld, void* stream) {
@@ -1083,6 +1164,111 @@ int bimp_batch_detect_host(bimp_batch* b, const uint8_t* const* images, const si
     }
   }
   if (status != BIMP_OK) return fail(status, "keypoints exceed capacity for some image");
+  return BIMP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pipelined host frames
+// ---------------------------------------------------------------------------
+int bimp_pipeline_destroy(bimp_pipeline* p) {
+  if (!p) return BIMP_OK;
+  cudaSetDevice(p->device);
+  for (cudaStream_t st : p->streams)
+    if (st) cudaStreamSynchronize(st);
+  for (bimp_context* c : p->ctx) bimp_ctx_destroy(c);
+  for (cudaStream_t st : p->streams)
+    if (st) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : p->done)
+    if (ev) cudaEventDestroy(ev);
+  delete p;
+  return BIMP_OK;
+}
+
+int bimp_pipeline_create(bimp_pipeline** out, int width, int height, const float* lambdas, int n_lambdas,
+                         const bimp_params* params, int depth, int capacity) {
+  if (!out) return fail(BIMP_ERR_INVALID, "pipeline is null");
+  *out = nullptr;
+  if (depth < 1 || depth > 8 || capacity < 1) return fail(BIMP_ERR_INVALID, "depth must be 1..8, capacity >= 1");
+  bimp_pipeline* p = new bimp_pipeline();
+  cudaGetDevice(&p->device);
+  p->depth = depth;
+  p->capacity = capacity;
+  p->ctx.assign(depth, nullptr);
+  p->streams.assign(depth, nullptr);
+  p->done.assign(depth, nullptr);
+  p->spec.assign(depth, 0);
+  for (int k = 0; k < depth; ++k) {
+    int rc = bimp_ctx_create(&p->ctx[k], width, height, lambdas, n_lambdas, params);
+    if (rc == BIMP_OK) rc = ensure_host_buffers(p->ctx[k], capacity);
+    cudaError_t e = cudaSuccess;
+    if (rc == BIMP_OK) e = cudaStreamCreateWithFlags(&p->streams[k], cudaStreamNonBlocking);
+    if (rc == BIMP_OK && e == cudaSuccess) e = cudaEventCreateWithFlags(&p->done[k], cudaEventDisableTiming);
+    if (rc == BIMP_OK && e != cudaSuccess) rc = fail(BIMP_ERR_CUDA, std::string("pipeline setup: ") + cudaGetErrorString(e));
+    if (rc != BIMP_OK) {
+      const std::string msg = g_last_error;
+      bimp_pipeline_destroy(p);
+      return fail(rc, msg);
+    }
+  }
+  *out = p;
+  return BIMP_OK;
+}
+
+int bimp_pipeline_in_flight(const bimp_pipeline* p) { return p ? p->inFlight : 0; }
+
+int bimp_pipeline_push(bimp_pipeline* p, const uint8_t* image, size_t pitch, int width, int height) {
+  if (!p || !image) return fail(BIMP_ERR_INVALID, "null argument");
+  if (p->inFlight == p->depth) return fail(BIMP_ERR_INVALID, "pipeline full: pop a frame first");
+  const int k = (p->head + p->inFlight) % p->depth;
+  int rc = host_enqueue(p->ctx[k], image, pitch, width, height, p->capacity, p->streams[k], &p->spec[k]);
+  if (rc != BIMP_OK) return rc;
+  BIMP_CUDA(cudaEventRecord(p->done[k], p->streams[k]));
+  ++p->inFlight;
+  return BIMP_OK;
+}
+
+int bimp_pipeline_pop(bimp_pipeline* p, bimp_keypoint* out, int capacity, int* n_found) {
+  if (!p || !n_found || capacity < 0 || (capacity > 0 && !out)) return fail(BIMP_ERR_INVALID, "null argument");
+  if (p->inFlight == 0) return fail(BIMP_ERR_INVALID, "no frame in flight");
+  const int k = p->head;
+  p->head = (p->head + 1) % p->depth;
+  --p->inFlight;
+  BIMP_CUDA(cudaSetDevice(p->device));
+  BIMP_CUDA(cudaEventSynchronize(p->done[k]));
+  int total = 0;
+  const int rc = host_finish(p->ctx[k], p->spec[k], out, std::min(capacity, p->capacity), &total, p->streams[k]);
+  *n_found = total;
+  if (rc == BIMP_ERR_CAPACITY && total <= capacity) {
+    // more than the pipeline's own capacity was found: the records beyond it
+    // were never written
+    return fail(BIMP_ERR_CAPACITY, "keypoints exceed the pipeline capacity (" + std::to_string(total) + ")");
+  }
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// device memory helpers (for callers without the CUDA runtime headers)
+// ---------------------------------------------------------------------------
+int bimp_device_alloc(void** ptr, size_t bytes) {
+  if (!ptr) return fail(BIMP_ERR_INVALID, "ptr is null");
+  *ptr = nullptr;
+  if (bytes == 0) return BIMP_OK;
+  BIMP_CUDA(cudaMalloc(ptr, bytes));
+  return BIMP_OK;
+}
+
+int bimp_device_free(void* ptr) {
+  if (ptr) BIMP_CUDA(cudaFree(ptr));
+  return BIMP_OK;
+}
+
+int bimp_copy_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width_bytes, size_t rows,
+                 void* stream) {
+  if (rows == 0 || width_bytes == 0) return BIMP_OK;
+  if (!dst || !src || dpitch < width_bytes || spitch < width_bytes) return fail(BIMP_ERR_INVALID, "bad copy arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BIMP_CUDA(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width_bytes, rows, cudaMemcpyDefault, s));
+  BIMP_CUDA(cudaStreamSynchronize(s));
   return BIMP_OK;
 }
 

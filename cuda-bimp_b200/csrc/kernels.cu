@@ -659,6 +659,79 @@ k_scan(const int* __restrict__ counts, int* __restrict__ offsets, int n,
   }
 }
 
+// One keypoint record of row y at column x, slot idx: subpixel position from
+// the parabolas through the 3 samples per axis (cuda_bimp.cuh:114-132),
+// cv::KeyPoint fields.
+__device__ __forceinline__ void nms_emit(const ScaleDev* __restrict__ sd, const KpOut& out, int y, int x, int idx) {
+  const float* __restrict__ D = sd->D;
+  const int dp = sd->dPitch;
+  const float pyr = sd->pyrstep, kpSize = sd->kpSize;
+  const int kpOctave = sd->kpOctave;
+  const float* r1 = D + (size_t)y * dp;
+  const float xv1 = r1[x - 1], xv2 = r1[x], xv3 = r1[x + 1];
+  const float yv1 = r1[x - dp], yv3 = r1[x + dp];
+  float xpos = (float)x, ypos = (float)y;
+  const float denx = xv1 + xv3 - 2.f * xv2;
+  const float deny = yv1 + yv3 - 2.f * xv2;
+  const float numx = 0.5f * (xv1 - xv3);
+  const float numy = 0.5f * (yv1 - yv3);
+  if (denx != 0.f) xpos += __fdiv_rn(numx, denx);
+  if (deny != 0.f) ypos += __fdiv_rn(numy, deny);
+  float* kpm = out.kp;
+  if (out.aos) {   // pt.x, pt.y, size, angle, response, octave, class_id
+    float* k = kpm + (size_t)7 * idx;
+    k[0] = xpos * pyr;
+    k[1] = ypos * pyr;
+    k[2] = kpSize;
+    k[3] = -1.f;
+    k[4] = xv2;
+    reinterpret_cast<int*>(k)[5] = kpOctave;
+    reinterpret_cast<int*>(k)[6] = 1;
+  } else {
+    const size_t ld = out.ld;
+    kpm[0 * ld + idx] = xpos * pyr;
+    kpm[1 * ld + idx] = ypos * pyr;
+    reinterpret_cast<int*>(kpm)[2 * ld + idx] = 1;
+    reinterpret_cast<int*>(kpm)[3 * ld + idx] = kpOctave;
+    kpm[4 * ld + idx] = kpSize;
+    kpm[5 * ld + idx] = -1.f;
+    kpm[6 * ld + idx] = xv2;
+  }
+}
+
+// One warp: the records of candidate row `iy` from its stored decision words,
+// at slots base, base + 1, ... (x order).  32 words per round, one per lane:
+// each lane writes its word's keypoints at the word's place in the row (a
+// warp prefix sum of the word popcounts keeps x order), so a dense row costs
+// as many steps as its densest word has bits, not one step per chunk.
+__device__ __forceinline__ void nms_write_row(const ScaleDev* __restrict__ sd, const KpOut& out, int iy, int base,
+                                              int lane) {
+  const int off = sd->off;
+  const int y = off + 1 + iy;
+  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
+  const int nch = (xEnd - off - 1 + 31) / 32;
+  const unsigned int* __restrict__ mask = sd->nmsMask + (size_t)iy * sd->nmsChunks;
+  for (int c0 = 0; c0 < nch && base < out.capacity; c0 += 32) {
+    unsigned int word = c0 + lane < nch ? mask[c0 + lane] : 0u;
+    const int pc = __popc(word);
+    int incl = pc;
+#pragma unroll
+    for (int m = 1; m < 32; m <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, m);
+      if (lane >= m) incl += u;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    int idx = base + incl - pc;
+    while (word) {
+      const int bit = __ffs(word) - 1;
+      word &= word - 1u;
+      if (idx < out.capacity) nms_emit(sd, out, y, off + 1 + 32 * (c0 + lane) + bit, idx);
+      ++idx;
+    }
+    base += total;
+  }
+}
+
 // Records of a row in x order at the row's offset (one warp per row).
 __global__ void __launch_bounds__(32 * kNmsWriteRows)
 k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int nrows,
@@ -670,90 +743,157 @@ k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int
   const int2 item = rows[r];
   const ScaleDev* sd = sds + item.x;
   const KpOut out = outs[sd->image];
-  const int off = sd->off;
-  const int y = off + 1 + item.y;
-  const float thr = scale_thresh(sd);
-  int base = offsets[r] - offsets[imageRowStart[sd->image]];
+  const int base = offsets[r] - offsets[imageRowStart[sd->image]];
   if (base >= out.capacity) return;
-  const float* __restrict__ D = sd->D;
-  const int dp = sd->dPitch;
-  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
-  const float pyr = sd->pyrstep, kpSize = sd->kpSize;
-  const int kpOctave = sd->kpOctave;
-  const unsigned int* __restrict__ mask = sd->nmsMask ? sd->nmsMask + (size_t)item.y * sd->nmsChunks : nullptr;
-  const int nch = (xEnd - off - 1 + 31) / 32;
-  // One keypoint record: subpixel position from the parabolas through the
-  // 3 samples per axis (cuda_bimp.cuh:114-132), cv::KeyPoint fields.
-  auto emit = [&](int x, int idx) {
-    const float* r1 = D + (size_t)y * dp;
-    const float xv1 = r1[x - 1], xv2 = r1[x], xv3 = r1[x + 1];
-    const float yv1 = r1[x - dp], yv3 = r1[x + dp];
-    float xpos = (float)x, ypos = (float)y;
-    const float denx = xv1 + xv3 - 2.f * xv2;
-    const float deny = yv1 + yv3 - 2.f * xv2;
-    const float numx = 0.5f * (xv1 - xv3);
-    const float numy = 0.5f * (yv1 - yv3);
-    if (denx != 0.f) xpos += __fdiv_rn(numx, denx);
-    if (deny != 0.f) ypos += __fdiv_rn(numy, deny);
-    float* kpm = out.kp;
-    if (out.aos) {   // pt.x, pt.y, size, angle, response, octave, class_id
-      float* k = kpm + (size_t)7 * idx;
-      k[0] = xpos * pyr;
-      k[1] = ypos * pyr;
-      k[2] = kpSize;
-      k[3] = -1.f;
-      k[4] = xv2;
-      reinterpret_cast<int*>(k)[5] = kpOctave;
-      reinterpret_cast<int*>(k)[6] = 1;
-    } else {
-      const size_t ld = out.ld;
-      kpm[0 * ld + idx] = xpos * pyr;
-      kpm[1 * ld + idx] = ypos * pyr;
-      reinterpret_cast<int*>(kpm)[2 * ld + idx] = 1;
-      reinterpret_cast<int*>(kpm)[3 * ld + idx] = kpOctave;
-      kpm[4 * ld + idx] = kpSize;
-      kpm[5 * ld + idx] = -1.f;
-      kpm[6 * ld + idx] = xv2;
-    }
-  };
-  if (mask) {
-    // 32 decision words per round, one per lane: each lane writes its word's
-    // keypoints at the word's place in the row (a warp prefix sum of the
-    // word popcounts keeps x order), so a dense row costs as many steps as
-    // its densest word has bits, not one step per chunk with a keypoint
-    for (int c0 = 0; c0 < nch; c0 += 32) {
-      unsigned int word = c0 + lane < nch ? mask[c0 + lane] : 0u;
-      const int pc = __popc(word);
-      int incl = pc;
-#pragma unroll
-      for (int m = 1; m < 32; m <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, incl, m);
-        if (lane >= m) incl += u;
-      }
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
-      int idx = base + incl - pc;
-      while (word) {
-        const int bit = __ffs(word) - 1;
-        word &= word - 1u;
-        if (idx < out.capacity) emit(off + 1 + 32 * (c0 + lane) + bit, idx);
-        ++idx;
-      }
-      base += total;
-      if (base >= out.capacity) return;
-    }
+  if (sd->nmsMask) {
+    nms_write_row(sd, out, item.y, base, lane);
     return;
   }
   // no stored decisions: test each chunk's pixels (one ballot per chunk)
+  const int off = sd->off;
+  const int y = off + 1 + item.y;
+  const float thr = scale_thresh(sd);
+  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
+  const int nch = (xEnd - off - 1 + 31) / 32;
+  int b = base;
   for (int c = 0; c < nch; ++c) {
     const int x = off + 1 + 32 * c + lane;
-    const unsigned int bal = __ballot_sync(0xffffffffu, x < xEnd && is_keypoint(D, dp, x, y, thr));
+    const unsigned int bal = __ballot_sync(0xffffffffu, x < xEnd && is_keypoint(sd->D, sd->dPitch, x, y, thr));
     if (!bal) continue;
     if ((bal >> lane) & 1u) {
-      const int idx = base + __popc(bal & ((1u << lane) - 1u));
-      if (idx < out.capacity) emit(x, idx);
+      const int idx = b + __popc(bal & ((1u << lane) - 1u));
+      if (idx < out.capacity) nms_emit(sd, out, y, x, idx);
     }
-    base += __popc(bal);
-    if (base >= out.capacity) return;
+    b += __popc(bal);
+    if (b >= out.capacity) return;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// single-pass NMS: decisions, the per-image chained row prefix, records
+// ---------------------------------------------------------------------------
+// One CTA per group of up to kNmsRowsPerCta candidate rows of one image (one
+// warp per row).  Each warp decides its row (strict 8-neighbour maximum above
+// the threshold) and stores the row's decision words; the CTA publishes its
+// keypoint count, learns the count of all earlier rows of its image from its
+// predecessors' published values (decoupled look-back: a predecessor's
+// inclusive prefix ends the walk, its bare count adds to it), publishes its
+// own inclusive prefix, and the warps write their rows' records.  The image's
+// last CTA writes the image total.  Every wait is bounded: on expiry the CTA
+// sets bit 2 of *fault and counts the missing predecessors as empty.
+constexpr unsigned long long kNmsAgg = 1ull << 62, kNmsInc = 2ull << 62;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// One warp: decision words of candidate row iy (stored to the row's mask
+// words) and its keypoint count.  The centre values of four chunks are loaded
+// together; the 8 neighbours only where the centre passes the threshold.
+__device__ __forceinline__ int nms_decide_row(const ScaleDev* __restrict__ sd, int iy, int lane) {
+  const int off = sd->off;
+  const int y = off + 1 + iy;
+  const float thr = scale_thresh(sd);
+  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
+  const int nch = (xEnd - off - 1 + 31) / 32;
+  const float* __restrict__ D = sd->D;
+  const int dp = sd->dPitch;
+  const float* __restrict__ row = D + (size_t)y * dp;
+  unsigned int* __restrict__ mask = sd->nmsMask + (size_t)iy * sd->nmsChunks;
+  int n = 0;
+  for (int c0 = 0; c0 < nch; c0 += 4) {
+    float v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int x = off + 1 + 32 * (c0 + u) + lane;
+      v[u] = (c0 + u < nch && x < xEnd) ? row[x] : -INFINITY;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (c0 + u >= nch) break;
+      const int x = off + 1 + 32 * (c0 + u) + lane;
+      bool k = false;
+      if (v[u] > thr) {
+        const float* r0 = row - dp;
+        const float* r2 = row + dp;
+        float dil = fmaxf(fmaxf(r0[x - 1], r0[x]), r0[x + 1]);
+        dil = fmaxf(dil, fmaxf(row[x - 1], row[x + 1]));
+        dil = fmaxf(dil, fmaxf(fmaxf(r2[x - 1], r2[x]), r2[x + 1]));
+        k = v[u] - dil > 0.f;
+      }
+      const unsigned int bal = __ballot_sync(0xffffffffu, k);
+      n += __popc(bal);
+      if (lane == 0) mask[c0 + u] = bal;
+    }
+  }
+  return n;
+}
+
+__global__ void __launch_bounds__(32 * kNmsRowsPerCta)
+k_nms_fused(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, const NmsCta* __restrict__ ctas,
+            unsigned long long* __restrict__ status, int* __restrict__ imageTotals, const KpOut* __restrict__ outs,
+            unsigned int* __restrict__ fault_word) {
+  __shared__ int s_cnt[kNmsRowsPerCta];
+  __shared__ int s_base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const NmsCta cta = ctas[blockIdx.x];
+  int2 item = make_int2(0, 0);
+  int cnt = 0;
+  if (warp < cta.nRows) {
+    item = rows[cta.rowStart + warp];
+    cnt = nms_decide_row(sds + item.x, item.y, lane);
+  }
+  if (lane == 0) s_cnt[warp] = cnt;
+  __syncthreads();
+  if (warp == 0) {
+    int total = lane < kNmsRowsPerCta ? s_cnt[lane] : 0;
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) total += __shfl_xor_sync(0xffffffffu, total, m);
+    const int b = blockIdx.x, first = cta.firstCta;
+    if (b != first && lane == 0) st_release_u64(status + b, kNmsAgg | (unsigned int)total);
+    unsigned long long prefix = 0;
+    int j = b - 1, spins = 0;
+    while (j >= first) {
+      const int idx = j - lane;
+      const unsigned long long v = idx >= first ? ld_acquire_u64(status + idx) : kNmsInc;
+      const unsigned int flag = (unsigned int)(v >> 62);
+      const unsigned int inc = __ballot_sync(0xffffffffu, flag == 2u);
+      const unsigned int none = __ballot_sync(0xffffffffu, flag == 0u);
+      const int L = inc ? __ffs(inc) - 1 : 31;
+      const unsigned int upto = L == 31 ? 0xffffffffu : ((2u << L) - 1u);
+      if (none & upto) {
+        if (++spins > (1 << 20)) {   // a predecessor never published: give up, count it as empty
+          if (lane == 0) atomicOr(fault_word, 4u);
+          break;
+        }
+        __nanosleep(64);
+        continue;
+      }
+      unsigned long long val = lane <= L ? (v & 0xffffffffull) : 0ull;
+#pragma unroll
+      for (int m = 16; m > 0; m >>= 1) val += __shfl_xor_sync(0xffffffffu, val, m);
+      prefix += val;
+      if (inc) break;
+      j -= 32;
+    }
+    if (lane == 0) {
+      st_release_u64(status + b, kNmsInc | (unsigned int)(prefix + total));
+      s_base = (int)prefix;
+      if (cta.last) imageTotals[cta.image] = (int)(prefix + total);
+    }
+  }
+  __syncthreads();
+  if (warp < cta.nRows && cnt > 0) {
+    const ScaleDev* sd = sds + item.x;
+    const KpOut out = outs[cta.image];
+    int base = s_base;
+    for (int w = 0; w < warp; ++w) base += s_cnt[w];
+    if (base < out.capacity) nms_write_row(sd, out, item.y, base, lane);
   }
 }
 
@@ -975,6 +1115,12 @@ void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigne
     k_stencil<kStencilAdj><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
   else
     k_stencil<kStencilD><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+}
+void launch_nms_fused(const ScaleDev* d_sd, const int2* d_rows, const NmsCta* d_ctas, int nctas,
+                      unsigned long long* d_status, int* d_totals, const KpOut* d_outs, unsigned int* d_fault,
+                      cudaStream_t s) {
+  if (nctas > 0)
+    k_nms_fused<<<nctas, 32 * kNmsRowsPerCta, 0, s>>>(d_sd, d_rows, d_ctas, d_status, d_totals, d_outs, d_fault);
 }
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,

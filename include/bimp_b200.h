@@ -114,6 +114,16 @@ int bimp_snap_transform_size(int data_size);
 int bimp_ctx_create(bimp_context** ctx, int width, int height,
                     const float* lambdas, int n_lambdas,
                     const bimp_params* params);
+/* The reference's Context(cv::Mat&) builds its CudaStuff from the image's
+ * own size (bimp/src/bimp.cpp:7-8) but detects on getGPUImage's output,
+ * which is upscaled when a side is below 350 pixels
+ * (bimp/src/cuda_bimp.cu:156-168).  Each scale then filters the top-left
+ * data_w x data_h window of its pyramid level of the larger image (convertTo
+ * and collectCVMemory, bimp/src/cuda_bimp.cu:481-486).  This creates such a
+ * context: geometry from width x height, detections taking images of
+ * input_width x input_height (>= width x height). */
+int bimp_ctx_create_for_input(bimp_context** ctx, int width, int height, int input_width, int input_height,
+                              const float* lambdas, int n_lambdas, const bimp_params* params);
 /* ~CudaStuff, bimp/src/cuda_bimp.cu:399-460. */
 int bimp_ctx_destroy(bimp_context* ctx);
 int bimp_ctx_num_scales(const bimp_context* ctx);
@@ -140,12 +150,40 @@ int bimp_detect_device_async(bimp_context* ctx, const uint8_t* d_image, size_t p
  * bimp/include/detection/bimp.hpp:35,38, bimp/src/bimp.cpp:7-20,89-92,
  * for an already-grey image: host uint8 image in, host cv::KeyPoint-layout
  * records out (utils.cpp:130-150 downloadKeypoints).  The records are
- * written on the device in this layout and copied once into `out` after the
- * count is known (pinned memory keeps the copies asynchronous); the call
- * synchronises `stream`. */
+ * written on the device in this layout and come back through the context's
+ * pinned staging with the count: as many as the previous call found plus a
+ * margin before the one synchronisation of `stream`, the rest (a count well
+ * above the previous call's) with one more copy and synchronisation. */
 int bimp_detect_host(bimp_context* ctx, const uint8_t* image, size_t pitch,
                      int width, int height, bimp_keypoint* out, int capacity,
                      int* n_found, void* stream);
+
+/* ---- pipelined host frames (no counterpart in the reference) -------------
+ * The reference handles one frame per call and synchronises the device at
+ * entry and exit (bimp/src/bimp.cpp:62, bimp/src/cuda_bimp.cu:115), so a
+ * frame's copies never overlap another frame's work.  A pipeline holds
+ * `depth` (1..8) contexts of one image size, each with its own stream, used
+ * round robin: push() enqueues a host frame (its copy to the device, the
+ * detection and the copy back of its records) and returns at once; pop()
+ * waits for the oldest frame and returns its records as bimp_detect_host
+ * does.  Up to `depth` frames are in flight, so the copies of one overlap
+ * the kernels of the others.
+ *
+ * The frame memory passed to push() must stay unchanged until that frame is
+ * popped; pinned memory keeps its copy asynchronous (pageable memory makes
+ * push() wait for the copy).  `capacity` records per frame at most;
+ * pop(capacity) returns BIMP_ERR_CAPACITY with the true total in *n_found
+ * when a frame had more than min(capacity, the pipeline's capacity). */
+typedef struct bimp_pipeline bimp_pipeline;
+int bimp_pipeline_create(bimp_pipeline** pipeline, int width, int height, const float* lambdas, int n_lambdas,
+                         const bimp_params* params, int depth, int capacity);
+int bimp_pipeline_destroy(bimp_pipeline* pipeline);
+/* BIMP_ERR_INVALID when `depth` frames are already in flight. */
+int bimp_pipeline_push(bimp_pipeline* pipeline, const uint8_t* image, size_t pitch, int width, int height);
+/* Records of the oldest frame in flight, in (scale, y, x) order;
+ * BIMP_ERR_INVALID when no frame is in flight. */
+int bimp_pipeline_pop(bimp_pipeline* pipeline, bimp_keypoint* out, int capacity, int* n_found);
+int bimp_pipeline_in_flight(const bimp_pipeline* pipeline);
 
 /* Per-scale dense maps of the last detection (Context::getResponses,
  * bimp/src/bimp.cpp:94-104; k.d_ResultDouble / k.d_ResultSingle).
@@ -243,6 +281,17 @@ int bimp_ctx_kernel_launches(const bimp_context* ctx);
  * detection's keypoint destination).  Inputs of the stage are the buffers
  * left by the previous detection, so the results are unchanged. */
 int bimp_ctx_run_stage(bimp_context* ctx, int stage, void* stream);
+
+/* ---- device memory helpers ------------------------------------------------
+ * For callers (such as the header-only C++ mirror) that do not include the
+ * CUDA runtime: GpuMat::create / release and upload / download
+ * (cv::cuda::GpuMat, used throughout bimp/src/bimp.cpp).  bimp_copy_2d copies
+ * `rows` rows of `width_bytes` between any host or device memory (direction
+ * from the pointers) on `stream` and synchronises it. */
+int bimp_device_alloc(void** ptr, size_t bytes);
+int bimp_device_free(void* ptr);
+int bimp_copy_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width_bytes, size_t rows,
+                 void* stream);
 
 /* downloadKeypoints, bimp/src/utils.cpp:130-150: device 7 x ld matrix with n
  * columns -> host records (synchronous). */

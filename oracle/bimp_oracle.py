@@ -453,9 +453,17 @@ def extract_keypoints(D: np.ndarray, sc: Scale, scale_index: int, p: Params = Pa
 # ---------------------------------------------------------------------------
 # whole pipeline
 # ---------------------------------------------------------------------------
-def run(img_u8: np.ndarray, lambdas, p: Params = Params(), keep_maps: bool = True):
-    """Full BIMP on one uint8 grayscale image: per-scale maps and keypoints."""
-    H, W = img_u8.shape
+def run(img_u8: np.ndarray, lambdas, p: Params = Params(), keep_maps: bool = True, geometry_size=None):
+    """Full BIMP on one uint8 grayscale image: per-scale maps and keypoints.
+
+    geometry_size (W, H), default the image's own: the size the CudaStuff is
+    built for.  The reference's Context builds it from the size of the image
+    before getGPUImage upscales it (bimp/src/bimp.cpp:7-8,
+    bimp/src/cuda_bimp.cu:156-168); each scale then takes the top-left
+    dataW x dataH window of its level of the larger image (convertTo and
+    collectCVMemory, bimp/src/cuda_bimp.cu:481-486), which level_image does.
+    """
+    H, W = img_u8.shape if geometry_size is None else (geometry_size[1], geometry_size[0])
     scales = scale_geometry(W, H, lambdas, p)
     out = []
     for i, sc in enumerate(scales):

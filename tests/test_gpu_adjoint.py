@@ -122,3 +122,51 @@ def test_adjoint_uhd_crop_with_12_scales():
     frame = synth.uhd_frames(1, 1004)[0]
     crop = np.ascontiguousarray(frame[568:1592, 1408:2432]).astype(np.float32) / np.float32(255.0)
     _check(*_run(1024, 1024, 1, synth.bank(12), seed=43, imgs=crop[None]))
+
+
+def test_autograd_wrapper_matches_finite_differences_on_one_linear_piece():
+    """torch.autograd through SummedKeypointMapLoss on two 96x80 images whose
+    content has no exactly flat regions (uint8 content plus U(-0.5, 0.5),
+    / 255): the directional derivative of the GPU gradient along a seeded
+    direction, and the four parameter gradients, against central finite
+    differences of the FP64 loss.  The steps (1e-7 along a unit-variance
+    direction on the image, 1e-6 on the parameters) keep every ReLU argument
+    on its side, so the differences see one linear piece (on the FP64
+    reference they match its gradient to about 1e-8; at 1e-6 on the image
+    they already cross kinks); tolerance 1e-3 relative."""
+    import torch
+    from bimp_b200.autograd import summed_map_loss, summed_map_theta
+    w, h, n = 96, 80, 2
+    lam = [4.0, 5.656854, 8.0]
+    imgs = np.stack([synth.dequantised(synth.synth_image(w, h, 4, seed=60 + i), seed=70 + i) for i in range(n)])
+    adj = api.Adjoint(w, h, n, lam)
+    rng = np.random.default_rng(8)
+    masks = rng.standard_normal(n * adj.mask_stride).astype(np.float32)
+    x = torch.from_numpy(imgs).cuda().requires_grad_(True)
+    theta = summed_map_theta(adj)
+    loss = summed_map_loss(x, theta, torch.from_numpy(masks).cuda(), adj)
+    gx, gth = torch.autograd.grad(loss, [x, theta])
+    gx = gx.cpu().numpy().astype(np.float64)
+    gth = gth.cpu().numpy()
+    views = [[masks[i * adj.mask_stride + off:i * adj.mask_stride + off + ww * hh].reshape(hh, ww).astype(np.float64)
+              for (off, ww, hh) in adj.layout] for i in range(n)]
+    adj.close()
+    X = imgs.astype(np.float64)
+
+    def L(Xs, th=A.Theta()):
+        return sum(A.loss(Xs[i], lam, views[i], th) for i in range(n))
+
+    v = np.random.default_rng(12).standard_normal(X.shape)
+    hx = 1e-7
+    fd = (L(X + hx * v) - L(X - hx * v)) / (2 * hx)
+    dd = float((gx * v).sum())
+    print("directional derivative: gpu", dd, "finite difference", fd)
+    assert abs(dd - fd) <= 1e-3 * abs(fd)
+    base = A.Theta()
+    for k, name in enumerate(("alpha", "rho", "w_tan", "w_rad")):
+        hp = 1e-6
+        up = A.Theta(**{**base.__dict__, name: getattr(base, name) + hp})
+        dn = A.Theta(**{**base.__dict__, name: getattr(base, name) - hp})
+        fdp = (L(X, up) - L(X, dn)) / (2 * hp)
+        print(name, "gpu", gth[k], "finite difference", fdp)
+        assert abs(gth[k] - fdp) <= 1e-3 * abs(fdp) + 1e-9

@@ -308,26 +308,66 @@ def test_persistent_tile_loop_matches(monkeypatch):
         assert np.array_equal(d_ref[i], cs2.dense_map(i).cpu().numpy())
 
 
-def test_cpp_context_shim_matches_python_api(tmp_path):
-    """bimp::Context (include/bimp/bimp.hpp) from a C++ program: the same
-    keypoints as the Python path through the C ABI."""
+def _shim_image(w, h, cn, seed):
+    grey = synth.synth_image(w, h, max(3, w * h // 15000), seed=seed)
+    if cn == 1:
+        return grey
+    rng = np.random.default_rng(seed)
+    return np.ascontiguousarray(np.stack([grey, np.roll(grey, 7, 1), rng.integers(0, 256, grey.shape, dtype=np.uint8)],
+                                         -1))
+
+
+@pytest.mark.parametrize("w,h,cn", [(640, 480, 1), (640, 480, 3), (300, 200, 3), (200, 500, 1)])
+def test_cpp_context_shim_matches_python_api(tmp_path, w, h, cn):
+    """bimp::Context (include/bimp/bimp.hpp) from a C++ program, on grey and
+    BGR images, including images below 350 pixels (getGPUImage upscales them
+    and the context's geometry stays that of the original size, as in the
+    reference): the device keypoint matrix, the responses and the colour
+    histograms equal the Python mirror's, whose keypoints and maps match the
+    FP64 oracle run on the same upscaled image with the original geometry."""
     import subprocess
     from test_capi_cpu import _build_shim_demo
     exe = _build_shim_demo()
-    imgs, lam = synth.workload("vga")
-    img = imgs[0]
+    img = _shim_image(w, h, cn, seed=w + 3 * h + cn)
+    lam = [4.0, 5.656854, 8.0, 16.0]
     raw = tmp_path / "img.raw"
-    raw.write_bytes(np.ascontiguousarray(img).tobytes())
-    res = subprocess.run([str(exe), str(img.shape[1]), str(img.shape[0]), str(raw)] + [repr(x) for x in lam],
+    raw.write_bytes(img.tobytes())
+    res = subprocess.run([str(exe), str(w), str(h), str(cn), str(raw)] + [repr(x) for x in lam],
                          check=True, capture_output=True, text=True)
-    rows = [ln.split() for ln in res.stdout.splitlines()]
-    cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
-    ref = api.keypoint_matrix_to_records(api.getKeypoints(img, cs, capacity=200000))
-    assert len(rows) == len(ref) > 0
-    got = np.array([[float(r[0]), float(r[1]), float(r[2])] for r in rows], dtype=np.float32)
+    lines = [ln.split() for ln in res.stdout.splitlines()]
+    kps = [ln[1:] for ln in lines if ln[0] == "kp"]
+    ctx_line = next(ln for ln in lines if ln[0] == "ctx")
+    resp = [ln for ln in lines if ln[0] == "resp"]
+    ctx = api.Context(img, lambdas=lam)
+    uw, uh = api.min_size_dims(w, h)
+    assert (int(ctx_line[1]), int(ctx_line[2])) == (ctx.width(), ctx.height()) == (uw, uh)
+    ref = api.keypoint_matrix_to_records(ctx.getKeypoints())
+    assert int(ctx_line[3]) == len(ref) == len(kps) > 0
+    got = np.array([[float(r[0]), float(r[1]), float(r[2]), float(r[3])] for r in kps], dtype=np.float32)
     assert np.array_equal(got[:, 0], ref["x"]) and np.array_equal(got[:, 1], ref["y"])
-    assert np.array_equal(got[:, 2], ref["size"])
-    assert all(int(r[5]) == 1 and float(r[6]) == -1.0 for r in rows)
+    assert np.array_equal(got[:, 2], ref["size"]) and np.array_equal(got[:, 3], ref["response"])
+    assert all(int(r[5]) == 1 and float(r[6]) == -1.0 for r in kps)
+    py_resp = ctx.getResponses()
+    assert len(resp) == len(py_resp) == len(lam)
+    for ln, r in zip(resp, py_resp):
+        D = r["D"].cpu().numpy().astype(np.float64)
+        S = r["S"].cpu().numpy().astype(np.float64)
+        assert (int(ln[2]), int(ln[3])) == (r["data_w"], r["data_h"])
+        assert float(ln[4]) == np.float32(D.max())
+        assert abs(float(ln[5]) - D.sum()) <= 1e-6 * np.abs(D).sum()
+        assert abs(float(ln[6]) - S.sum()) <= 1e-6 * np.abs(S).sum()
+    if cn == 3:
+        col = next(ln for ln in lines if ln[0] == "color")
+        feats = ctx.getColorFeatures()
+        assert int(col[1]) == len(ref) == feats.shape[0]
+        s_py = float(np.sum(feats, dtype=np.float64))
+        assert (np.isnan(s_py) and col[2] == "nan") or abs(float(col[2]) - s_py) <= 1e-6 * abs(s_py)
+    # the Python mirror against the FP64 oracle on the same upscaled image
+    grey = O.gpu_image(img, grayscale=True)
+    res_o = O.run(grey, lam, geometry_size=(w, h))
+    for i, r in enumerate(res_o):
+        assert peak_rel_error(ctx.cuda_data.dense_map(i, 0).cpu().numpy(), r["D"]) <= MAP_TOL
+    _check_keypoints(ref, res_o)
 
 
 @pytest.mark.parametrize("w,h,cn", [(300, 120, 3), (640, 480, 3), (200, 500, 1), (123, 77, 3)])
@@ -432,3 +472,41 @@ def test_async_detection_captured_in_a_caller_graph():
     torch.cuda.synchronize()
     assert torch.equal(other[:, :n_ref], ref[:, :n_ref])
     del g
+
+
+@pytest.mark.parametrize("depth", [1, 3])
+def test_pipeline_matches_detect_host(depth):
+    """bimp_pipeline_*: frames pushed ahead of their pops give the same
+    records as bimp_detect_host one by one, including frames with no
+    keypoints, a count far above the previous frame's (the records beyond the
+    speculative copy) and a capacity overflow on pop."""
+    imgs, lam = synth.workload("vga")
+    base = imgs[0]
+    seq = [base, np.full_like(base, 128), base[:, ::-1].copy(), np.full_like(base, 9), base[::-1].copy(), base,
+           base[:, ::-1].copy()]
+    cs = api.CudaStuff(640, 480, lam)
+    refs = [api.detect_host(cs, im, capacity=100000) for im in seq]
+    pl = api.Pipeline(640, 480, lam, depth=depth, capacity=100000)
+    got = []
+    for im in seq:
+        if pl.in_flight() == depth:
+            got.append(pl.pop())
+        pl.push(im)
+    while pl.in_flight():
+        got.append(pl.pop())
+    assert len(got) == len(seq)
+    for (r, n, rc), (g, m, rc2) in zip(refs, got):
+        assert rc == rc2 == 0 and n == m and np.array_equal(r, g)
+    # a full pipeline refuses another frame
+    for im in seq[:depth]:
+        pl.push(im)
+    import ctypes as C
+    from bimp_b200 import _lib as L
+    assert L.lib().bimp_pipeline_push(pl._h, C.c_void_p(base.ctypes.data), 640, 640, 480) == L.BIMP_ERR_INVALID
+    # capacity overflow on pop: the first records and the true total
+    rec, n, rc = pl.pop(capacity=100)
+    assert rc == L.BIMP_ERR_CAPACITY and n == refs[0][1] and np.array_equal(rec, refs[0][0][:100])
+    while pl.in_flight():
+        pl.pop()
+    pl.close()
+    cs.close()
