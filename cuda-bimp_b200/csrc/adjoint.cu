@@ -1,10 +1,17 @@
 // Host side of the adjoint (include/bimp_b200_adjoint.h): one arena holding
-// the float pyramid, saved responses, maps and gradients of n equally sized
+// the float pyramid, maps, ReLU states and gradients of n equally sized
 // images, and the launch sequences of the forward and backward.
+//
+// Nothing of the responses survives the forward: the backward recomputes each
+// tile's spectrum and e + i o.  The per-cell scratch (complex cells C and
+// their gradient, the inhibition maps T and R) exists for a chunk of images
+// at a time; the forward and the backward walk the chunks in order, and the
+// entries of images in different chunks share the same scratch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -80,7 +87,11 @@ struct bimp_adjoint {
   float* d_M = nullptr;
   size_t maskStride = 0;
   std::vector<size_t> maskOff;
-  float2* d_xsave = nullptr;              // per work item: the tile image spectrum of the last forward
+  float2* d_xscr = nullptr;               // per tile-backward CTA: the tile's image spectrum (Hermitian half)
+  int bwdGrid = 0;                        // CTAs of the tile backward
+  int chunk = 0;                          // images per chunk of the per-cell scratch
+  bool pipelined = false;                 // the warp-specialised forward tile kernel fits every scale
+  std::vector<int> tileStart, stenStart, stenBStart;   // per image (n + 1 entries)
   double* d_loss = nullptr;               // [0] loss, [1..4] parameter gradients
   double* d_gp = nullptr;
   unsigned int* d_max = nullptr;          // per entry + fault word
@@ -138,8 +149,39 @@ struct bimp_adjoint {
     std::vector<TileWork> tiles;
     std::vector<int2> sten, stenB;
     std::vector<ScaleDev> sds;
-    std::vector<size_t> offC, offZ, offD, offT, offR, offBits, offGC, offGW;
+    std::vector<size_t> offD, offBits;                  // per entry
+    std::vector<size_t> offC, offT, offR, offGC, offGW;  // per (chunk slot, scale)
+    // images per chunk: all of them while their per-cell scratch stays under
+    // kChunkBudget (BIMP_ADJOINT_CHUNK overrides it, for tests)
+    {
+      size_t per = 0;
+      for (const ScaleHost& sc : geo) {
+        const size_t cStride = (size_t)(sc.dataH + 2) * up(sc.dataW + 1, 32);
+        per += 2 * sizeof(float) * kNumOri * cStride + sizeof(float) * kNumOri * (sc.dataH + 1) +
+               2 * sizeof(float) * (size_t)sc.dataH * up(sc.dataW, 32);
+      }
+      constexpr size_t kChunkBudget = size_t(8) << 30;
+      chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(n, kChunkBudget / std::max<size_t>(per, 1))));
+      if (const char* e = std::getenv("BIMP_ADJOINT_CHUNK")) {
+        const int c = std::atoi(e);
+        if (c > 0) chunk = std::min(c, n);
+      }
+    }
+    for (int k = 0; k < chunk; ++k) {
+      for (const ScaleHost& sc : geo) {
+        const size_t cStride = (size_t)(sc.dataH + 2) * up(sc.dataW + 1, 32);
+        const size_t mapB = sizeof(float) * (size_t)sc.dataH * up(sc.dataW, 32);
+        offC.push_back(take(sizeof(float) * kNumOri * cStride));
+        offGC.push_back(take(sizeof(float) * kNumOri * cStride));
+        offGW.push_back(take(sizeof(float) * kNumOri * (sc.dataH + 1)));
+        offT.push_back(take(mapB));
+        offR.push_back(take(mapB));
+      }
+    }
     for (int i = 0; i < n; ++i) {
+      tileStart.push_back(static_cast<int>(tiles.size()));
+      stenStart.push_back(static_cast<int>(sten.size()));
+      stenBStart.push_back(static_cast<int>(stenB.size()));
       for (int si = 0; si < nScales; ++si) {
         const ScaleHost& s = geo[si];
         ScaleDev d;
@@ -187,17 +229,14 @@ struct bimp_adjoint {
         const int nbx2 = (s.dataW + 1 + 31) / 32, nby2 = (s.dataH + 2 + 31) / 32;   // window + row dataH + 1
         for (int b = 0; b < nbx2 * nby2; ++b) stenB.push_back(make_int2(entry, b));
         const size_t mapB = sizeof(float) * (size_t)s.dataH * d.dPitch;
-        offC.push_back(take(sizeof(float) * (size_t)kNumOri * d.cStride));
-        offZ.push_back(take(sizeof(float2) * (size_t)kNumOri * d.cStride));
-        offGC.push_back(take(sizeof(float) * (size_t)kNumOri * d.cStride));
-        offGW.push_back(take(sizeof(float) * (size_t)kNumOri * (s.dataH + 1)));
         offD.push_back(take(mapB));
-        offT.push_back(take(mapB));
-        offR.push_back(take(mapB));
         offBits.push_back(take(mapB));
         sds.push_back(d);
       }
     }
+    tileStart.push_back(static_cast<int>(tiles.size()));
+    stenStart.push_back(static_cast<int>(sten.size()));
+    stenBStart.push_back(static_cast<int>(stenB.size()));
     nTiles = static_cast<int>(tiles.size());
     nSten = static_cast<int>(sten.size());
     nStenB = static_cast<int>(stenB.size());
@@ -207,7 +246,8 @@ struct bimp_adjoint {
     const size_t offStB = take(sizeof(int2) * stenB.size());
     const size_t offPyr = take(sizeof(PyrJobF) * std::max(1, maxLevel * n));
     const size_t offPyrA = take(sizeof(PyrJobF) * std::max(1, maxLevel * n));
-    const size_t offXs = take(sizeof(float2) * (size_t)nTiles * kSpecHalf);
+    bwdGrid = std::max(1, std::min(nTiles, num_sms()));
+    const size_t offXs = take(sizeof(float2) * (size_t)bwdGrid * kSpecHalf);
     const size_t offLoss = take(sizeof(double) * 8);
     const size_t offMax = take(sizeof(unsigned int) * (sds.size() + 1));
     const size_t offMaps = take(kTensorMapBytes * sds.size());
@@ -240,13 +280,14 @@ struct bimp_adjoint {
       d.G = dG + (size_t)si * kNumOri * kSpecFloats;
       d.bwA = dBA + (size_t)si * kNumOri * kSpecHalf;
       d.bwB = dBB + (size_t)si * kNumOri * kSpecHalf;
-      d.C = reinterpret_cast<float*>(b + offC[e2]);
-      d.Z = reinterpret_cast<float2*>(b + offZ[e2]);
-      d.gC = reinterpret_cast<float*>(b + offGC[e2]);
-      d.gWrap = reinterpret_cast<float*>(b + offGW[e2]);
+      const size_t slot = (size_t)(i % chunk) * nScales + si;   // chunk scratch shared across chunks
+      d.C = reinterpret_cast<float*>(b + offC[slot]);
+      d.Z = nullptr;
+      d.gC = reinterpret_cast<float*>(b + offGC[slot]);
+      d.gWrap = reinterpret_cast<float*>(b + offGW[slot]);
+      d.T = reinterpret_cast<float*>(b + offT[slot]);
+      d.R = reinterpret_cast<float*>(b + offR[slot]);
       d.D = reinterpret_cast<float*>(b + offD[e2]);
-      d.T = reinterpret_cast<float*>(b + offT[e2]);
-      d.R = reinterpret_cast<float*>(b + offR[e2]);
       d.bits = reinterpret_cast<unsigned int*>(b + offBits[e2]);
       d.M = d_M + (size_t)i * maskStride + maskOff[si];
       d.maxKey = d_max + e2;
@@ -259,13 +300,17 @@ struct bimp_adjoint {
       for (size_t e2 = 0; e2 < sds.size(); ++e2) sds[e2].cMap = b + offMaps + e2 * kTensorMapBytes;
     }
     h_sd = sds;
+    pipelined = true;
+    for (const ScaleDev& d : sds) pipelined = pipelined && d.V <= pipelined_tile_max_valid();
+    if (const char* k = std::getenv("BIMP_TILE_KERNEL"))
+      if (std::strcmp(k, "phased") == 0) pipelined = false;
     d_sd = reinterpret_cast<ScaleDev*>(b + offSd);
     d_tiles = reinterpret_cast<TileWork*>(b + offT2);
     d_sten = reinterpret_cast<int2*>(b + offSt);
     d_stenB = reinterpret_cast<int2*>(b + offStB);
     d_pyr = reinterpret_cast<PyrJobF*>(b + offPyr);
     d_pyrAdj = reinterpret_cast<PyrJobF*>(b + offPyrA);
-    d_xsave = reinterpret_cast<float2*>(b + offXs);
+    d_xscr = reinterpret_cast<float2*>(b + offXs);
     d_loss = reinterpret_cast<double*>(b + offLoss);
     d_gp = d_loss + 1;
     // uploads
@@ -310,9 +355,13 @@ struct bimp_adjoint {
     for (int l = 1; l <= maxLevel; ++l) launch_pyr_f(d_pyr + (l - 1) * n, n, lw[l], lh[l], s);
     ADJ_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int) * (h_sd.size() + 1), s));
     ADJ_CUDA(cudaMemsetAsync(d_loss, 0, sizeof(double) * 5, s));
-    launch_gabor_save(d_sd, d_tiles, nTiles, nTiles, d_max + h_sd.size(), d_xsave, s);
-    launch_stencil(d_sd, d_sten, nSten, d_max + h_sd.size(), s, kStencilAdj);
-    launch_masked_loss(d_sd, d_sten, nSten, d_loss, d_gp, s);
+    unsigned int* fault = d_max + h_sd.size();
+    for (int i0 = 0; i0 < n; i0 += chunk) {
+      const int i1 = std::min(n, i0 + chunk);
+      launch_gabor_flt(d_sd, d_tiles + tileStart[i0], tileStart[i1] - tileStart[i0], fault, s, pipelined);
+      launch_stencil(d_sd, d_sten + stenStart[i0], stenStart[i1] - stenStart[i0], fault, s, kStencilAdj);
+      launch_masked_loss(d_sd, d_sten + stenStart[i0], stenStart[i1] - stenStart[i0], d_loss, d_gp, s);
+    }
     if (loss) ADJ_CUDA(cudaMemcpyAsync(loss, d_loss, sizeof(double), cudaMemcpyDeviceToDevice, s));
     ADJ_CUDA(cudaGetLastError());
     return BIMP_OK;
@@ -323,8 +372,11 @@ struct bimp_adjoint {
   int backward(float* grad, size_t pitch, double* gparams, cudaStream_t s) {
     ADJ_CUDA(cudaMemsetAsync(d_glvl, 0, glvlBytes, s));
     ADJ_CUDA(cudaMemsetAsync(d_gp, 0, sizeof(double) * 2, s));
-    launch_stencil_bwd(d_sd, d_stenB, nStenB, s);
-    launch_gabor_bwd(d_sd, d_tiles, nTiles, nTiles, d_xsave, d_gp, s);
+    for (int i0 = 0; i0 < n; i0 += chunk) {
+      const int i1 = std::min(n, i0 + chunk);
+      launch_stencil_bwd(d_sd, d_stenB + stenBStart[i0], stenBStart[i1] - stenBStart[i0], s);
+      launch_gabor_bwd(d_sd, d_tiles + tileStart[i0], tileStart[i1] - tileStart[i0], bwdGrid, d_xscr, d_gp, s);
+    }
     for (int l = maxLevel; l >= 1; --l) launch_pyr_f_adj(d_pyrAdj + (l - 1) * n, n, lw[l], lh[l], s);
     ADJ_CUDA(cudaMemcpy2DAsync(grad, sizeof(float) * pitch, d_glvl, sizeof(float) * lp[0], sizeof(float) * W,
                                (size_t)n * H, cudaMemcpyDeviceToDevice, s));
@@ -413,6 +465,10 @@ int bimp_adjoint_complex_map(bimp_adjoint* a, int image, int scale, int orientat
     return afail(BIMP_ERR_INVALID, "bad complex-map arguments");
   const ScaleDev& d = a->h_sd[(size_t)image * a->nScales + scale];
   if (ld < (size_t)d.cCols) return afail(BIMP_ERR_INVALID, "ld smaller than data width + 1");
+  // the complex cells survive the forward only for the images of its last chunk
+  if (image < (a->n - 1) / a->chunk * a->chunk)
+    return afail(BIMP_ERR_UNSUPPORTED, "complex cells of image " + std::to_string(image) +
+                                           " were overwritten by a later chunk of the forward");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float* src = d.C + (size_t)orientation * d.cStride;
   ADJ_CUDA(cudaMemcpy2DAsync(d_out, ld * sizeof(float), src, d.cPitch * sizeof(float), d.cCols * sizeof(float),

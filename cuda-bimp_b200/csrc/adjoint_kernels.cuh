@@ -9,12 +9,13 @@
 //                       fftW == dataW, window column dataW is the torus
 //                       element (r+1, 0): its gradient is kept aside and
 //                       added there by the tile backward)
-//   k_gabor_tiles_bwd   per tile and orientation a = dL/dC * z/|z|, A = FFT(a),
-//                       alpha/rho dot products sum dG Re(conj(A) X) with the
-//                       image spectrum X the forward saved, and the sum of
-//                       A G in the frequency domain; one inverse transform
-//                       per tile gives the window gradient, scattered to
-//                       the level
+//   k_gabor_tiles_bwd   per tile: the image spectrum X and, per orientation,
+//                       z = e + i o recomputed as the forward computes them
+//                       (nothing of the forward's responses is stored);
+//                       a = dL/dC * z/|z|, A = FFT(a), alpha/rho dot products
+//                       sum dG Re(conj(A) X), and the sum of A G in the
+//                       frequency domain; one inverse transform per tile
+//                       gives the window gradient, scattered to the level
 #pragma once
 
 __global__ void k_pyr_down_f(const PyrJobF* __restrict__ jobs) {
@@ -206,24 +207,31 @@ k_stencil_bwd(const ScaleDev* __restrict__ sds, const int2* __restrict__ work) {
 // absolute value for images on the [0, 1] scale.
 constexpr float kMagFloor = 3.0e-5f;
 constexpr int kSmemBh = kSmemXh;   // Hermitian half of the accumulated spectrum
-constexpr int kGaborBwdSmem = kSmemW + kSmemBh + kSmemTw + kSmemMaps;
-static_assert(kGaborBwdSmem <= 232448, "tile backward exceeds the 227 KB shared-memory limit");
 
 // Position of natural frequency k in the digit-permuted order of the 8x16
 // transforms (the order of G and of the saved spectra).
 __device__ __forceinline__ int perm128d(int k) { return 8 * (k & 15) + (k >> 4); }
 
-// One CTA per tile.  The window gradient is linear in the per-orientation
-// spectra, Re IFFT(sum_o A_o G_o), so the products are summed in the
-// frequency domain (Hermitian half, Bh) and ONE inverse transform per tile
-// replaces one per orientation.  Per orientation: a = dL/dC * z/|z| on the
-// valid outputs, A = FFT(a), the alpha/rho dot products sum dG Re(conj(A) X)
-// against the image spectrum X the forward saved (Hermitian half), and
-// Bh += (A G + conj(A G)(-k))/2.  The per-orientation coefficients G(+-k),
-// dGa, dGr come pre-gathered in the half layout (ScaleDev::bwA, bwB).
+// Persistent CTAs walk the tiles (one CTA per SM: 196 KB of shared memory
+// and all 512 TMEM columns).  The window gradient is linear in the
+// per-orientation spectra, Re IFFT(sum_o A_o G_o), so the products are summed
+// in the frequency domain (Hermitian half, Bh) and ONE inverse transform per
+// tile replaces one per orientation.  Nothing of the forward's responses is
+// stored: per tile the image spectrum X is recomputed from the float level
+// (the forward's transform: full spectrum into TMEM, Hermitian half into this
+// CTA's slot of `xscratch`), and per orientation e + i o is recomputed on the
+// valid outputs by the forward's inverse passes (G read from L2 instead of
+// staged); then a = dL/dC * z/|z| (0 where |z| <= kMagFloor or outside the
+// valid outputs), A = FFT(a), the alpha/rho dot products
+// sum dG Re(conj(A) X), and Bh += (A G + conj(A G)(-k))/2.  The
+// per-orientation coefficients G(+-k), dGa, dGr come pre-gathered in the
+// half layout (ScaleDev::bwA, bwB).
+constexpr int kGaborBwdSmem = kSmemW + kSmemBh + kSmemTw + kSmemMaps + 16;
+static_assert(kGaborBwdSmem <= 232448, "tile backward exceeds the 227 KB shared-memory limit");
+
 __global__ void __launch_bounds__(kTileThreads, 1)
 k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ work, int nwork,
-                  const float2* __restrict__ xsave, double* __restrict__ gparams) {
+                  float2* __restrict__ xscratch, double* __restrict__ gparams) {
   extern __shared__ float4 smem4b[];
   char* base = reinterpret_cast<char*>(smem4b);
   float2* W = reinterpret_cast<float2*>(base);
@@ -231,11 +239,29 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
   float2* tw = reinterpret_cast<float2*>(base + kSmemW + kSmemBh);
   short* rmap = reinterpret_cast<short*>(base + kSmemW + kSmemBh + kSmemTw);
   short* cmap = rmap + kTile;
+  uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(base + kSmemW + kSmemBh + kSmemTw + kSmemMaps);
+  float2* Xh64 = W + 64 * kTile;   // forward transform only
+  float2* Nyq = Bh;                // forward transform only (Bh is cleared after it)
+  float2* __restrict__ Xs = xscratch + (size_t)blockIdx.x * kSpecHalf;
   const int t = threadIdx.x;
   if (t < 8 * 17) {
     const int n1 = t / 17, k2 = t % 17;
     tw[t] = k2 < 16 ? c_w128[(n1 * k2) & 127] : make_float2(0.f, 0.f);
   }
+  if ((t >> 5) == 0) tmem_alloc_warp(smem_u32(tmemSlot));
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  const uint32_t tlane = *tmemSlot + ((uint32_t)((t >> 5) & 3) << 21);
+  // column p of the full spectrum in the Hermitian half (as the forward)
+  const int pI1 = t & 127, h = t >> 7;
+  const int pa = pI1 >> 3, pb = pI1 & 7;
+  const bool pNyq = pb == 4 && pa == 0;
+  const bool pConj = pb >= 4 && !pNyq;
+  const int pSlot = pb < 4 ? 4 * pa + pb : (pNyq ? 64 : (pa > 0 ? 4 * (16 - pa) + (7 - pb) : 8 - pb));
+  const float pSign = pConj ? -1.f : 1.f;
+  const float2* pSrc = pNyq ? Nyq : Xh64 + pSlot;
+  const int pStride = pNyq ? 1 : 64;
   double accA = 0.0, accR = 0.0;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const TileWork item = work[w];
@@ -243,59 +269,107 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
     const int kX = sd->kX, V = sd->V;
     const int ty = item.tile / sd->tilesX, tx = item.tile - ty * sd->tilesX;
     const int R0 = ty * V, C0 = tx * V;
-    const float2* __restrict__ Xs = xsave + (size_t)w * kSpecHalf;   // Hermitian half of X
     __syncthreads();   // previous tile finished with every buffer
-    if (t < kTile) {
-      rmap[t] = (short)pad_src(pmod(R0 - kX + t, sd->fftH), sd->dataH, kX);
-    } else if (t < 2 * kTile) {
-      const int i = t - kTile;
-      cmap[i] = (short)pad_src(pmod(C0 - kX + i, sd->fftW), sd->dataW, kX);
+    tile_forward_spectrum<true>(sd, R0, C0, W, Xh64, Nyq, tw, rmap, cmap, t);
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+      const int k2 = h + 4 * q;
+      float2 x[8];
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) {
+        const int row = pConj ? (k2 > 0 ? 8 * (16 - k2) + (7 - k1) : (8 - k1) & 7) : 8 * k2 + k1;
+        x[k1] = pSrc[row * pStride];
+        x[k1].y *= pSign;
+      }
+      tmem_store8(tlane + 16 * k2, x);
     }
+    for (int j = t; j < kSpecHalf; j += kTileThreads) {
+      const int r = j / kXhCols, sl = j - r * kXhCols;
+      Xs[j] = *xh_ptr(Xh64, Nyq, r, sl);
+    }
+    tmem_fence_before();
+    __syncthreads();   // the Hermitian half in W / Bh is dead from here
+    tmem_fence_after();
     for (int j = t; j < kTile * kXhCols; j += kTileThreads) Bh[j] = make_float2(0.f, 0.f);
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     const long long cStride = sd->cStride;
     const int wrapW = sd->wrapW;
     for (int o = 0; o < kNumOri; ++o) {
-      // a = dL/dC * z / |z| on the valid outputs, zero elsewhere; four
-      // pixels per thread with their loads issued together
+      const float* __restrict__ Go = sd->G + (size_t)o * kSpecFloats;
+      // I1: y-dim pass B' with the spectrum product X * G_o (TMEM in, TMEM out)
 #pragma unroll 1
-      for (int j0 = t; j0 < kTile * kTile; j0 += 4 * kTileThreads) {
-        float m[4], gc[4];
-        float2 z[4];
-        bool ok[4];
+      for (int q = 0; q < 4; ++q) {
+        const int k2 = h + 4 * q;
+        float2 v[8];
+        tmem_load8(tlane + 16 * k2, v);
+        const float* __restrict__ Gq = Go + (size_t)(8 * k2) * kTile + pI1;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int j = j0 + u * kTileThreads;
-          const int y = j >> 7, x = j & 127;
-          const int gy = R0 + y - kX, gx = C0 + x - kX;
-          ok[u] = y >= kX && y < kX + V && x >= kX && x < kX + V && gy < cRows && gx < cCols;
-          const size_t k = ok[u] ? (size_t)o * cStride + (size_t)gy * cPitch + gx : 0;
-          gc[u] = ok[u] ? __ldg(sd->gC + k) : 0.f;
-          if (ok[u] && wrapW && gx == 0 && gy >= 1) gc[u] += __ldg(sd->gWrap + o * (sd->dataH + 1) + gy - 1);
-          z[u] = ok[u] ? __ldg(sd->Z + k) : make_float2(0.f, 0.f);
-        }
-        // |z| as the forward computed it (the forward stored C = cmag(z)),
-        // recomputed instead of read back
+        for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], __ldg(Gq + k1 * kTile));
+        dft8<true>(v);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) m[u] = ok[u] ? cmag(z[u]) : 0.f;
+        for (int n1 = 0; n1 < 8; ++n1)
+          tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0]);
+      }
+      tmem_wait_st();
+      tmem_fence_before();
+      __syncthreads();   // the y-pass output is complete; no thread still reads W
+      tmem_fence_after();
+      // I2: y-dim pass A' -> natural y; rows outside the valid band are zero
+      // (a is zero there, and the transform of a below reads every row)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int j = j0 + u * kTileThreads;
-          float2 a = make_float2(0.f, 0.f);
-          if (ok[u] && m[u] > kMagFloor) {
-            const float sc = gc[u] / m[u];
-            a = make_float2(sc * z[u].x, sc * z[u].y);
-          }
-          W[widx(j >> 7, j & 127)] = a;
+      for (int it = 0; it < 2; ++it) {
+        const int j = t + it * kTileThreads;
+        const int p = j & 127, n1 = j >> 7;
+        float2 v[16];
+        tmem_load16(tlane + kTmemY + 32 * n1, v);
+        dft16<true>(v);
+#pragma unroll
+        for (int n2 = 0; n2 < 16; ++n2) {
+          const int y = n1 + 8 * n2;
+          W[widx(y, p)] = (y >= kX && y < kX + V) ? v[n2] : make_float2(0.f, 0.f);
         }
       }
+      tmem_fence_before();
       __syncthreads();
-      // forward FFT of a: x-dim on the valid rows (the others are zero), then y-dim
+      tmem_fence_after();
+      // I3: x-dim pass B' on the valid rows
+      for (int j = t; j < V * 16; j += kTileThreads) {
+        const int y = kX + (j >> 4), k2 = j & 15;
+        float2 v[8];
+#pragma unroll
+        for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
+        dft8<true>(v);
+#pragma unroll
+        for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0];
+      }
+      __syncthreads();
+      // I4 + the first pass of FFT(a): x-dim pass A' gives z = e + i o at the
+      // row's outputs x = n1 + 8 n2; a = dL/dC * z/|z| on the valid outputs
+      // (|z| as the forward computed it); then the forward x-dim pass A of a
+      // on the same 16 elements, in registers
       for (int j = t; j < V * 8; j += kTileThreads) {
         const int y = kX + (j >> 3), n1 = j & 7;
         float2 v[16];
 #pragma unroll
-        for (int m = 0; m < 16; ++m) v[m] = W[widx(y, n1 + 8 * m)];
+        for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(y, 8 * k2 + n1)];
+        dft16<true>(v);
+        const int gy = R0 + y - kX;
+#pragma unroll
+        for (int n2 = 0; n2 < 16; ++n2) {
+          const int x = n1 + 8 * n2;
+          const int gx = C0 + x - kX;
+          float2 a = make_float2(0.f, 0.f);
+          if (x >= kX && x < kX + V && gy < cRows && gx < cCols) {
+            float gc = __ldg(sd->gC + (size_t)o * cStride + (size_t)gy * cPitch + gx);
+            if (wrapW && gx == 0 && gy >= 1) gc += __ldg(sd->gWrap + o * (sd->dataH + 1) + gy - 1);
+            const float m = cmag(v[n2]);
+            if (m > kMagFloor) {
+              const float sc = gc / m;
+              a = make_float2(sc * v[n2].x, sc * v[n2].y);
+            }
+          }
+          v[n2] = a;
+        }
         dft16<false>(v);
 #pragma unroll
         for (int k2 = 0; k2 < 16; ++k2) W[widx(y, n1 + 8 * k2)] = c_mul(v[k2], tw[n1 * 17 + k2]);
@@ -349,7 +423,7 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
           const int j = py * kXhCols + sl;
           const float4 c4 = __ldg(cA + j);   // G(k), G(-k), dGa(k), dGr(k)
           const float2 c2 = __ldg(cB + j);   // dGa(-k), dGr(-k)
-          const float2 X = __ldg(Xs + j);
+          const float2 X = Xs[j];   // written by this CTA for this tile: a coherent load
           const int ky = 16 * (py & 7) + (py >> 3);
           const int npy = perm128d((kTile - ky) & 127);
           const float2 A1 = W[wp], A2 = W[widx(npy, np)];
@@ -383,8 +457,10 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
         accA += sa;
         accR += sr;
       }
-      __syncthreads();
+      // no barrier: every Bh entry has one owner thread, and the next
+      // orientation's I1 touches only TMEM until its barrier
     }
+    __syncthreads();
     // one inverse transform of the Hermitian sum: Re -> window gradient,
     // scattered to the float level through the padded-torus index maps.
     // Column p = t & 127 of the full spectrum is read from the half Bh
@@ -452,6 +528,10 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
       }
     }
   }
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  if ((t >> 5) == 0) tmem_dealloc_warp(*tmemSlot);
   block_add_double(accA, gparams + 0);
   block_add_double(accR, gparams + 1);
 }

@@ -133,6 +133,7 @@ struct Engine {
   float* d_kpInternal = nullptr;
   int kpCapInternal = 0;
   int tileGrid = 0;    // CTAs of the tile kernel (each loops over tiles)
+  bool tilePipelined = false;   // the warp-specialised tile kernel (every scale's V fits its row buffers)
   int tileCap = 0;     // capacity of d_tiles (the largest tile plan)
   int tilePolicy = 0, tileOrder = 0;
 
@@ -183,7 +184,17 @@ struct Engine {
     tileGrid = grid > 0 ? std::min(grid, nTiles) : nTiles;
     tilePolicy = policy;
     tileOrder = order;
+    tilePipelined = pipelined_fits();
     return BIMP_OK;
+  }
+  // The warp-specialised tile kernel takes every scale with V up to its row
+  // buffers' height (BIMP_TILE_KERNEL=phased selects the phased kernel).
+  bool pipelined_fits() const {
+    if (const char* k = std::getenv("BIMP_TILE_KERNEL"))
+      if (std::strcmp(k, "phased") == 0) return false;
+    for (const ScaleDev& d : h_sd)
+      if (d.V > pipelined_tile_max_valid()) return false;
+    return true;
   }
 
   // inW/inH (null: the geometry sizes) are the sizes of the images a
@@ -417,6 +428,7 @@ struct Engine {
       for (size_t e2 = 0; e2 < sds.size(); ++e2) sds[e2].cMap = base + offMaps + e2 * kTensorMapBytes;
     }
     h_sd = sds;
+    tilePipelined = pipelined_fits();
     d_sd = reinterpret_cast<ScaleDev*>(base + offSd);
     d_tiles = reinterpret_cast<TileWork*>(base + offTiles);
     d_sten = reinterpret_cast<int2*>(base + offSten);
@@ -470,7 +482,7 @@ struct Engine {
           launch_pyr(d_pyr + pyrFirst[l], pyrCount[l], pyrLevels[l], pyrMaxW[l], pyrMaxH[l], s);
         break;
       case 1:
-        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s);
+        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s, tilePipelined);
         break;
       case 2:
         if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD);

@@ -507,3 +507,209 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
   tmem_fence_after();
   if ((t >> 5) == 0) tmem_dealloc_warp(*tmemSlot);
 }
+
+// ---------------------------------------------------------------------------
+// k_gabor_tiles_ws: the same tile computation with warp-specialised,
+// pipelined orientations
+// ---------------------------------------------------------------------------
+// After the tile's forward transform (all 16 warps, as above), warps 0-7
+// (group Y) run the spectrum product and the two inverse y-passes of each
+// orientation (TMEM in, TMEM y-area, then the valid rows into a shared-memory
+// row buffer), while warps 8-15 (group X) run the two inverse x-passes and
+// the complex magnitude of the previous orientation from the other buffer.
+// Two row buffers of kWsRows x 128 complex alternate between orientations;
+// named barriers hand them over (full: Y -> X, empty: X -> Y), and each group
+// orders its own passes with a 256-thread named barrier, so no CTA-wide
+// barrier stands inside the orientation loop.  G_o is read from L2 (the
+// space of the TMA ring holds the second buffer).  Needs V <= kWsRows.
+constexpr int kWsRows = 104;                                  // largest V this kernel takes
+constexpr int kWsBuf = kWsRows * kTile;                       // complex per row buffer
+constexpr int kWsSmemW = 2 * kWsBuf * 8;                      // both row buffers (also the forward scratch)
+constexpr int kWsSmem = kWsSmemW + kSmemTw + kSmemMaps + 16;  // + twiddles, index maps, TMEM base slot
+static_assert(kWsSmem <= 232448, "warp-specialised tile kernel exceeds the 227 KB shared-memory limit");
+// forward transform scratch inside the two buffers: packed rows 0..63, the
+// Hermitian half at rows 64..127, the Nyquist slot column at row 192
+static_assert(2 * kWsRows >= 193, "forward-transform scratch does not fit the row buffers");
+constexpr int kWsGroup = kTileThreads / 2;   // threads per group
+enum : int { kBarY = 1, kBarX = 2, kBarFull0 = 3, kBarEmpty0 = 5 };   // named barrier ids (0 is __syncthreads)
+
+__device__ __forceinline__ void nbar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ void nbar_arrive(int id, int n) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+template <bool FLT>
+__global__ void __launch_bounds__(kTileThreads, 1)
+k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ work, int nwork) {
+  extern __shared__ float4 smem4[];
+  char* base = reinterpret_cast<char*>(smem4);
+  float2* Wb = reinterpret_cast<float2*>(base);
+  float2* tw = reinterpret_cast<float2*>(base + kWsSmemW);
+  short* rmap = reinterpret_cast<short*>(base + kWsSmemW + kSmemTw);
+  short* cmap = rmap + kTile;
+  uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(base + kWsSmemW + kSmemTw + kSmemMaps);
+  float2* Xh64 = Wb + 64 * kTile;    // forward transform only
+  float2* Nyq = Wb + 192 * kTile;    // forward transform only
+  const int t = threadIdx.x;
+  if (t < 8 * 17) {
+    const int n1 = t / 17, k2 = t % 17;
+    tw[t] = k2 < 16 ? c_w128[(n1 * k2) & 127] : make_float2(0.f, 0.f);
+  }
+  if ((t >> 5) == 0) tmem_alloc_warp(smem_u32(tmemSlot));
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  const uint32_t tlane = *tmemSlot + ((uint32_t)((t >> 5) & 3) << 21);
+  // spectrum store (all warps): column p of the full spectrum in the half
+  const int pI1 = t & 127, h4 = t >> 7;
+  const int pa = pI1 >> 3, pb = pI1 & 7;
+  const bool pNyq = pb == 4 && pa == 0;
+  const bool pConj = pb >= 4 && !pNyq;
+  const int pSlot = pb < 4 ? 4 * pa + pb : (pNyq ? 64 : (pa > 0 ? 4 * (16 - pa) + (7 - pb) : 8 - pb));
+  const float pSign = pConj ? -1.f : 1.f;
+  const float2* pSrc = pNyq ? Nyq : Xh64 + pSlot;
+  const int pStride = pNyq ? 1 : 64;
+  const bool groupY = t < kWsGroup;
+  const int tg = t & (kWsGroup - 1);   // index within the group
+  const int hY = tg >> 7;              // group Y: spectrum rows k2 = hY + 2 q
+
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const TileWork item = work[w];
+    const ScaleDev* sd = sds + item.entry;
+    const int kX = sd->kX, V = sd->V;
+    const int ty = item.tile / sd->tilesX, tx = item.tile - ty * sd->tilesX;
+    const int R0 = ty * V, C0 = tx * V;
+    __syncthreads();   // previous tile finished with every buffer
+    tile_forward_spectrum<FLT>(sd, R0, C0, Wb, Xh64, Nyq, tw, rmap, cmap, t);
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+      const int k2 = h4 + 4 * q;
+      float2 x[8];
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) {
+        const int row = pConj ? (k2 > 0 ? 8 * (16 - k2) + (7 - k1) : (8 - k1) & 7) : 8 * k2 + k1;
+        x[k1] = pSrc[row * pStride];
+        x[k1].y *= pSign;
+      }
+      tmem_store8(tlane + 16 * k2, x);
+    }
+    tmem_fence_before();
+    __syncthreads();   // spectrum in TMEM; the forward scratch in the row buffers is dead
+    tmem_fence_after();
+    if (groupY) {
+      for (int o = 0; o < kNumOri; ++o) {
+        const int b = o & 1;
+        float2* Wo = Wb + b * kWsBuf;
+        const float* __restrict__ Go = sd->G + (size_t)o * kSpecFloats;
+        // I1: y-dim pass B' with the spectrum product (TMEM in, TMEM y-area out)
+#pragma unroll 1
+        for (int q = 0; q < 8; ++q) {
+          const int k2 = hY + 2 * q;
+          float2 v[8];
+          const float* __restrict__ Gq = Go + (size_t)(8 * k2) * kTile + pI1;
+          float g[8];
+#pragma unroll
+          for (int k1 = 0; k1 < 8; ++k1) g[k1] = __ldg(Gq + k1 * kTile);
+          tmem_load8(tlane + 16 * k2, v);
+#pragma unroll
+          for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], g[k1]);
+          dft8<true>(v);
+#pragma unroll
+          for (int n1 = 0; n1 < 8; ++n1)
+            tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0]);
+        }
+        tmem_wait_st();
+        tmem_fence_before();
+        nbar_sync(kBarY, kWsGroup);   // the y-area holds orientation o's first y-pass
+        tmem_fence_after();
+        if (o >= 2) nbar_sync(kBarEmpty0 + b, kTileThreads);   // group X is done with orientation o - 2
+        // I2: y-dim pass A' -> natural y; the valid rows into buffer b
+#pragma unroll
+        for (int it = 0; it < 4; ++it) {
+          const int j = tg + it * kWsGroup;
+          const int p = j & 127, n1 = j >> 7;
+          float2 v[16];
+          tmem_load16(tlane + kTmemY + 32 * n1, v);
+          dft16<true>(v);
+#pragma unroll
+          for (int n2 = 0; n2 < 16; ++n2) {
+            const int y = n1 + 8 * n2 - kX;
+            if (y >= 0 && y < V) Wo[widx(y, p)] = v[n2];
+          }
+        }
+        tmem_fence_before();
+        nbar_arrive(kBarFull0 + b, kTileThreads);   // buffer b holds orientation o
+        nbar_sync(kBarY, kWsGroup);                 // every thread is done reading the y-area
+        tmem_fence_after();
+      }
+    } else {
+      const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
+      const bool wrapTile = sd->wrapW != 0 && (C0 == 0 || C0 + V >= cCols);
+      const int xHi = min(kX + V, cCols - C0 + kX);
+      // I4 keeps column group n1 = tg mod 8 for the whole tile
+      unsigned int xMask = 0;
+#pragma unroll
+      for (int n2 = 0; n2 < 16; ++n2) {
+        const int x = (tg & 7) + 8 * n2;
+        xMask |= (x >= kX && x < xHi ? 1u : 0u) << n2;
+      }
+      float* __restrict__ C0p = sd->C;
+      const long long cStride = sd->cStride;
+      for (int o = 0; o < kNumOri; ++o) {
+        const int b = o & 1;
+        float2* Wo = Wb + b * kWsBuf;
+        float* __restrict__ Cout = C0p + (size_t)o * cStride;
+        nbar_sync(kBarFull0 + b, kTileThreads);
+        // I3: x-dim pass B' on the V rows of the buffer
+        for (int j = tg; j < V * 16; j += kWsGroup) {
+          const int y = j >> 4, k2 = j & 15;
+          float2 v[8];
+#pragma unroll
+          for (int k1 = 0; k1 < 8; ++k1) v[k1] = Wo[widx(y, 8 * k2 + k1)];
+          dft8<true>(v);
+#pragma unroll
+          for (int n1 = 0; n1 < 8; ++n1) Wo[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0];
+        }
+        nbar_sync(kBarX, kWsGroup);
+        // I4: x-dim pass A' -> natural x; complex magnitude of valid outputs
+        for (int j = tg; j < V * 8; j += kWsGroup) {
+          const int y = j >> 3, n1 = j & 7;
+          float2 v[16];
+#pragma unroll
+          for (int k2 = 0; k2 < 16; ++k2) v[k2] = Wo[widx(y, 8 * k2 + n1)];
+          dft16<true>(v);
+          const int gy = R0 + y;
+          if (gy < cRows) {
+            float* dst = Cout + (size_t)gy * cPitch;
+            if (!wrapTile) {
+              float* dstx = dst + (C0 - kX);
+#pragma unroll
+              for (int n2 = 0; n2 < 16; ++n2)
+                if ((xMask >> n2) & 1u) dstx[n1 + 8 * n2] = cmag(v[n2]);
+            } else {
+              // fftW == dataW: window column dataW of row r is the torus
+              // element (r + 1, 0) (see k_gabor_tiles)
+#pragma unroll
+              for (int n2 = 0; n2 < 16; ++n2) {
+                const int x = n1 + 8 * n2;
+                const int gx = C0 + x - kX;
+                if (x >= kX && x < kX + V && gx < cCols) {
+                  const float m = cmag(v[n2]);
+                  if (!(gx == cCols - 1 && gy < cRows - 1)) dst[gx] = m;
+                  if (gx == 0 && gy >= 1) Cout[(size_t)(gy - 1) * cPitch + cCols - 1] = m;
+                }
+              }
+            }
+          }
+        }
+        // buffer b may be refilled by orientation o + 2; the last two
+        // orientations are ordered against the next tile by its barrier
+        if (o < kNumOri - 2) nbar_arrive(kBarEmpty0 + b, kTileThreads);
+      }
+    }
+  }
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  if ((t >> 5) == 0) tmem_dealloc_warp(*tmemSlot);
+}

@@ -983,6 +983,7 @@ cudaError_t upload_twiddles() {
 }
 
 size_t gabor_smem_bytes() { return kGaborSmem; }
+int pipelined_tile_max_valid() { return kWsRows; }
 size_t stencil_smem_bytes() { return sizeof(float) * kStBufs * kStBuf + 128; }
 
 namespace {
@@ -1041,12 +1042,14 @@ int num_sms() {
 cudaError_t configure_kernels() {
   const cudaFuncAttribute big = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaFuncSetAttribute(k_gabor_tiles<false, false>, big, (int)gabor_smem_bytes());
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles<true, true>, big, (int)gabor_smem_bytes());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles<true, false>, big, (int)gabor_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles<false, true>, big, (int)gabor_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilD>, big, (int)stencil_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilDS>, big, (int)stencil_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stencil<kStencilAdj>, big, (int)stencil_smem_bytes());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles_bwd, big, (int)kGaborBwdSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles_ws<false>, big, (int)kWsSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gabor_tiles_ws<true>, big, (int)kWsSmem);
   if (e != cudaSuccess) return e;
   return upload_twiddles();
 }
@@ -1066,13 +1069,20 @@ void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH,
   else k_pyr_down<1><<<g, 256, 0, s>>>(d_jobs);
 }
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
-                  cudaStream_t s) {
-  k_gabor_tiles<false, false><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault,
-                                                                              nullptr);
+                  cudaStream_t s, bool pipelined) {
+  if (pipelined)
+    k_gabor_tiles_ws<false><<<grid, kTileThreads, kWsSmem, s>>>(d_sd, d_work, nwork);
+  else
+    k_gabor_tiles<false, false><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault,
+                                                                                nullptr);
 }
-void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
-                       float2* d_xsave, cudaStream_t s) {
-  k_gabor_tiles<true, true><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault, d_xsave);
+void launch_gabor_flt(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
+                      cudaStream_t s, bool pipelined) {
+  if (nwork <= 0) return;
+  if (pipelined)
+    k_gabor_tiles_ws<true><<<nwork, kTileThreads, kWsSmem, s>>>(d_sd, d_work, nwork);
+  else
+    k_gabor_tiles<true, false><<<nwork, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault, nullptr);
 }
 void launch_gabor_keep_z(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
                          cudaStream_t s) {
@@ -1100,10 +1110,11 @@ void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cud
   if (nwork > 0) k_stencil_bwd<<<nwork, kStBwThreads, 0, s>>>(d_sd, d_work);
 }
 
-void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, const float2* d_xsave,
+void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, float2* d_xscratch,
                       double* d_gparams, cudaStream_t s) {
   if (nwork > 0)
-    k_gabor_tiles_bwd<<<grid, kTileThreads, kGaborBwdSmem, s>>>(d_sd, d_work, nwork, d_xsave, d_gparams);
+    k_gabor_tiles_bwd<<<std::min(grid, nwork), kTileThreads, kGaborBwdSmem, s>>>(d_sd, d_work, nwork, d_xscratch,
+                                                                                 d_gparams);
 }
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigned int* d_fault, cudaStream_t s,
                     int mode) {

@@ -51,8 +51,11 @@ size_t stencil_smem_bytes();
 void launch_set_out(KpOut* d, const KpOut& v, cudaStream_t s);
 void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s);
 // d_fault: word that receives 1 if a bounded device wait expired.
+// pipelined: the warp-specialised variant (k_gabor_tiles_ws), for work whose
+// scales all have V <= pipelined_tile_max_valid(); otherwise the phased one
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
-                  cudaStream_t s);
+                  cudaStream_t s, bool pipelined);
+int pipelined_tile_max_valid();
 // One TMA tensor map per scale entry over its complex-cell maps (x: cPitch
 // columns, y: cRows rows, z: the 8 orientations; box 48 x 48 x 8 floats,
 // zero fill outside), written to maps[e] (128-byte CUtensorMap blobs).
@@ -91,11 +94,10 @@ void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_coun
 // differentiable path and its adjoint
 void launch_pyr_f(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
 void launch_pyr_f_adj(const PyrJobF* d_jobs, int njobs, int maxW, int maxH, cudaStream_t s);
-// differentiable forward: also stores e + i o (ScaleDev::Z) and each work
-// item's tile image spectrum (Hermitian half, kSpecHalf float2 at
-// d_xsave + w * kSpecHalf)
-void launch_gabor_save(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
-                       float2* d_xsave, cudaStream_t s);
+// differentiable forward: the tile kernel on the float levels (one CTA per
+// work item)
+void launch_gabor_flt(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
+                      cudaStream_t s, bool pipelined);
 // detection-path tile kernel that also keeps e + i o (ScaleDev::Z) for the
 // line/edge detector; one CTA per work item
 void launch_gabor_keep_z(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
@@ -106,7 +108,9 @@ void launch_detect_le(const ScaleDev* d_sd, int dataW, int dataH, const float* d
 void launch_masked_loss(const ScaleDev* d_sd, const int2* d_work, int nwork, double* d_loss, double* d_gparams,
                         cudaStream_t s);
 void launch_stencil_bwd(const ScaleDev* d_sd, const int2* d_work, int nwork, cudaStream_t s);
-void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, const float2* d_xsave,
+// tile backward, recomputing the responses; `grid` persistent CTAs (at most
+// nwork), d_xscratch holds grid x kSpecHalf float2 (one tile spectrum per CTA)
+void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, float2* d_xscratch,
                       double* d_gparams, cudaStream_t s);
 
 }  // namespace bimp_b200

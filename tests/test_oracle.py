@@ -212,3 +212,33 @@ def test_lines_edges_known_answers():
     t_down = run(255 - step)[2][20:76, 64]
     assert set(np.unique(t_up)) | set(np.unique(t_down)) == {3, 4}
     assert (t_up != t_down).all()
+
+
+def test_oracle_matches_reference_kernels_golden():
+    """The FP64 oracle against outputs of the reference's own BIMP device
+    kernels (bimp/include/detection/cuda_bimp.cuh compiled unmodified, driven
+    in DoFullGPUFiltering's order with cuFFT; fixture made by
+    tests/golden/make_ref_golden.py): summed keypoint maps D and single-stopped
+    maps S within 1e-4 of the map peak, identical keypoint sets outside
+    decision ties, subpixel positions within 2e-3 level pixels.  Case b has
+    fftW == dataW and fftH == dataH, so the stencils' flat reads pass the
+    torus."""
+    from pathlib import Path
+
+    from parity import MAP_TOL, SUBPIX_TOL, compare_keypoints, peak_rel_error
+    g = np.load(Path(__file__).parent / "golden" / "ref_small.npz")
+    for name in ("a", "b"):
+        img = g[f"{name}_image"]
+        lam = [float(x) for x in g[f"{name}_lambdas"]]
+        res = O.run(img, lam)
+        for i, r in enumerate(res):
+            assert peak_rel_error(g[f"{name}_D{i}"], r["D"]) <= MAP_TOL, (name, i)
+            assert peak_rel_error(g[f"{name}_S{i}"], r["S"]) <= MAP_TOL, (name, i)
+        rec = np.zeros(len(g[f"{name}_kp_x"]), dtype=[("x", "f4"), ("y", "f4"), ("size", "f4"), ("response", "f4")])
+        for f in ("x", "y", "size", "response"):
+            rec[f] = g[f"{name}_kp_{f}"]
+        assert len(rec) > 100
+        rep = compare_keypoints(rec, res)
+        assert not rep["missing"] and not rep["extra"], (name, rep["missing"][:5], rep["extra"][:5])
+        assert rep["max_subpix"] <= SUBPIX_TOL and rep["max_resp_rel"] <= MAP_TOL
+        assert (g[f"{name}_kp_class_id"] == 1).all() and (g[f"{name}_kp_angle"] == -1).all()
