@@ -364,7 +364,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         px = sum(w * h for w, h in sizes)
         bt = api.Batch(sizes, lam_b, kp_capacity=65536)
         bt.load(imgs)
-        tune = bt.autotune(reps=3)   # tile plan: valid-block policy, tile order, tile-kernel grid
+        tune = bt.autotune(reps=3)   # tile plan: kernel variant, valid-block policy, tile order, grid
         for _ in range(3):
             bt.run()
         torch.cuda.synchronize()
@@ -402,9 +402,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "plain_value": round(world * kb * px / (ms_p * 1e-3) / 1e6, 2),
                    "ratio": round(ms_p / ms_b, 3), "unit": UNIT, "graph": True,
                    "autotune": {"chosen": tune["chosen"], "plans_timed": len(tune["tried"]),
+                                "kernels_tried": sorted({t["kernel"] for t in tune["tried"]}),
+                                "valid_block_policies_tried": sorted({t["policy"] for t in tune["tried"]}),
                                 "default_plan_ms": next((t["ms"] for t in tune["tried"]
                                                          if t["policy"] == 0 and t["order"] == 0
-                                                         and t["grid"] == t["tiles"]), None)}}
+                                                         and t["grid"] == t["tiles"] and t["kernel"] == 1),
+                                                        None)}}
         for c2 in ctxs:
             c2.close()
         bt.close()
@@ -597,8 +600,9 @@ def run_configs(args):
                                "train_step_mpixel_s": round(32 * 3840 * 2160 / ((f_ms + b_ms) * 1e-3) / 1e6, 1),
                                "device_bytes_arena": adj.device_bytes(),
                                "device_bytes_held": int(held),
-                               "note": "responses (e + i o, |e + i o|) are stored, not recomputed: "
-                                       "all 32 frames fit in HBM"},
+                               "note": "the backward recomputes each tile's spectrum and e + i o (nothing of "
+                                       "the forward's responses is stored); complex cells, their gradient and "
+                                       "the inhibition maps exist for a chunk of frames at a time"},
                    "cpu_baseline_one_frame": cpu(synth.uhd_frames(1, 1004)[0], lam12, 1)}
     adj.close()
     print(json.dumps({"configs": out}), flush=True)

@@ -35,12 +35,12 @@ NUM_ORI = 8
 
 class TilePlan(C.Structure):
     """bimp_tile_plan (include/bimp_b200_batch.h)."""
-    _fields_ = [("policy", C.c_int), ("order", C.c_int), ("grid", C.c_int), ("tiles", C.c_int),
-                ("ms", C.c_float)]
+    _fields_ = [("policy", C.c_int), ("order", C.c_int), ("kernel", C.c_int), ("grid", C.c_int),
+                ("tiles", C.c_int), ("ms", C.c_float)]
 
     def as_dict(self) -> dict:
-        return {"policy": self.policy, "order": self.order, "grid": self.grid, "tiles": self.tiles,
-                "ms": round(float(self.ms), 4)}
+        return {"policy": self.policy, "order": self.order, "kernel": self.kernel, "grid": self.grid,
+                "tiles": self.tiles, "ms": round(float(self.ms), 4)}
 
 
 class Params(C.Structure):
@@ -129,7 +129,7 @@ _PROTOS = [
     ("bimp_batch_num_images", C.c_int, [C.c_void_p]),
     ("bimp_batch_image", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
     ("bimp_batch_run", C.c_int, [C.c_void_p, C.c_void_p]),
-    ("bimp_batch_set_tile_plan", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    ("bimp_batch_set_tile_plan", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("bimp_batch_autotune", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(TilePlan), C.POINTER(TilePlan),
                                       C.c_int, C.POINTER(C.c_int)]),
     ("bimp_batch_counts", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

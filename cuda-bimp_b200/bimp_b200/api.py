@@ -337,6 +337,7 @@ class Context:
         h, w = img.shape[:2]
         self.cuda_data = CudaStuff(w, h, self.lambdas, params, input_size=min_size_dims(w, h))
         self.current_keypoints = None
+        self.capacity = KP_MAX_POINTS   # keypoint limit, as KP_MAX_POINTS (bimp::Context::capacity)
         self.loadImage(img)
 
     def width(self) -> int:
@@ -363,7 +364,7 @@ class Context:
 
     def getKeypoints(self):
         if self.has_changed_keypoints:
-            self.current_keypoints = getKeypoints(self.current_image, self.cuda_data)
+            self.current_keypoints = getKeypoints(self.current_image, self.cuda_data, capacity=self.capacity)
             self.has_changed_keypoints = False
         return self.current_keypoints
 
@@ -492,9 +493,11 @@ class Batch:
     def run(self, stream=None):
         L.check(L.lib().bimp_batch_run(self._h, _stream_ptr(stream)), "batch_run")
 
-    def set_tile_plan(self, policy: int, order: int, grid: int = 0):
-        """Use a tile plan (bimp_batch_set_tile_plan); grid <= 0: one CTA per tile."""
-        L.check(L.lib().bimp_batch_set_tile_plan(self._h, int(policy), int(order), int(grid)), "batch_tile_plan")
+    def set_tile_plan(self, policy: int, order: int, grid: int = 0, kernel: int = 1):
+        """Use a tile plan (bimp_batch_set_tile_plan); grid <= 0: one CTA per
+        tile; kernel 1: warp-specialised tile kernel where it fits, 0: phased."""
+        L.check(L.lib().bimp_batch_set_tile_plan(self._h, int(policy), int(order), int(grid), int(kernel)),
+                "batch_tile_plan")
 
     def autotune(self, reps: int = 5, stream=None) -> dict:
         """Time every tile plan on the loaded images, keep the fastest

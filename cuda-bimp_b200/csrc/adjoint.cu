@@ -300,10 +300,10 @@ struct bimp_adjoint {
       for (size_t e2 = 0; e2 < sds.size(); ++e2) sds[e2].cMap = b + offMaps + e2 * kTensorMapBytes;
     }
     h_sd = sds;
-    pipelined = true;
+    // the phased forward tile kernel unless BIMP_TILE_KERNEL=pipelined
+    const char* kern = std::getenv("BIMP_TILE_KERNEL");
+    pipelined = kern && std::strcmp(kern, "pipelined") == 0;
     for (const ScaleDev& d : sds) pipelined = pipelined && d.V <= pipelined_tile_max_valid();
-    if (const char* k = std::getenv("BIMP_TILE_KERNEL"))
-      if (std::strcmp(k, "phased") == 0) pipelined = false;
     d_sd = reinterpret_cast<ScaleDev*>(b + offSd);
     d_tiles = reinterpret_cast<TileWork*>(b + offT2);
     d_sten = reinterpret_cast<int2*>(b + offSt);

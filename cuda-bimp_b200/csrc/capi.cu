@@ -171,7 +171,7 @@ struct Engine {
     }
     return out;
   }
-  int retile(int policy, int order, int grid) {
+  int retile(int policy, int order, int grid, int kernel = 0) {
     std::vector<ScaleDev> sds = h_sd;
     const std::vector<TileWork> tiles = tile_plan(sds, policy, order);
     if ((int)tiles.size() > tileCap) return fail(BIMP_ERR_INVALID, "tile plan larger than its buffer");
@@ -184,17 +184,22 @@ struct Engine {
     tileGrid = grid > 0 ? std::min(grid, nTiles) : nTiles;
     tilePolicy = policy;
     tileOrder = order;
-    tilePipelined = pipelined_fits();
+    tilePipelined = kernel == 1 && pipelined_fits();
     return BIMP_OK;
   }
   // The warp-specialised tile kernel takes every scale with V up to its row
-  // buffers' height (BIMP_TILE_KERNEL=phased selects the phased kernel).
+  // buffers' height.
   bool pipelined_fits() const {
-    if (const char* k = std::getenv("BIMP_TILE_KERNEL"))
-      if (std::strcmp(k, "phased") == 0) return false;
     for (const ScaleDev& d : h_sd)
       if (d.V > pipelined_tile_max_valid()) return false;
     return true;
+  }
+  // Default kernel: the phased one (measured faster on the plain 1080p
+  // detection); BIMP_TILE_KERNEL=pipelined selects the warp-specialised one,
+  // and a batch's tile plan (or its autotuner) may choose either.
+  bool pipelined_by_default() const {
+    const char* k = std::getenv("BIMP_TILE_KERNEL");
+    return k && std::strcmp(k, "pipelined") == 0 && pipelined_fits();
   }
 
   // inW/inH (null: the geometry sizes) are the sizes of the images a
@@ -315,9 +320,10 @@ struct Engine {
         for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
         const int yEnd = std::min(s.dataH - s.off - 1, s.dataH - 2);
         for (int y = s.off + 1; y <= yEnd; ++y) rows.push_back(make_int2(entry, y - s.off - 1));
-        // keypoint-decision words: one per 32 candidate pixels of a row
+        // keypoint-decision words: 32-pixel-aligned words covering a row's
+        // candidate pixels (off, xEnd)
         const int xEnd = std::min(s.dataW - s.off, s.dataW - 1);
-        d.nmsChunks = std::max(0, (xEnd - s.off - 1 + 31) / 32);
+        d.nmsChunks = xEnd > s.off + 1 ? ((xEnd - 1) >> 5) - ((s.off + 1) >> 5) + 1 : 0;
         maskWords.push_back((size_t)std::max(0, yEnd - s.off) * d.nmsChunks);
         sds.push_back(d);
       }
@@ -428,7 +434,7 @@ struct Engine {
       for (size_t e2 = 0; e2 < sds.size(); ++e2) sds[e2].cMap = base + offMaps + e2 * kTensorMapBytes;
     }
     h_sd = sds;
-    tilePipelined = pipelined_fits();
+    tilePipelined = pipelined_by_default();
     d_sd = reinterpret_cast<ScaleDev*>(base + offSd);
     d_tiles = reinterpret_cast<TileWork*>(base + offTiles);
     d_sten = reinterpret_cast<int2*>(base + offSten);
@@ -1041,10 +1047,11 @@ int bimp_batch_image(bimp_batch* b, int i, uint8_t** d_image, size_t* pitch) {
   return BIMP_OK;
 }
 
-int bimp_batch_set_tile_plan(bimp_batch* b, int policy, int order, int grid) {
-  if (!b || policy < 0 || policy > 1 || order < 0 || order > 1) return fail(BIMP_ERR_INVALID, "bad tile plan");
+int bimp_batch_set_tile_plan(bimp_batch* b, int policy, int order, int grid, int kernel) {
+  if (!b || policy < 0 || policy > 1 || order < 0 || order > 1 || kernel < 0 || kernel > 1)
+    return fail(BIMP_ERR_INVALID, "bad tile plan");
   BIMP_CUDA(cudaSetDevice(b->eng.device));
-  const int rc = b->eng.retile(policy, order, grid);
+  const int rc = b->eng.retile(policy, order, grid, kernel);
   if (rc != BIMP_OK) return rc;
   return capture_batch(b);
 }
@@ -1058,37 +1065,41 @@ int bimp_batch_autotune(bimp_batch* b, void* stream, int reps, bimp_tile_plan* c
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->eng.device) != cudaSuccess || sms <= 0)
     sms = 148;
   const int grids[3] = {0, sms, 2 * sms};
+  // the pipelined kernel takes every scale only when its valid blocks fit
+  const int kernels = b->eng.pipelined_fits() ? 2 : 1;
   cudaEvent_t e0, e1;
   BIMP_CUDA(cudaEventCreate(&e0));
   BIMP_CUDA(cudaEventCreate(&e1));
   bimp_tile_plan best{};
   best.ms = -1.f;
   int count = 0, rc = BIMP_OK;
-  for (int policy = 0; policy < 2 && rc == BIMP_OK; ++policy)
-    for (int order = 0; order < 2 && rc == BIMP_OK; ++order)
-      for (int g = 0; g < 3 && rc == BIMP_OK; ++g) {
-        rc = b->eng.retile(policy, order, grids[g]);
-        for (int i = 0; i < 2 && rc == BIMP_OK; ++i) rc = b->eng.enqueue(s);
-        if (rc != BIMP_OK) break;
-        cudaEventRecord(e0, s);
-        for (int i = 0; i < reps && rc == BIMP_OK; ++i) rc = b->eng.enqueue(s);
-        cudaEventRecord(e1, s);
-        if (rc != BIMP_OK) break;
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-          rc = fail(BIMP_ERR_CUDA, "autotune timing failed");
-          break;
+  for (int kernel = kernels - 1; kernel >= 0 && rc == BIMP_OK; --kernel)
+    for (int policy = 0; policy < 2 && rc == BIMP_OK; ++policy)
+      for (int order = 0; order < 2 && rc == BIMP_OK; ++order)
+        for (int g = 0; g < 3 && rc == BIMP_OK; ++g) {
+          rc = b->eng.retile(policy, order, grids[g], kernel);
+          for (int i = 0; i < 2 && rc == BIMP_OK; ++i) rc = b->eng.enqueue(s);
+          if (rc != BIMP_OK) break;
+          cudaEventRecord(e0, s);
+          for (int i = 0; i < reps && rc == BIMP_OK; ++i) rc = b->eng.enqueue(s);
+          cudaEventRecord(e1, s);
+          if (rc != BIMP_OK) break;
+          if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = fail(BIMP_ERR_CUDA, "autotune timing failed");
+            break;
+          }
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          const bimp_tile_plan pl{policy, order, b->eng.tilePipelined ? 1 : 0, b->eng.tileGrid, b->eng.nTiles,
+                                  ms / reps};
+          if (count < max_tried) tried[count] = pl;
+          ++count;
+          if (best.ms < 0.f || pl.ms < best.ms) best = pl;
         }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        const bimp_tile_plan pl{policy, order, b->eng.tileGrid, b->eng.nTiles, ms / reps};
-        if (count < max_tried) tried[count] = pl;
-        ++count;
-        if (best.ms < 0.f || pl.ms < best.ms) best = pl;
-      }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != BIMP_OK) return rc;
-  rc = b->eng.retile(best.policy, best.order, best.grid >= best.tiles ? 0 : best.grid);
+  rc = b->eng.retile(best.policy, best.order, best.grid >= best.tiles ? 0 : best.grid, best.kernel);
   if (rc == BIMP_OK) rc = capture_batch(b);
   if (rc != BIMP_OK) return rc;
   if (chosen) *chosen = best;

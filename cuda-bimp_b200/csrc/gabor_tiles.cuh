@@ -601,15 +601,19 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
         const int b = o & 1;
         float2* Wo = Wb + b * kWsBuf;
         const float* __restrict__ Go = sd->G + (size_t)o * kSpecFloats;
-        // I1: y-dim pass B' with the spectrum product (TMEM in, TMEM y-area out)
+        // I1: y-dim pass B' with the spectrum product (TMEM in, TMEM y-area
+        // out); each quarter's G values are loaded one quarter ahead
+        float g[8];
+#pragma unroll
+        for (int k1 = 0; k1 < 8; ++k1) g[k1] = __ldg(Go + (size_t)(8 * hY + k1) * kTile + pI1);
 #pragma unroll 1
         for (int q = 0; q < 8; ++q) {
           const int k2 = hY + 2 * q;
           float2 v[8];
-          const float* __restrict__ Gq = Go + (size_t)(8 * k2) * kTile + pI1;
-          float g[8];
+          float gn[8];
+          const int k2n = q < 7 ? k2 + 2 : k2;
 #pragma unroll
-          for (int k1 = 0; k1 < 8; ++k1) g[k1] = __ldg(Gq + k1 * kTile);
+          for (int k1 = 0; k1 < 8; ++k1) gn[k1] = __ldg(Go + (size_t)(8 * k2n + k1) * kTile + pI1);
           tmem_load8(tlane + 16 * k2, v);
 #pragma unroll
           for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], g[k1]);
@@ -617,6 +621,8 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
 #pragma unroll
           for (int n1 = 0; n1 < 8; ++n1)
             tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0]);
+#pragma unroll
+          for (int k1 = 0; k1 < 8; ++k1) g[k1] = gn[k1];
         }
         tmem_wait_st();
         tmem_fence_before();

@@ -699,18 +699,15 @@ __device__ __forceinline__ void nms_emit(const ScaleDev* __restrict__ sd, const 
   }
 }
 
-// One warp: the records of candidate row `iy` from its stored decision words,
-// at slots base, base + 1, ... (x order).  32 words per round, one per lane:
-// each lane writes its word's keypoints at the word's place in the row (a
-// warp prefix sum of the word popcounts keeps x order), so a dense row costs
-// as many steps as its densest word has bits, not one step per chunk.
-__device__ __forceinline__ void nms_write_row(const ScaleDev* __restrict__ sd, const KpOut& out, int iy, int base,
-                                              int lane) {
-  const int off = sd->off;
-  const int y = off + 1 + iy;
-  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
-  const int nch = (xEnd - off - 1 + 31) / 32;
-  const unsigned int* __restrict__ mask = sd->nmsMask + (size_t)iy * sd->nmsChunks;
+// One warp: the records of candidate row `iy` from its stored decision words
+// (bit i of word c is the pixel x0 + 32 c + i; nch words), at slots base,
+// base + 1, ... (x order).  32 words per round, one per lane: each lane
+// writes its word's keypoints at the word's place in the row (a warp prefix
+// sum of the word popcounts keeps x order), so a dense row costs as many
+// steps as its densest word has bits, not one step per chunk.
+__device__ __forceinline__ void nms_write_words(const ScaleDev* __restrict__ sd, const KpOut& out, int y,
+                                                const unsigned int* __restrict__ mask, int nch, int x0, int base,
+                                                int lane) {
   for (int c0 = 0; c0 < nch && base < out.capacity; c0 += 32) {
     unsigned int word = c0 + lane < nch ? mask[c0 + lane] : 0u;
     const int pc = __popc(word);
@@ -725,11 +722,20 @@ __device__ __forceinline__ void nms_write_row(const ScaleDev* __restrict__ sd, c
     while (word) {
       const int bit = __ffs(word) - 1;
       word &= word - 1u;
-      if (idx < out.capacity) nms_emit(sd, out, y, off + 1 + 32 * (c0 + lane) + bit, idx);
+      if (idx < out.capacity) nms_emit(sd, out, y, x0 + 32 * (c0 + lane) + bit, idx);
       ++idx;
     }
     base += total;
   }
+}
+
+// The three-kernel path's words: bit i of word c is the pixel off + 1 + 32 c + i.
+__device__ __forceinline__ void nms_write_row(const ScaleDev* __restrict__ sd, const KpOut& out, int iy, int base,
+                                              int lane) {
+  const int off = sd->off;
+  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
+  const int nch = (xEnd - off - 1 + 31) / 32;
+  nms_write_words(sd, out, off + 1 + iy, sd->nmsMask + (size_t)iy * sd->nmsChunks, nch, off + 1, base, lane);
 }
 
 // Records of a row in x order at the row's offset (one warp per row).
@@ -792,43 +798,107 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// One warp: decision words of candidate row iy (stored to the row's mask
-// words) and its keypoint count.  The centre values of four chunks are loaded
-// together; the 8 neighbours only where the centre passes the threshold.
+// Spreads bit i of an 8-bit value to bit 4 i.
+__device__ __forceinline__ unsigned int spread4(unsigned int x) {
+  x &= 0xffu;
+  x = (x | (x << 12)) & 0x000f000fu;
+  x = (x | (x << 6)) & 0x03030303u;
+  x = (x | (x << 3)) & 0x11111111u;
+  return x;
+}
+
+// Aligned decision words of a candidate row: word c covers the pixels
+// 32 (first + c) .. 32 (first + c) + 31, first = (off + 1) / 32; pixels outside
+// the candidate range (off, xEnd) are 0.
+__device__ __forceinline__ void nms_row_words(const ScaleDev* __restrict__ sd, int& first, int& nch) {
+  const int off = sd->off;
+  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
+  first = (off + 1) >> 5;
+  nch = xEnd > off + 1 ? ((xEnd - 1) >> 5) - first + 1 : 0;
+}
+
+// One warp: the aligned decision words of candidate row iy (stored to the
+// row's mask words) and its keypoint count.  A segment is 128 pixels, four per
+// lane: the lane reads them and the rows above and below as 16-byte vectors
+// (the row pitch is a multiple of 32 floats), four segments per round, so a
+// row costs about one memory latency per 512 pixels; the neighbours across
+// lanes come by shuffles, across segments by two scalar loads.
+constexpr int kNmsSegBatch = 4;
 __device__ __forceinline__ int nms_decide_row(const ScaleDev* __restrict__ sd, int iy, int lane) {
   const int off = sd->off;
   const int y = off + 1 + iy;
+  const int W = sd->dataW;
+  const int xEnd = min(W - off, W - 1);
   const float thr = scale_thresh(sd);
-  const int xEnd = min(sd->dataW - off, sd->dataW - 1);
-  const int nch = (xEnd - off - 1 + 31) / 32;
   const float* __restrict__ D = sd->D;
   const int dp = sd->dPitch;
-  const float* __restrict__ row = D + (size_t)y * dp;
+  const float* __restrict__ rc = D + (size_t)y * dp;
+  const float* __restrict__ ru = rc - dp;
+  const float* __restrict__ rd = rc + dp;
+  int first, nch;
+  nms_row_words(sd, first, nch);
   unsigned int* __restrict__ mask = sd->nmsMask + (size_t)iy * sd->nmsChunks;
+  if (nch <= 0) return 0;
+  const int seg0 = (off + 1) >> 7, seg1 = (xEnd - 1) >> 7;
   int n = 0;
-  for (int c0 = 0; c0 < nch; c0 += 4) {
-    float v[4];
+  for (int sb = seg0; sb <= seg1; sb += kNmsSegBatch) {
+    float4 c[kNmsSegBatch], u[kNmsSegBatch], d[kNmsSegBatch];
+    float cl[kNmsSegBatch], ul[kNmsSegBatch], dl[kNmsSegBatch], cr[kNmsSegBatch], ur[kNmsSegBatch], dr[kNmsSegBatch];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int x = off + 1 + 32 * (c0 + u) + lane;
-      v[u] = (c0 + u < nch && x < xEnd) ? row[x] : -INFINITY;
+    for (int k = 0; k < kNmsSegBatch; ++k) {
+      const int x4 = 128 * (sb + k) + 4 * lane;
+      const bool in = sb + k <= seg1 && x4 < W;
+      c[k] = in ? *reinterpret_cast<const float4*>(rc + x4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      u[k] = in ? *reinterpret_cast<const float4*>(ru + x4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      d[k] = in ? *reinterpret_cast<const float4*>(rd + x4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      // the pixels beyond the lane group: left of lane 0, right of lane 31
+      const bool le = in && lane == 0 && x4 >= 1, ri = in && lane == 31 && x4 + 4 < W;
+      cl[k] = le ? rc[x4 - 1] : 0.f;
+      ul[k] = le ? ru[x4 - 1] : 0.f;
+      dl[k] = le ? rd[x4 - 1] : 0.f;
+      cr[k] = ri ? rc[x4 + 4] : 0.f;
+      ur[k] = ri ? ru[x4 + 4] : 0.f;
+      dr[k] = ri ? rd[x4 + 4] : 0.f;
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (c0 + u >= nch) break;
-      const int x = off + 1 + 32 * (c0 + u) + lane;
-      bool k = false;
-      if (v[u] > thr) {
-        const float* r0 = row - dp;
-        const float* r2 = row + dp;
-        float dil = fmaxf(fmaxf(r0[x - 1], r0[x]), r0[x + 1]);
-        dil = fmaxf(dil, fmaxf(row[x - 1], row[x + 1]));
-        dil = fmaxf(dil, fmaxf(fmaxf(r2[x - 1], r2[x]), r2[x + 1]));
-        k = v[u] - dil > 0.f;
+    for (int k = 0; k < kNmsSegBatch; ++k) {
+      if (sb + k > seg1) break;
+      const int x4 = 128 * (sb + k) + 4 * lane;
+      // left neighbour column of x4 and right neighbour column of x4 + 3
+      float lc = __shfl_up_sync(0xffffffffu, c[k].w, 1), lu = __shfl_up_sync(0xffffffffu, u[k].w, 1),
+            ld = __shfl_up_sync(0xffffffffu, d[k].w, 1);
+      float rcv = __shfl_down_sync(0xffffffffu, c[k].x, 1), ruv = __shfl_down_sync(0xffffffffu, u[k].x, 1),
+            rdv = __shfl_down_sync(0xffffffffu, d[k].x, 1);
+      if (lane == 0) { lc = cl[k]; lu = ul[k]; ld = dl[k]; }
+      if (lane == 31) { rcv = cr[k]; ruv = ur[k]; rdv = dr[k]; }
+      const float cv[6] = {lc, c[k].x, c[k].y, c[k].z, c[k].w, rcv};
+      const float uv[6] = {lu, u[k].x, u[k].y, u[k].z, u[k].w, ruv};
+      const float dv[6] = {ld, d[k].x, d[k].y, d[k].z, d[k].w, rdv};
+      unsigned int b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int x = x4 + i;
+        const float v = cv[i + 1];
+        bool keep = false;
+        if (x > off && x < xEnd && v > thr) {
+          float dil = fmaxf(fmaxf(uv[i], uv[i + 1]), uv[i + 2]);
+          dil = fmaxf(dil, fmaxf(cv[i], cv[i + 2]));
+          dil = fmaxf(dil, fmaxf(fmaxf(dv[i], dv[i + 1]), dv[i + 2]));
+          keep = v - dil > 0.f;
+        }
+        b[i] = __ballot_sync(0xffffffffu, keep);
+        n += __popc(b[i]);
       }
-      const unsigned int bal = __ballot_sync(0xffffffffu, k);
-      n += __popc(bal);
-      if (lane == 0) mask[c0 + u] = bal;
+      // word w of the segment: lanes 8 w .. 8 w + 7, bit 4 (lane - 8 w) + i
+      if (lane < 4) {
+        const int widx = 4 * (sb + k) + lane - first;
+        if (widx >= 0 && widx < nch) {
+          unsigned int word = 0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) word |= spread4(b[i] >> (8 * lane)) << i;
+          mask[widx] = word;
+        }
+      }
     }
   }
   return n;
@@ -893,7 +963,11 @@ k_nms_fused(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, con
     const KpOut out = outs[cta.image];
     int base = s_base;
     for (int w = 0; w < warp; ++w) base += s_cnt[w];
-    if (base < out.capacity) nms_write_row(sd, out, item.y, base, lane);
+    int first, nch;
+    nms_row_words(sd, first, nch);
+    if (base < out.capacity)
+      nms_write_words(sd, out, sd->off + 1 + item.y, sd->nmsMask + (size_t)item.y * sd->nmsChunks, nch, 32 * first,
+                      base, lane);
   }
 }
 

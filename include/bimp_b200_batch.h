@@ -38,19 +38,24 @@ int bimp_batch_image(bimp_batch* batch, int i, uint8_t** d_image, size_t* pitch)
  * valid block per 128 x 128 tile (128 - 2 kX outputs per side), 1 rounds it
  * down to a multiple of 32 where that keeps at least 3/4 of it (more tiles,
  * evenly split passes); `order` 0 queues tiles scale by scale, 1 interleaves
- * the scales' tiles; `grid` is the number of CTAs of the tile kernel (each
- * walks tiles; the tile count means one CTA per tile).  `ms` is the
- * measured time of one detection of the batch with the plan. */
+ * the scales' tiles; `kernel` 1 runs the warp-specialised tile kernel (the
+ * inverse y-passes of one orientation overlap the x-passes of the previous
+ * one; needs every valid block <= 104), 0 the phased one (all warps pass by
+ * pass); `grid` is the number of CTAs of the tile kernel (each walks tiles;
+ * the tile count means one CTA per tile).  `ms` is the measured time of one
+ * detection of the batch with the plan. */
 typedef struct {
   int policy;
   int order;
+  int kernel;
   int grid;
   int tiles;
   float ms;
 } bimp_tile_plan;
 
 /* Autotuner (no counterpart in the reference): times every tile plan
- * (2 policies x 2 orders x 3 grids: one CTA per tile, one and two per SM)
+ * (2 kernels x 2 policies x 2 orders x 3 grids: one CTA per tile, one and two
+ * per SM)
  * over `reps` detections of the batch's current inputs on `stream`, keeps
  * the fastest and recaptures the graph with it.  Plans of one policy give
  * bitwise identical results; policy 1 moves tile boundaries, which changes
@@ -61,8 +66,9 @@ int bimp_batch_autotune(bimp_batch* batch, void* stream, int reps, bimp_tile_pla
                         bimp_tile_plan* tried, int max_tried, int* n_tried);
 
 /* Uses the given tile plan (e.g. one the autotuner chose earlier) and
- * recaptures the graph; grid <= 0 means one CTA per tile. */
-int bimp_batch_set_tile_plan(bimp_batch* batch, int policy, int order, int grid);
+ * recaptures the graph; grid <= 0 means one CTA per tile; kernel 1 falls back
+ * to the phased kernel where the pipelined one does not fit. */
+int bimp_batch_set_tile_plan(bimp_batch* batch, int policy, int order, int grid, int kernel);
 
 /* Replays the captured graph on `stream` (no host synchronisation). */
 int bimp_batch_run(bimp_batch* batch, void* stream);

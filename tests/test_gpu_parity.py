@@ -264,8 +264,10 @@ def test_batch_matches_single():
 
 
 def test_batch_tile_plans_and_autotune():
-    """Every tile plan keeps parity with the oracle; plans of one policy are
-    bitwise identical; the autotuner times all 12 and keeps the fastest."""
+    """Every tile plan keeps parity with the oracle; plans of one policy and
+    kernel variant are bitwise identical (tile order, grid); the autotuner
+    times all 24 (2 kernels x 2 policies x 2 orders x 3 grids) and keeps the
+    fastest."""
     rng = np.random.default_rng(9)
     sizes = [(int(rng.integers(20, 50)) * 16, int(rng.integers(15, 35)) * 16) for _ in range(3)]
     imgs = [synth.synth_image(w, h, 8, seed=90 + i) for i, (w, h) in enumerate(sizes)]
@@ -275,20 +277,24 @@ def test_batch_tile_plans_and_autotune():
     b.load(imgs)
     outs = {}
     for policy in (0, 1):
-        for order, grid in ((0, 0), (1, 148)):
-            b.set_tile_plan(policy, order, grid)
+        for order, grid, kernel in ((0, 0, 1), (1, 148, 1), (0, 0, 0), (1, 296, 0)):
+            b.set_tile_plan(policy, order, grid, kernel)
             b.run()
-            outs[(policy, order)] = [api.keypoint_matrix_to_records(b.keypoints(i)) for i in range(len(imgs))]
+            outs[(policy, order, kernel)] = [api.keypoint_matrix_to_records(b.keypoints(i)) for i in range(len(imgs))]
         for i in range(len(imgs)):
-            assert np.array_equal(outs[(policy, 0)][i], outs[(policy, 1)][i])
-            _check_keypoints(outs[(policy, 0)][i], refs[i])
+            # tile order and grid leave every record bitwise unchanged
+            for kernel in (0, 1):
+                assert np.array_equal(outs[(policy, 0, kernel)][i], outs[(policy, 1, kernel)][i]), kernel
+                _check_keypoints(outs[(policy, 0, kernel)][i], refs[i])
     rep = b.autotune(reps=2)
-    assert len(rep["tried"]) == 12 and rep["chosen"]["ms"] > 0
+    assert len(rep["tried"]) == 24 and rep["chosen"]["ms"] > 0
+    assert {t["kernel"] for t in rep["tried"]} == {0, 1}
     assert rep["chosen"]["ms"] == min(t["ms"] for t in rep["tried"])
     b.run()
+    ch = rep["chosen"]
     for i in range(len(imgs)):
         got = api.keypoint_matrix_to_records(b.keypoints(i))
-        assert np.array_equal(got, outs[(rep["chosen"]["policy"], 0)][i])
+        assert np.array_equal(got, outs[(ch["policy"], 0, ch["kernel"])][i])
     b.close()
 
 
@@ -339,6 +345,7 @@ def test_cpp_context_shim_matches_python_api(tmp_path, w, h, cn):
     ctx_line = next(ln for ln in lines if ln[0] == "ctx")
     resp = [ln for ln in lines if ln[0] == "resp"]
     ctx = api.Context(img, lambdas=lam)
+    ctx.capacity = 1 << 20   # as the C++ program sets it
     uw, uh = api.min_size_dims(w, h)
     assert (int(ctx_line[1]), int(ctx_line[2])) == (ctx.width(), ctx.height()) == (uw, uh)
     ref = api.keypoint_matrix_to_records(ctx.getKeypoints())
