@@ -287,6 +287,52 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
   }
 }
 
+// Detection mode, interior blocks: the two pixels of a thread (rows cy0 and
+// cy1 of the window, column cx) through packed FP32x2 arithmetic.  Each lane
+// of a packed operation rounds as a scalar one: the double-stopped term is
+// two fused multiply-adds and the radial term centre - gain * C one, as in
+// stencil_pixel.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 relu2(float2 v) { return make_float2(fmaxf(v.x, 0.f), fmaxf(v.y, 0.f)); }
+
+template <int PAT>
+__device__ __forceinline__ float2 stencil_pair_d(const float* __restrict__ s_c, const StencilPar& P, int cy0, int cy1,
+                                                 int cx, float gain, float wT, float wR) {
+  float2 D = f2(0.f, 0.f), T = f2(0.f, 0.f), R = f2(0.f, 0.f);
+  const float* a0 = s_c + cy0 * kStW + cx;
+  const float* a1 = s_c + cy1 * kStW + cx;
+  const float2 mhalf = f2(-0.5f, -0.5f), mgain = f2(-gain, -gain);
+#pragma unroll
+  for (int o = 0; o < kNumOri; ++o) {
+    const int o1 = soff<PAT>(P, 0, o), o2 = soff<PAT>(P, 1, o);
+    const float* c0 = a0 + o * (kStH * kStW);
+    const float* c1 = a1 + o * (kStH * kStW);
+    const int tb = 2 * o1 * kStW - 2 * o2;
+    const float2 c = f2(c0[0], c1[0]);
+    const float2 d = __ffma2_rn(mhalf, f2(c0[tb], c1[tb]), __ffma2_rn(mhalf, f2(c0[-tb], c1[-tb]), c));
+    D = __fadd2_rn(D, relu2(d));
+  }
+#pragma unroll
+  for (int o = 0; o < kNumOri; ++o) {
+    const int o1 = soff<PAT>(P, 2, o), o2 = soff<PAT>(P, 3, o);
+    const int op = (o + kNumOri / 2) % kNumOri;
+    const float* c0 = a0 + o * (kStH * kStW);
+    const float* c1 = a1 + o * (kStH * kStW);
+    const float* p0 = a0 + op * (kStH * kStW);
+    const float* p1 = a1 + op * (kStH * kStW);
+    const float2 centre = f2(c0[0], c1[0]);
+    const int tt = -o1 * kStW - o2;
+    T = __fadd2_rn(T, relu2(__fadd2_rn(f2(c0[tt], c1[tt]), f2(-centre.x, -centre.y))));
+    const int h1 = soff<PAT>(P, 4, o), h2 = soff<PAT>(P, 5, o);
+    const int th = h1 * kStW + h2;
+    float2 r = relu2(__ffma2_rn(mgain, f2(p0[th], p1[th]), centre));
+    r = __fadd2_rn(r, __ffma2_rn(mgain, f2(p0[-th], p1[-th]), centre));
+    R = __fadd2_rn(R, relu2(r));
+  }
+  const float2 inhib = __ffma2_rn(f2(wT, wT), T, __fmul2_rn(f2(wR, wR), R));
+  return __fadd2_rn(D, f2(-inhib.x, -inhib.y));
+}
+
 // Output maps of one stencil block.
 struct StencilOut {
   float* D;
@@ -309,11 +355,17 @@ __device__ __forceinline__ float stencil_rows(const float* __restrict__ s_c, con
   constexpr int kRows = kFwY / (NT / 32);
   float D[kRows], S[kRows], T[kRows], R[kRows];
   unsigned int b[kRows];
+  if constexpr (!CHECK && MODE == kStencilD && kRows == 2) {
+    const float2 d = stencil_pair_d<PAT>(s_c, P, ly0 + kHalo, ly0 + NT / 32 + kHalo, lx + kHalo, gain, wT, wR);
+    D[0] = d.x;
+    D[1] = d.y;
+  } else {
 #pragma unroll
-  for (int i = 0; i < kRows; ++i) {
-    const int ly = ly0 + (NT / 32) * i;
-    stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i], R[i],
-                                    b[i]);
+    for (int i = 0; i < kRows; ++i) {
+      const int ly = ly0 + (NT / 32) * i;
+      stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i],
+                                      R[i], b[i]);
+    }
   }
   float dmax = -INFINITY;
 #pragma unroll
@@ -820,10 +872,12 @@ __device__ __forceinline__ void nms_row_words(const ScaleDev* __restrict__ sd, i
 // One warp: the aligned decision words of candidate row iy (stored to the
 // row's mask words) and its keypoint count.  A segment is 128 pixels, four per
 // lane: the lane reads them and the rows above and below as 16-byte vectors
-// (the row pitch is a multiple of 32 floats), four segments per round, so a
-// row costs about one memory latency per 512 pixels; the neighbours across
-// lanes come by shuffles, across segments by two scalar loads.
-constexpr int kNmsSegBatch = 4;
+// (the row pitch is a multiple of 32 floats), two segments per round, so a
+// row costs about one memory latency per 256 pixels; the neighbours across
+// lanes come by shuffles, across segments by two scalar loads.  Two segments
+// per round keep the kernel within 64 registers, so that every CTA of a 1080p
+// detection is resident at once (four per SM).
+constexpr int kNmsSegBatch = 2;
 __device__ __forceinline__ int nms_decide_row(const ScaleDev* __restrict__ sd, int iy, int lane) {
   const int off = sd->off;
   const int y = off + 1 + iy;
@@ -904,7 +958,7 @@ __device__ __forceinline__ int nms_decide_row(const ScaleDev* __restrict__ sd, i
   return n;
 }
 
-__global__ void __launch_bounds__(32 * kNmsRowsPerCta)
+__global__ void __launch_bounds__(32 * kNmsRowsPerCta, 4)
 k_nms_fused(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, const NmsCta* __restrict__ ctas,
             unsigned long long* __restrict__ status, int* __restrict__ imageTotals, const KpOut* __restrict__ outs,
             unsigned int* __restrict__ fault_word) {
