@@ -487,14 +487,16 @@ struct Engine {
         for (size_t l = 0; l < pyrFirst.size(); ++l)
           launch_pyr(d_pyr + pyrFirst[l], pyrCount[l], pyrLevels[l], pyrMaxW[l], pyrMaxH[l], s);
         break;
+      // stages 1-3 follow the previous stage's kernel with programmatic
+      // dependent launch (each waits in the kernel for its predecessor)
       case 1:
-        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s, tilePipelined);
+        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s, tilePipelined, true);
         break;
       case 2:
-        if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD);
+        if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD, true);
         break;
       case 3:
-        launch_nms_fused(d_sd, d_rows, d_nmsCtas, nNmsCtas, d_nmsStatus, d_totals, d_outs, d_fault, s);
+        launch_nms_fused(d_sd, d_rows, d_nmsCtas, nNmsCtas, d_nmsStatus, d_totals, d_outs, d_fault, s, true);
         break;
       default:
         return fail(BIMP_ERR_INVALID, "unknown stage");
@@ -509,9 +511,10 @@ struct Engine {
 
   // Everything after the level-0 images are in place.
   int enqueue(cudaStream_t s) {
+    // the reset first, so that the four kernels follow one another directly
+    BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, resetBytes, s));
     int rc = stage(0, s);
     if (rc != BIMP_OK) return rc;
-    BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, resetBytes, s));
     for (int k = 1; k <= 3; ++k) {
       rc = stage(k, s);
       if (rc != BIMP_OK) return rc;

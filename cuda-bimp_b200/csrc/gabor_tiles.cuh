@@ -309,9 +309,11 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     fence_mbar_init();
   }
   if ((t >> 5) == 0) tmem_alloc_warp(smem_u32(tmemSlot));
+  griddep_launch_dependents();
   tmem_fence_before();
   __syncthreads();
   tmem_fence_after();
+  griddep_wait();   // the pyramid levels come from the previous kernel
   // this thread's lane (t mod 128) of the spectrum; (warp mod 4) * 32 is the
   // lane block the warp may access
   const uint32_t tlane = *tmemSlot + ((uint32_t)((t >> 5) & 3) << 21);
@@ -556,9 +558,11 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
     tw[t] = k2 < 16 ? c_w128[(n1 * k2) & 127] : make_float2(0.f, 0.f);
   }
   if ((t >> 5) == 0) tmem_alloc_warp(smem_u32(tmemSlot));
+  griddep_launch_dependents();
   tmem_fence_before();
   __syncthreads();
   tmem_fence_after();
+  griddep_wait();   // the pyramid levels come from the previous kernel
   const uint32_t tlane = *tmemSlot + ((uint32_t)((t >> 5) & 3) << 21);
   // spectrum store (all warps): column p of the full spectrum in the half
   const int pI1 = t & 127, h4 = t >> 7;

@@ -23,6 +23,18 @@
 
 namespace bimp_b200 {
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialisation may start before its predecessor in the stream has finished:
+// griddep_wait() blocks until the predecessor grid has completed and its
+// memory is visible (a no-op after an ordinary launch), and
+// griddep_launch_dependents() lets the successor's CTAs be scheduled once
+// every CTA of this grid has started (they then wait in griddep_wait, on SMs
+// this grid's last wave leaves free).
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------
 // pyramid
 // ---------------------------------------------------------------------------
@@ -69,6 +81,7 @@ template <int K>
 __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ jobs) {
   __shared__ uint8_t s_lvl[pyr_smem(K)];
   __shared__ uint16_t s_h[pyr_hbuf(K)];
+  griddep_launch_dependents();
   const PyrJob& j = jobs[blockIdx.z];
   constexpr int T = pyr_tile(K);
   const int oy = blockIdx.y * T, ox = blockIdx.x * T;
@@ -512,6 +525,7 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
   __shared__ StencilBlk blk[kStBufs];
   __shared__ __align__(8) uint64_t s_full[kStBufs], s_empty[kStBufs];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  griddep_launch_dependents();
   if ((int)blockIdx.x >= nwork) return;
   const uint32_t full0 = smem_u32(&s_full[0]), empty0 = smem_u32(&s_empty[0]);
   if (t == 0) {
@@ -522,6 +536,7 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
     fence_mbar_init();
   }
   __syncthreads();
+  griddep_wait();   // the complex cells come from the previous kernel
   const int nk = (nwork - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;   // blocks of this CTA
   if (warp == kStConsumers / 32) {
     // producer warp: block k goes to buffer k mod kStBufs, its use k / kStBufs
@@ -966,6 +981,7 @@ k_nms_fused(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, con
   __shared__ int s_base;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const NmsCta cta = ctas[blockIdx.x];
+  griddep_wait();   // the summed maps and their maxima come from the previous kernel
   int2 item = make_int2(0, 0);
   int cnt = 0;
   if (warp < cta.nRows) {
@@ -1182,6 +1198,25 @@ cudaError_t configure_kernels() {
   return upload_twiddles();
 }
 
+// Launches kernel k with programmatic stream serialisation when pdl is set
+// (the kernel must call griddep_wait() before it reads its predecessor's
+// output).
+template <typename... Params, typename... Args>
+static void launch_ex(void (*k)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, bool pdl,
+                      Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, static_cast<Params>(args)...);
+}
+
 // The keypoint destination descriptor of a context, written in stream order
 // from a kernel argument (no host memory involved, so the write is also
 // valid inside a stream capture).
@@ -1197,12 +1232,12 @@ void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH,
   else k_pyr_down<1><<<g, 256, 0, s>>>(d_jobs);
 }
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
-                  cudaStream_t s, bool pipelined) {
+                  cudaStream_t s, bool pipelined, bool pdl) {
   if (pipelined)
-    k_gabor_tiles_ws<false><<<grid, kTileThreads, kWsSmem, s>>>(d_sd, d_work, nwork);
+    launch_ex(k_gabor_tiles_ws<false>, grid, kTileThreads, kWsSmem, s, pdl, d_sd, d_work, nwork);
   else
-    k_gabor_tiles<false, false><<<grid, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault,
-                                                                                nullptr);
+    launch_ex(k_gabor_tiles<false, false>, grid, kTileThreads, gabor_smem_bytes(), s, pdl, d_sd, d_work, nwork,
+              d_fault, static_cast<float2*>(nullptr));
 }
 void launch_gabor_flt(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
                       cudaStream_t s, bool pipelined) {
@@ -1245,21 +1280,22 @@ void launch_gabor_bwd(const ScaleDev* d_sd, const TileWork* d_work, int nwork, i
                                                                                  d_gparams);
 }
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigned int* d_fault, cudaStream_t s,
-                    int mode) {
+                    int mode, bool pdl) {
   if (nwork <= 0) return;
   const int grid = std::min(nwork, kStCtasPerSm * num_sms());
   if (mode == kStencilDS)
-    k_stencil<kStencilDS><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+    launch_ex(k_stencil<kStencilDS>, grid, kStThreads, stencil_smem_bytes(), s, pdl, d_sd, d_work, nwork, d_fault);
   else if (mode == kStencilAdj)
-    k_stencil<kStencilAdj><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+    launch_ex(k_stencil<kStencilAdj>, grid, kStThreads, stencil_smem_bytes(), s, pdl, d_sd, d_work, nwork, d_fault);
   else
-    k_stencil<kStencilD><<<grid, kStThreads, stencil_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
+    launch_ex(k_stencil<kStencilD>, grid, kStThreads, stencil_smem_bytes(), s, pdl, d_sd, d_work, nwork, d_fault);
 }
 void launch_nms_fused(const ScaleDev* d_sd, const int2* d_rows, const NmsCta* d_ctas, int nctas,
                       unsigned long long* d_status, int* d_totals, const KpOut* d_outs, unsigned int* d_fault,
-                      cudaStream_t s) {
+                      cudaStream_t s, bool pdl) {
   if (nctas > 0)
-    k_nms_fused<<<nctas, 32 * kNmsRowsPerCta, 0, s>>>(d_sd, d_rows, d_ctas, d_status, d_totals, d_outs, d_fault);
+    launch_ex(k_nms_fused, nctas, 32 * kNmsRowsPerCta, 0, s, pdl, d_sd, d_rows, d_ctas, d_status, d_totals, d_outs,
+              d_fault);
 }
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,

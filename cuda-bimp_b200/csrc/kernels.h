@@ -53,8 +53,10 @@ void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH,
 // d_fault: word that receives 1 if a bounded device wait expired.
 // pipelined: the warp-specialised variant (k_gabor_tiles_ws), for work whose
 // scales all have V <= pipelined_tile_max_valid(); otherwise the phased one
+// pdl: launched with programmatic stream serialisation after the previous
+// kernel of the detection sequence (see griddep_wait in kernels.cu)
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
-                  cudaStream_t s, bool pipelined);
+                  cudaStream_t s, bool pipelined, bool pdl = false);
 int pipelined_tile_max_valid();
 // One TMA tensor map per scale entry over its complex-cell maps (x: cPitch
 // columns, y: cRows rows, z: the 8 orientations; box 48 x 48 x 8 floats,
@@ -71,7 +73,7 @@ enum StencilMode { kStencilD = 0, kStencilDS = 1, kStencilAdj = 2 };
 // Persistent stencil (one CTA per SM); an expired staging wait sets bit 1 of
 // *d_fault.
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigned int* d_fault, cudaStream_t s,
-                    int mode = kStencilD);
+                    int mode = kStencilD, bool pdl = false);
 // Single-pass NMS (decisions, chained per-image prefix, records): one CTA per
 // group of up to kNmsRowsPerCta candidate rows of one image.  d_status
 // (nctas words) must be zero at launch; an expired wait sets bit 2 of
@@ -86,7 +88,7 @@ struct NmsCta {
 };
 void launch_nms_fused(const ScaleDev* d_sd, const int2* d_rows, const NmsCta* d_ctas, int nctas,
                       unsigned long long* d_status, int* d_totals, const KpOut* d_outs, unsigned int* d_fault,
-                      cudaStream_t s);
+                      cudaStream_t s, bool pdl = false);
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,
                 cudaStream_t s);

@@ -224,6 +224,20 @@ inline int getKeypoints(const uint8_t* d_image, size_t pitch, CudaStuff& cs, flo
   return n;
 }
 
+// GpuMat getKeypoints(GpuMat& input, CudaStuff& cs), bimp/src/cuda_bimp.cu:129-140:
+// a fresh 7 x capacity device matrix whose `cols` is set to the keypoints
+// kept (as the reference's colRange view); more than `capacity` found are
+// truncated, as the reference warns and truncates.  `found` (optional)
+// receives the count before truncation.
+inline DeviceMat getKeypoints(const uint8_t* d_image, size_t pitch, CudaStuff& cs, int capacity = KP_MAX_POINTS,
+                              int* found = nullptr) {
+  DeviceMat kp(KP_VECTOR_LENGTH, capacity, sizeof(float));
+  const int n = getKeypoints(d_image, pitch, cs, kp.ptr<float>(), kp.step / sizeof(float), capacity);
+  if (found) *found = n;
+  kp.cols = n < capacity ? n : capacity;
+  return kp;
+}
+
 // getGPUImage(cv::Mat&, bool grayscale), bimp/src/cuda_bimp.cu:156-180: the
 // host image uploaded, upscaled when a side is below 350 pixels, and for a
 // 3-channel BGR image with grayscale set converted to grey.

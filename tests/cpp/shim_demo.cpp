@@ -5,6 +5,8 @@
 //   one "kp x y size response octave class_id angle" line per keypoint (from
 //   the device 7 x n matrix of Context::getKeypoints(), downloaded);
 //   "ctx width height found" (the uploaded image's size, as Context::width());
+//   "lowlevel found same" (bimp::cuda::getKeypoints on the context's device
+//   image: its count, and 1 if its records equal the context's);
 //   one "resp scale data_w data_h maxD sumD sumS" line per scale
 //   (Context::downloadResultsToCPU());
 //   "color n sum" for a BGR image (Context::getColorFeatures()).
@@ -45,6 +47,15 @@ int main(int argc, char** argv) {
       std::printf("kp %.9g %.9g %.9g %.9g %d %d %.1f\n", k.pt.x, k.pt.y, k.size, k.response, k.octave, k.class_id,
                   k.angle);
     std::printf("ctx %d %d %d\n", ctx.width(), ctx.height(), ctx.found);
+    // the lower-level pair on the context's device image (GpuMat getKeypoints(GpuMat&, CudaStuff&))
+    int found = 0;
+    bimp::DeviceMat low = bimp::cuda::getKeypoints(ctx.current_image.data, ctx.current_image.step, ctx.cuda_data,
+                                                   1 << 20, &found);
+    const std::vector<bimp::KeyPoint> pts2 = bimp::utils::downloadKeypoints(low);
+    bool same = pts2.size() == pts.size();
+    for (size_t i = 0; same && i < pts.size(); ++i)
+      same = pts2[i].pt.x == pts[i].pt.x && pts2[i].pt.y == pts[i].pt.y && pts2[i].response == pts[i].response;
+    std::printf("lowlevel %d %d\n", found, same ? 1 : 0);
     for (const auto& r : ctx.downloadResultsToCPU()) {
       double mx = -1e300, sd = 0, ss = 0;
       for (float x : r.h_ResultDouble) {

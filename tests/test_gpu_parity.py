@@ -343,6 +343,8 @@ def test_cpp_context_shim_matches_python_api(tmp_path, w, h, cn):
     lines = [ln.split() for ln in res.stdout.splitlines()]
     kps = [ln[1:] for ln in lines if ln[0] == "kp"]
     ctx_line = next(ln for ln in lines if ln[0] == "ctx")
+    low = next(ln for ln in lines if ln[0] == "lowlevel")
+    assert int(low[1]) == int(ctx_line[3]) and low[2] == "1"
     resp = [ln for ln in lines if ln[0] == "resp"]
     ctx = api.Context(img, lambdas=lam)
     ctx.capacity = 1 << 20   # as the C++ program sets it
