@@ -118,10 +118,10 @@ struct Engine {
   int nSten = 0;
   int2* d_rows = nullptr;
   int nRows = 0;
-  NmsCta* d_nmsCtas = nullptr;          // the NMS kernel's row groups (one image each)
+  NmsCta* d_nmsCtas = nullptr;          // the NMS kernels' row groups (one image each)
   int nNmsCtas = 0;
-  unsigned long long* d_nmsStatus = nullptr;   // the NMS CTAs' published prefixes (zeroed per detection)
-  size_t resetBytes = 0;                // d_maxKeys .. end of d_nmsStatus, zeroed per detection
+  int* d_nmsCount = nullptr;            // keypoints per NMS row group
+  size_t resetBytes = 0;                // d_maxKeys and the fault word, zeroed per detection
   int* d_totals = nullptr;
   unsigned int* d_maxKeys = nullptr;
   unsigned int* d_fault = nullptr;      // set by the tile kernel, the stencil or the NMS if a bounded wait expired
@@ -379,11 +379,10 @@ struct Engine {
     const size_t offRows = a.reserve(sizeof(int2) * std::max<size_t>(1, rows.size()));
     const size_t offNmsCtas = a.reserve(sizeof(NmsCta) * std::max<size_t>(1, nmsCtas.size()));
     const size_t offTotals = a.reserve(sizeof(int) * n);
-    // per-detection reset region: the map maxima, the fault word, the NMS
-    // status words (8-byte aligned), cleared by one memset
-    const size_t maxBytes = align_up(sizeof(unsigned int) * (sds.size() + 1), 8);
-    const size_t offMax = a.reserve(maxBytes + sizeof(unsigned long long) * std::max<size_t>(1, nmsCtas.size()));
-    resetBytes = maxBytes + sizeof(unsigned long long) * std::max<size_t>(1, nmsCtas.size());
+    // per-detection reset region: the map maxima and the fault word
+    resetBytes = sizeof(unsigned int) * (sds.size() + 1);
+    const size_t offMax = a.reserve(resetBytes);
+    const size_t offNmsCount = a.reserve(sizeof(int) * std::max<size_t>(1, nmsCtas.size()));
     const size_t offOuts = a.reserve(sizeof(KpOut) * n);
     const size_t offPyr = a.reserve(sizeof(PyrJob) * std::max<size_t>(1, h_pyr.size()));
     const size_t offMaps = a.reserve(kTensorMapBytes * sds.size());
@@ -442,7 +441,7 @@ struct Engine {
     d_nmsCtas = reinterpret_cast<NmsCta*>(base + offNmsCtas);
     d_totals = reinterpret_cast<int*>(base + offTotals);
     d_maxKeys = reinterpret_cast<unsigned int*>(base + offMax);
-    d_nmsStatus = reinterpret_cast<unsigned long long*>(base + offMax + maxBytes);
+    d_nmsCount = reinterpret_cast<int*>(base + offNmsCount);
     d_fault = d_maxKeys + sds.size();
     d_outs = reinterpret_cast<KpOut*>(base + offOuts);
     d_pyr = reinterpret_cast<PyrJob*>(base + offPyr);
@@ -496,7 +495,7 @@ struct Engine {
         if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD, true);
         break;
       case 3:
-        launch_nms_fused(d_sd, d_rows, d_nmsCtas, nNmsCtas, d_nmsStatus, d_totals, d_outs, d_fault, s, true);
+        launch_nms_two_pass(d_sd, d_rows, d_nmsCtas, nNmsCtas, d_nmsCount, d_totals, d_outs, s, true);
         break;
       default:
         return fail(BIMP_ERR_INVALID, "unknown stage");
@@ -506,7 +505,7 @@ struct Engine {
   }
 
   int kernel_launches() const {
-    return static_cast<int>(pyrFirst.size()) + (nTiles > 0) + (nSten > 0) + (nNmsCtas > 0);
+    return static_cast<int>(pyrFirst.size()) + (nTiles > 0) + (nSten > 0) + 2 * (nNmsCtas > 0);
   }
 
   // Everything after the level-0 images are in place.

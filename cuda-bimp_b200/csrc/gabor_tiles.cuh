@@ -11,8 +11,8 @@
 // and no Hermitian lookup.  For each of the 8 orientations the spectrum is
 // multiplied by that orientation's real Gabor spectrum G_o, inverse
 // transformed as one complex FFT (e + i o) and reduced to |e + i o| on the
-// valid outputs.  The differentiable variant also stores e + i o and the
-// tile's image spectrum for the adjoint.
+// valid outputs.  SAVE_Z also stores e + i o (the line/edge detector's even
+// and odd responses).
 //
 // G_o (64 KB per orientation, L2-resident) is streamed in 16 KB chunks with
 // TMA bulk copies (cp.async.bulk + mbarrier) into a ring of 6 chunk slots:
@@ -285,7 +285,7 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
 template <bool FLT, bool SAVE_Z>
 __global__ void __launch_bounds__(kTileThreads, 1)
 k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ work, int nwork,
-              unsigned int* __restrict__ fault_word, float2* __restrict__ xsave) {
+              unsigned int* __restrict__ fault_word) {
   extern __shared__ float4 smem4[];
   char* base = reinterpret_cast<char*>(smem4);
   float2* W = reinterpret_cast<float2*>(base);
@@ -361,15 +361,6 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         x[k1].y *= pSign;
       }
       tmem_store8(tlane + 16 * k2, x);
-    }
-    if constexpr (SAVE_Z) {   // the adjoint keeps the tile's image spectrum (Hermitian half)
-      if (xsave) {
-        float2* __restrict__ xs = xsave + (size_t)w * kSpecHalf;
-        for (int j = t; j < kSpecHalf; j += kTileThreads) {
-          const int r = j / kXhCols, sl = j - r * kXhCols;
-          xs[j] = *xh_ptr(Xh64, Nyq, r, sl);
-        }
-      }
     }
     tmem_fence_before();
     __syncthreads();   // the Hermitian half in W / slot 4 is dead from here

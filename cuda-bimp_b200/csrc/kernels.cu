@@ -300,52 +300,6 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
   }
 }
 
-// Detection mode, interior blocks: the two pixels of a thread (rows cy0 and
-// cy1 of the window, column cx) through packed FP32x2 arithmetic.  Each lane
-// of a packed operation rounds as a scalar one: the double-stopped term is
-// two fused multiply-adds and the radial term centre - gain * C one, as in
-// stencil_pixel.
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 relu2(float2 v) { return make_float2(fmaxf(v.x, 0.f), fmaxf(v.y, 0.f)); }
-
-template <int PAT>
-__device__ __forceinline__ float2 stencil_pair_d(const float* __restrict__ s_c, const StencilPar& P, int cy0, int cy1,
-                                                 int cx, float gain, float wT, float wR) {
-  float2 D = f2(0.f, 0.f), T = f2(0.f, 0.f), R = f2(0.f, 0.f);
-  const float* a0 = s_c + cy0 * kStW + cx;
-  const float* a1 = s_c + cy1 * kStW + cx;
-  const float2 mhalf = f2(-0.5f, -0.5f), mgain = f2(-gain, -gain);
-#pragma unroll
-  for (int o = 0; o < kNumOri; ++o) {
-    const int o1 = soff<PAT>(P, 0, o), o2 = soff<PAT>(P, 1, o);
-    const float* c0 = a0 + o * (kStH * kStW);
-    const float* c1 = a1 + o * (kStH * kStW);
-    const int tb = 2 * o1 * kStW - 2 * o2;
-    const float2 c = f2(c0[0], c1[0]);
-    const float2 d = __ffma2_rn(mhalf, f2(c0[tb], c1[tb]), __ffma2_rn(mhalf, f2(c0[-tb], c1[-tb]), c));
-    D = __fadd2_rn(D, relu2(d));
-  }
-#pragma unroll
-  for (int o = 0; o < kNumOri; ++o) {
-    const int o1 = soff<PAT>(P, 2, o), o2 = soff<PAT>(P, 3, o);
-    const int op = (o + kNumOri / 2) % kNumOri;
-    const float* c0 = a0 + o * (kStH * kStW);
-    const float* c1 = a1 + o * (kStH * kStW);
-    const float* p0 = a0 + op * (kStH * kStW);
-    const float* p1 = a1 + op * (kStH * kStW);
-    const float2 centre = f2(c0[0], c1[0]);
-    const int tt = -o1 * kStW - o2;
-    T = __fadd2_rn(T, relu2(__fadd2_rn(f2(c0[tt], c1[tt]), f2(-centre.x, -centre.y))));
-    const int h1 = soff<PAT>(P, 4, o), h2 = soff<PAT>(P, 5, o);
-    const int th = h1 * kStW + h2;
-    float2 r = relu2(__ffma2_rn(mgain, f2(p0[th], p1[th]), centre));
-    r = __fadd2_rn(r, __ffma2_rn(mgain, f2(p0[-th], p1[-th]), centre));
-    R = __fadd2_rn(R, relu2(r));
-  }
-  const float2 inhib = __ffma2_rn(f2(wT, wT), T, __fmul2_rn(f2(wR, wR), R));
-  return __fadd2_rn(D, f2(-inhib.x, -inhib.y));
-}
-
 // Output maps of one stencil block.
 struct StencilOut {
   float* D;
@@ -368,17 +322,11 @@ __device__ __forceinline__ float stencil_rows(const float* __restrict__ s_c, con
   constexpr int kRows = kFwY / (NT / 32);
   float D[kRows], S[kRows], T[kRows], R[kRows];
   unsigned int b[kRows];
-  if constexpr (!CHECK && MODE == kStencilD && kRows == 2) {
-    const float2 d = stencil_pair_d<PAT>(s_c, P, ly0 + kHalo, ly0 + NT / 32 + kHalo, lx + kHalo, gain, wT, wR);
-    D[0] = d.x;
-    D[1] = d.y;
-  } else {
 #pragma unroll
-    for (int i = 0; i < kRows; ++i) {
-      const int ly = ly0 + (NT / 32) * i;
-      stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i],
-                                      R[i], b[i]);
-    }
+  for (int i = 0; i < kRows; ++i) {
+    const int ly = ly0 + (NT / 32) * i;
+    stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i], R[i],
+                                    b[i]);
   }
   float dmax = -INFINITY;
 #pragma unroll
@@ -843,28 +791,15 @@ k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int
 }
 
 // ---------------------------------------------------------------------------
-// single-pass NMS: decisions, the per-image chained row prefix, records
+// NMS in two launches: decisions and counts, then the records
 // ---------------------------------------------------------------------------
-// One CTA per group of up to kNmsRowsPerCta candidate rows of one image (one
-// warp per row).  Each warp decides its row (strict 8-neighbour maximum above
-// the threshold) and stores the row's decision words; the CTA publishes its
-// keypoint count, learns the count of all earlier rows of its image from its
-// predecessors' published values (decoupled look-back: a predecessor's
-// inclusive prefix ends the walk, its bare count adds to it), publishes its
-// own inclusive prefix, and the warps write their rows' records.  The image's
-// last CTA writes the image total.  Every wait is bounded: on expiry the CTA
-// sets bit 2 of *fault and counts the missing predecessors as empty.
-constexpr unsigned long long kNmsAgg = 1ull << 62, kNmsInc = 2ull << 62;
-
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
+// The candidate rows of an image are grouped kNmsRowsPerCta to a CTA (one
+// warp per row), the same grouping in both kernels.  k_nms_decide stores each
+// row's decision words and the CTA's keypoint count; k_nms_emit gives each CTA
+// its image-relative offset as the sum of the counts of the image's earlier
+// CTAs (one parallel read of at most a few hundred ints), the rows their
+// offsets within the CTA from the popcounts of their words, and writes the
+// records.  No CTA waits for another.
 // Spreads bit i of an 8-bit value to bit 4 i.
 __device__ __forceinline__ unsigned int spread4(unsigned int x) {
   x &= 0xffu;
@@ -974,67 +909,68 @@ __device__ __forceinline__ int nms_decide_row(const ScaleDev* __restrict__ sd, i
 }
 
 __global__ void __launch_bounds__(32 * kNmsRowsPerCta, 4)
-k_nms_fused(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, const NmsCta* __restrict__ ctas,
-            unsigned long long* __restrict__ status, int* __restrict__ imageTotals, const KpOut* __restrict__ outs,
-            unsigned int* __restrict__ fault_word) {
+k_nms_decide(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, const NmsCta* __restrict__ ctas,
+             int* __restrict__ ctaCount) {
   __shared__ int s_cnt[kNmsRowsPerCta];
-  __shared__ int s_base;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const NmsCta cta = ctas[blockIdx.x];
+  griddep_launch_dependents();
   griddep_wait();   // the summed maps and their maxima come from the previous kernel
-  int2 item = make_int2(0, 0);
   int cnt = 0;
   if (warp < cta.nRows) {
-    item = rows[cta.rowStart + warp];
+    const int2 item = rows[cta.rowStart + warp];
     cnt = nms_decide_row(sds + item.x, item.y, lane);
   }
   if (lane == 0) s_cnt[warp] = cnt;
   __syncthreads();
-  if (warp == 0) {
-    int total = lane < kNmsRowsPerCta ? s_cnt[lane] : 0;
+  if (threadIdx.x == 0) {
+    int total = 0;
+    for (int w = 0; w < kNmsRowsPerCta; ++w) total += s_cnt[w];
+    ctaCount[blockIdx.x] = total;
+  }
+}
+
+__global__ void __launch_bounds__(32 * kNmsRowsPerCta)
+k_nms_emit(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, const NmsCta* __restrict__ ctas,
+           const int* __restrict__ ctaCount, int* __restrict__ imageTotals, const KpOut* __restrict__ outs) {
+  __shared__ int s_cnt[kNmsRowsPerCta];
+  __shared__ int s_part[kNmsRowsPerCta];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const NmsCta cta = ctas[blockIdx.x];
+  int2 item = make_int2(0, 0);
+  int first = 0, nch = 0;
+  griddep_wait();   // the decision words and counts come from k_nms_decide
+  // this row's keypoint count from its decision words
+  int cnt = 0;
+  if (warp < cta.nRows) {
+    item = rows[cta.rowStart + warp];
+    const ScaleDev* sd = sds + item.x;
+    nms_row_words(sd, first, nch);
+    const unsigned int* mask = sd->nmsMask + (size_t)item.y * sd->nmsChunks;
+    for (int c = lane; c < nch; c += 32) cnt += __popc(mask[c]);
 #pragma unroll
-    for (int m = 16; m > 0; m >>= 1) total += __shfl_xor_sync(0xffffffffu, total, m);
-    const int b = blockIdx.x, first = cta.firstCta;
-    if (b != first && lane == 0) st_release_u64(status + b, kNmsAgg | (unsigned int)total);
-    unsigned long long prefix = 0;
-    int j = b - 1, spins = 0;
-    while (j >= first) {
-      const int idx = j - lane;
-      const unsigned long long v = idx >= first ? ld_acquire_u64(status + idx) : kNmsInc;
-      const unsigned int flag = (unsigned int)(v >> 62);
-      const unsigned int inc = __ballot_sync(0xffffffffu, flag == 2u);
-      const unsigned int none = __ballot_sync(0xffffffffu, flag == 0u);
-      const int L = inc ? __ffs(inc) - 1 : 31;
-      const unsigned int upto = L == 31 ? 0xffffffffu : ((2u << L) - 1u);
-      if (none & upto) {
-        if (++spins > (1 << 20)) {   // a predecessor never published: give up, count it as empty
-          if (lane == 0) atomicOr(fault_word, 4u);
-          break;
-        }
-        __nanosleep(64);
-        continue;
-      }
-      unsigned long long val = lane <= L ? (v & 0xffffffffull) : 0ull;
+    for (int m = 16; m > 0; m >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, m);
+  }
+  // the counts of the image's earlier CTAs
+  int before = 0;
+  for (int i = cta.firstCta + t; i < (int)blockIdx.x; i += blockDim.x) before += ctaCount[i];
 #pragma unroll
-      for (int m = 16; m > 0; m >>= 1) val += __shfl_xor_sync(0xffffffffu, val, m);
-      prefix += val;
-      if (inc) break;
-      j -= 32;
-    }
-    if (lane == 0) {
-      st_release_u64(status + b, kNmsInc | (unsigned int)(prefix + total));
-      s_base = (int)prefix;
-      if (cta.last) imageTotals[cta.image] = (int)(prefix + total);
-    }
+  for (int m = 16; m > 0; m >>= 1) before += __shfl_xor_sync(0xffffffffu, before, m);
+  if (lane == 0) {
+    s_cnt[warp] = cnt;
+    s_part[warp] = before;
   }
   __syncthreads();
+  int base = 0, total = 0;
+  for (int w = 0; w < kNmsRowsPerCta; ++w) {
+    base += s_part[w];
+    total += s_cnt[w];
+  }
+  if (cta.last && t == 0) imageTotals[cta.image] = base + total;
   if (warp < cta.nRows && cnt > 0) {
+    for (int w = 0; w < warp; ++w) base += s_cnt[w];
     const ScaleDev* sd = sds + item.x;
     const KpOut out = outs[cta.image];
-    int base = s_base;
-    for (int w = 0; w < warp; ++w) base += s_cnt[w];
-    int first, nch;
-    nms_row_words(sd, first, nch);
     if (base < out.capacity)
       nms_write_words(sd, out, sd->off + 1 + item.y, sd->nmsMask + (size_t)item.y * sd->nmsChunks, nch, 32 * first,
                       base, lane);
@@ -1237,7 +1173,7 @@ void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int g
     launch_ex(k_gabor_tiles_ws<false>, grid, kTileThreads, kWsSmem, s, pdl, d_sd, d_work, nwork);
   else
     launch_ex(k_gabor_tiles<false, false>, grid, kTileThreads, gabor_smem_bytes(), s, pdl, d_sd, d_work, nwork,
-              d_fault, static_cast<float2*>(nullptr));
+              d_fault);
 }
 void launch_gabor_flt(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
                       cudaStream_t s, bool pipelined) {
@@ -1245,12 +1181,12 @@ void launch_gabor_flt(const ScaleDev* d_sd, const TileWork* d_work, int nwork, u
   if (pipelined)
     k_gabor_tiles_ws<true><<<nwork, kTileThreads, kWsSmem, s>>>(d_sd, d_work, nwork);
   else
-    k_gabor_tiles<true, false><<<nwork, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault, nullptr);
+    k_gabor_tiles<true, false><<<nwork, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
 }
 void launch_gabor_keep_z(const ScaleDev* d_sd, const TileWork* d_work, int nwork, unsigned int* d_fault,
                          cudaStream_t s) {
   if (nwork > 0)
-    k_gabor_tiles<false, true><<<nwork, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault, nullptr);
+    k_gabor_tiles<false, true><<<nwork, kTileThreads, gabor_smem_bytes(), s>>>(d_sd, d_work, nwork, d_fault);
 }
 void launch_detect_le(const ScaleDev* d_sd, int dataW, int dataH, const float* d_ch, int chLd, float* d_result,
                       float* d_ori, int8_t* d_type, int ld, cudaStream_t s) {
@@ -1290,12 +1226,11 @@ void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigne
   else
     launch_ex(k_stencil<kStencilD>, grid, kStThreads, stencil_smem_bytes(), s, pdl, d_sd, d_work, nwork, d_fault);
 }
-void launch_nms_fused(const ScaleDev* d_sd, const int2* d_rows, const NmsCta* d_ctas, int nctas,
-                      unsigned long long* d_status, int* d_totals, const KpOut* d_outs, unsigned int* d_fault,
-                      cudaStream_t s, bool pdl) {
-  if (nctas > 0)
-    launch_ex(k_nms_fused, nctas, 32 * kNmsRowsPerCta, 0, s, pdl, d_sd, d_rows, d_ctas, d_status, d_totals, d_outs,
-              d_fault);
+void launch_nms_two_pass(const ScaleDev* d_sd, const int2* d_rows, const NmsCta* d_ctas, int nctas, int* d_ctaCount,
+                         int* d_totals, const KpOut* d_outs, cudaStream_t s, bool pdl) {
+  if (nctas <= 0) return;
+  launch_ex(k_nms_decide, nctas, 32 * kNmsRowsPerCta, 0, s, pdl, d_sd, d_rows, d_ctas, d_ctaCount);
+  launch_ex(k_nms_emit, nctas, 32 * kNmsRowsPerCta, 0, s, pdl, d_sd, d_rows, d_ctas, d_ctaCount, d_totals, d_outs);
 }
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,

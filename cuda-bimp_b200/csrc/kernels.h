@@ -74,10 +74,9 @@ enum StencilMode { kStencilD = 0, kStencilDS = 1, kStencilAdj = 2 };
 // *d_fault.
 void launch_stencil(const ScaleDev* d_sd, const int2* d_work, int nwork, unsigned int* d_fault, cudaStream_t s,
                     int mode = kStencilD, bool pdl = false);
-// Single-pass NMS (decisions, chained per-image prefix, records): one CTA per
-// group of up to kNmsRowsPerCta candidate rows of one image.  d_status
-// (nctas words) must be zero at launch; an expired wait sets bit 2 of
-// *d_fault.
+// NMS in two launches (k_nms_decide, k_nms_emit): one CTA per group of up to
+// kNmsRowsPerCta candidate rows of one image; d_ctaCount holds nctas ints
+// (written by the first kernel, read by the second).
 constexpr int kNmsRowsPerCta = 8;
 struct NmsCta {
   int rowStart;   // first entry of the CTA's rows in the row list
@@ -86,9 +85,8 @@ struct NmsCta {
   int image;
   int last;       // 1: the image's last CTA, which writes the image total
 };
-void launch_nms_fused(const ScaleDev* d_sd, const int2* d_rows, const NmsCta* d_ctas, int nctas,
-                      unsigned long long* d_status, int* d_totals, const KpOut* d_outs, unsigned int* d_fault,
-                      cudaStream_t s, bool pdl = false);
+void launch_nms_two_pass(const ScaleDev* d_sd, const int2* d_rows, const NmsCta* d_ctas, int nctas, int* d_ctaCount,
+                         int* d_totals, const KpOut* d_outs, cudaStream_t s, bool pdl = false);
 void launch_nms(const ScaleDev* d_sd, const int2* d_rows, int nrows, int* d_counts, int* d_offsets,
                 const int* d_imageRowStart, int nImages, int* d_totals, const KpOut* d_outs,
                 cudaStream_t s);
