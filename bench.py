@@ -303,7 +303,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         outs = (L.KeyPointC * cap)()
         n = C.c_int()
         d2h = []
-        depth = 3
+        depth = args.depth
         pl = api.Pipeline(W_HD, H_HD, lam, depth=depth, capacity=cap)
 
         def pop():
@@ -679,6 +679,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--depth", type=int, default=4, help="frames in flight of the end-to-end measurement")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")

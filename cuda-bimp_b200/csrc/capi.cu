@@ -72,6 +72,16 @@ int round_half_away(double v) {
   return static_cast<int>(v >= 0 ? std::floor(v + 0.5) : -std::floor(-v + 0.5));
 }
 
+// Programmatic dependent launch along the detection kernels: on unless
+// BIMP_PDL=0 (kept switchable to measure both).
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("BIMP_PDL");
+    return !(e && std::strcmp(e, "0") == 0);
+  }();
+  return on;
+}
+
 // Bump allocator over one device allocation.
 struct Arena {
   size_t size = 0;
@@ -319,11 +329,16 @@ struct Engine {
         const int nbx = (s.dataW + 31) / 32, nby = (s.dataH + kStencilBlockH - 1) / kStencilBlockH;
         for (int b = 0; b < nbx * nby; ++b) sten.push_back(make_int2(entry, b));
         const int yEnd = std::min(s.dataH - s.off - 1, s.dataH - 2);
-        for (int y = s.off + 1; y <= yEnd; ++y) rows.push_back(make_int2(entry, y - s.off - 1));
         // keypoint-decision words: 32-pixel-aligned words covering a row's
         // candidate pixels (off, xEnd)
         const int xEnd = std::min(s.dataW - s.off, s.dataW - 1);
         d.nmsChunks = xEnd > s.off + 1 ? ((xEnd - 1) >> 5) - ((s.off + 1) >> 5) + 1 : 0;
+        // the NMS work: each candidate row in 512-pixel-aligned pieces,
+        // {entry, row | piece << 16}
+        if (d.nmsChunks > 0)
+          for (int y = s.off + 1; y <= yEnd; ++y)
+            for (int pc = (s.off + 1) >> 9; pc <= (xEnd - 1) >> 9; ++pc)
+              rows.push_back(make_int2(entry, (y - s.off - 1) | (pc << 16)));
         maskWords.push_back((size_t)std::max(0, yEnd - s.off) * d.nmsChunks);
         sds.push_back(d);
       }
@@ -489,13 +504,13 @@ struct Engine {
       // stages 1-3 follow the previous stage's kernel with programmatic
       // dependent launch (each waits in the kernel for its predecessor)
       case 1:
-        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s, tilePipelined, true);
+        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s, tilePipelined, pdl_enabled());
         break;
       case 2:
-        if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD, true);
+        if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD, pdl_enabled());
         break;
       case 3:
-        launch_nms_two_pass(d_sd, d_rows, d_nmsCtas, nNmsCtas, d_nmsCount, d_totals, d_outs, s, true);
+        launch_nms_two_pass(d_sd, d_rows, d_nmsCtas, nNmsCtas, d_nmsCount, d_totals, d_outs, s, pdl_enabled());
         break;
       default:
         return fail(BIMP_ERR_INVALID, "unknown stage");

@@ -793,13 +793,14 @@ k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int
 // ---------------------------------------------------------------------------
 // NMS in two launches: decisions and counts, then the records
 // ---------------------------------------------------------------------------
-// The candidate rows of an image are grouped kNmsRowsPerCta to a CTA (one
-// warp per row), the same grouping in both kernels.  k_nms_decide stores each
-// row's decision words and the CTA's keypoint count; k_nms_emit gives each CTA
-// its image-relative offset as the sum of the counts of the image's earlier
-// CTAs (one parallel read of at most a few hundred ints), the rows their
-// offsets within the CTA from the popcounts of their words, and writes the
-// records.  No CTA waits for another.
+// The candidate rows of an image are cut into pieces of up to 512 pixels,
+// in (scale, row, x) order, and grouped kNmsRowsPerCta to a CTA (one warp per
+// piece), the same grouping in both kernels.  k_nms_decide stores each
+// piece's decision words and the CTA's keypoint count; k_nms_emit gives each
+// CTA its image-relative offset as the sum of the counts of the image's
+// earlier CTAs (one parallel read of at most a few thousand ints), the pieces
+// their offsets within the CTA from the popcounts of their words, and writes
+// the records.  No CTA waits for another.
 // Spreads bit i of an 8-bit value to bit 4 i.
 __device__ __forceinline__ unsigned int spread4(unsigned int x) {
   x &= 0xffu;
@@ -819,8 +820,8 @@ __device__ __forceinline__ void nms_row_words(const ScaleDev* __restrict__ sd, i
   nch = xEnd > off + 1 ? ((xEnd - 1) >> 5) - first + 1 : 0;
 }
 
-// One warp: the aligned decision words of candidate row iy (stored to the
-// row's mask words) and its keypoint count.  A segment is 128 pixels, four per
+// One warp: the aligned decision words of one piece of candidate row iy
+// (stored to the row's mask words) and its keypoint count.  A segment is 128 pixels, four per
 // lane: the lane reads them and the rows above and below as 16-byte vectors
 // (the row pitch is a multiple of 32 floats), two segments per round, so a
 // row costs about one memory latency per 256 pixels; the neighbours across
@@ -828,7 +829,11 @@ __device__ __forceinline__ void nms_row_words(const ScaleDev* __restrict__ sd, i
 // per round keep the kernel within 64 registers, so that every CTA of a 1080p
 // detection is resident at once (four per SM).
 constexpr int kNmsSegBatch = 2;
-__device__ __forceinline__ int nms_decide_row(const ScaleDev* __restrict__ sd, int iy, int lane) {
+// A piece is the part of a candidate row inside one 512-pixel-aligned span
+// (four segments, sixteen decision words), so that a long row is decided by
+// several warps at once.
+constexpr int kNmsPieceShift = 9;
+__device__ __forceinline__ int nms_decide_piece(const ScaleDev* __restrict__ sd, int iy, int piece, int lane) {
   const int off = sd->off;
   const int y = off + 1 + iy;
   const int W = sd->dataW;
@@ -843,7 +848,8 @@ __device__ __forceinline__ int nms_decide_row(const ScaleDev* __restrict__ sd, i
   nms_row_words(sd, first, nch);
   unsigned int* __restrict__ mask = sd->nmsMask + (size_t)iy * sd->nmsChunks;
   if (nch <= 0) return 0;
-  const int seg0 = (off + 1) >> 7, seg1 = (xEnd - 1) >> 7;
+  const int seg0 = max((off + 1) >> 7, piece << (kNmsPieceShift - 7));
+  const int seg1 = min((xEnd - 1) >> 7, ((piece + 1) << (kNmsPieceShift - 7)) - 1);
   int n = 0;
   for (int sb = seg0; sb <= seg1; sb += kNmsSegBatch) {
     float4 c[kNmsSegBatch], u[kNmsSegBatch], d[kNmsSegBatch];
@@ -918,8 +924,8 @@ k_nms_decide(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, co
   griddep_wait();   // the summed maps and their maxima come from the previous kernel
   int cnt = 0;
   if (warp < cta.nRows) {
-    const int2 item = rows[cta.rowStart + warp];
-    cnt = nms_decide_row(sds + item.x, item.y, lane);
+    const int2 item = rows[cta.rowStart + warp];   // {entry, row | piece << 16}
+    cnt = nms_decide_piece(sds + item.x, item.y & 0xffff, item.y >> 16, lane);
   }
   if (lane == 0) s_cnt[warp] = cnt;
   __syncthreads();
@@ -938,16 +944,21 @@ k_nms_emit(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, cons
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const NmsCta cta = ctas[blockIdx.x];
   int2 item = make_int2(0, 0);
-  int first = 0, nch = 0;
+  int first = 0, wlo = 0, whi = 0, iy = 0;
   griddep_wait();   // the decision words and counts come from k_nms_decide
-  // this row's keypoint count from its decision words
+  // this piece's keypoint count from its decision words
   int cnt = 0;
   if (warp < cta.nRows) {
-    item = rows[cta.rowStart + warp];
+    item = rows[cta.rowStart + warp];   // {entry, row | piece << 16}
+    iy = item.y & 0xffff;
+    const int piece = item.y >> 16;
     const ScaleDev* sd = sds + item.x;
+    int nch;
     nms_row_words(sd, first, nch);
-    const unsigned int* mask = sd->nmsMask + (size_t)item.y * sd->nmsChunks;
-    for (int c = lane; c < nch; c += 32) cnt += __popc(mask[c]);
+    wlo = max(0, (piece << (kNmsPieceShift - 5)) - first);
+    whi = min(nch, ((piece + 1) << (kNmsPieceShift - 5)) - first);
+    const unsigned int* mask = sd->nmsMask + (size_t)iy * sd->nmsChunks;
+    for (int c = wlo + lane; c < whi; c += 32) cnt += __popc(mask[c]);
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, m);
   }
@@ -972,8 +983,8 @@ k_nms_emit(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, cons
     const ScaleDev* sd = sds + item.x;
     const KpOut out = outs[cta.image];
     if (base < out.capacity)
-      nms_write_words(sd, out, sd->off + 1 + item.y, sd->nmsMask + (size_t)item.y * sd->nmsChunks, nch, 32 * first,
-                      base, lane);
+      nms_write_words(sd, out, sd->off + 1 + iy, sd->nmsMask + (size_t)iy * sd->nmsChunks + wlo, whi - wlo,
+                      32 * (first + wlo), base, lane);
   }
 }
 
