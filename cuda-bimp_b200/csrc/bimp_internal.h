@@ -96,10 +96,13 @@ constexpr int kNumOffsetSets = 2;
   }
 constexpr int kOffsetSets[kNumOffsetSets][6][8] = BIMP_OFFSET_SETS;
 
-// One unit of tiled-FFT work: tile `tile` of descriptor `entry`.
+// One unit of tiled-FFT work: orientations [oBegin, oEnd) of tile `tile` of
+// descriptor `entry`.  oBegin == oEnd is an empty slot of a padded plan.
 struct TileWork {
   int entry;
   int tile;
+  int oBegin = 0;
+  int oEnd = kNumOri;
 };
 
 // Host-side description of one scale (geometry + bank).

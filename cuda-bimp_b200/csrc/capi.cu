@@ -122,8 +122,9 @@ struct Engine {
   std::vector<std::vector<int>> lvlW, lvlH, lvlP;
   std::vector<ScaleDev> h_sd;
   ScaleDev* d_sd = nullptr;
-  TileWork* d_tiles = nullptr;
-  int nTiles = 0;
+  TileWork* d_tiles = nullptr;   // the tile kernel's work list
+  int nTiles = 0;                 // tiles of the current plan
+  int nWork = 0;                  // entries of the work list
   int2* d_sten = nullptr;
   int nSten = 0;
   int2* d_rows = nullptr;
@@ -142,7 +143,8 @@ struct Engine {
   std::vector<size_t> imgKpOffset;           // internal keypoint buffers (batch)
   float* d_kpInternal = nullptr;
   int kpCapInternal = 0;
-  int tileGrid = 0;    // CTAs of the tile kernel (each loops over tiles)
+  int tileGrid = 0;    // CTAs of the tile kernel (each walks its items of the work list)
+  int tileGridReq = 0; // the plan's grid: 0 one CTA per tile, > 0 the split plan's CTA bound
   bool tilePipelined = false;   // the warp-specialised tile kernel (every scale's V fits its row buffers)
   int tileCap = 0;     // capacity of d_tiles (the largest tile plan)
   int tilePolicy = 0, tileOrder = 0;
@@ -158,6 +160,65 @@ struct Engine {
     const int vmax = kTile - 2 * kX;
     const int v32 = vmax / 32 * 32;
     return (policy == 1 && v32 * 4 >= vmax * 3) ? v32 : vmax;
+  }
+  // Balanced plan for a persistent grid of `grid` CTAs.  The (tile,
+  // orientation) pairs, tile by tile in plan order, are cut into at most
+  // `grid` contiguous runs of about equal cost; a run becomes one work item
+  // per tile it touches (a tile cut between two CTAs is transformed forward by
+  // both).  Costs per pass, from the kernel's instruction counts per thread:
+  // an orientation 0.5 + 0.005 V (product and inverse y-passes on all 128
+  // columns, inverse x-passes and magnitudes on V rows), the forward
+  // transform 0.8.  The smallest run bound that fits in `grid` runs is found
+  // by bisection.  Item k of CTA b is placed at index k * grid + b (the kernel
+  // strides its work list by the grid); CTAs with fewer items get empty ones.
+  // *usedGrid receives the number of CTAs with work.
+  static std::vector<TileWork> split_plan(const std::vector<TileWork>& tiles, const std::vector<ScaleDev>& sds,
+                                          int grid, int* usedGrid) {
+    const double kFwd = 0.8;
+    std::vector<double> ori(tiles.size());
+    double total = 0.0, worst = 0.0;
+    for (size_t i = 0; i < tiles.size(); ++i) {
+      ori[i] = 0.5 + 0.005 * sds[tiles[i].entry].V;
+      total += kNumOri * ori[i] + kFwd;
+      worst = std::max(worst, ori[i] + kFwd);
+    }
+    // greedy runs of the pair sequence under bound tau (a pair joins the
+    // current run while the run stays within tau); returns the run count
+    auto cut = [&](double tau, std::vector<std::vector<TileWork>>* runs) {
+      int n = 0;
+      double acc = 0.0;
+      for (size_t i = 0; i < tiles.size(); ++i)
+        for (int o = 0; o < kNumOri;) {
+          if (n == 0 || (acc + kFwd + ori[i] > tau && acc > 0.0)) {
+            ++n;
+            acc = 0.0;
+            if (runs) runs->emplace_back();
+          }
+          acc += kFwd + ori[i];   // the item's forward transform and first orientation
+          int k = 1 + static_cast<int>(std::floor(std::max(0.0, tau - acc) / ori[i]));
+          k = std::min(k, kNumOri - o);
+          acc += (k - 1) * ori[i];
+          if (runs) runs->back().push_back({tiles[i].entry, tiles[i].tile, o, o + k});
+          o += k;
+        }
+      return n;
+    };
+    double lo = std::max(worst, total / std::max(1, grid)) * 0.999, hi = total + worst;
+    for (int it = 0; it < 60 && hi - lo > 1e-6 * hi; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (cut(mid, nullptr) <= grid) hi = mid;
+      else lo = mid;
+    }
+    std::vector<std::vector<TileWork>> runs;
+    cut(hi, &runs);
+    const int g = static_cast<int>(runs.size());
+    size_t depth = 0;
+    for (auto& r : runs) depth = std::max(depth, r.size());
+    std::vector<TileWork> out(depth * (size_t)g, TileWork{0, 0, 0, 0});
+    for (int b = 0; b < g; ++b)
+      for (size_t k = 0; k < runs[b].size(); ++k) out[k * (size_t)g + b] = runs[b][k];
+    *usedGrid = g;
+    return out;
   }
   static std::vector<TileWork> tile_plan(std::vector<ScaleDev>& sds, int policy, int order) {
     std::vector<std::vector<TileWork>> per(sds.size());
@@ -181,17 +242,30 @@ struct Engine {
     }
     return out;
   }
+  // The tile kernel's work list of a plan: one item per tile (grid <= 0, one
+  // CTA each) or the balanced split plan for `grid` persistent CTAs.
+  static std::vector<TileWork> work_list(std::vector<ScaleDev>& sds, int policy, int order, int grid, int* nTilesOut,
+                                         int* gridOut) {
+    std::vector<TileWork> tiles = tile_plan(sds, policy, order);
+    *nTilesOut = static_cast<int>(tiles.size());
+    *gridOut = static_cast<int>(tiles.size());
+    if (grid > 0 && !tiles.empty()) return split_plan(tiles, sds, grid, gridOut);
+    return tiles;
+  }
   int retile(int policy, int order, int grid, int kernel = 0) {
     std::vector<ScaleDev> sds = h_sd;
-    const std::vector<TileWork> tiles = tile_plan(sds, policy, order);
-    if ((int)tiles.size() > tileCap) return fail(BIMP_ERR_INVALID, "tile plan larger than its buffer");
+    int nt = 0, g = 0;
+    const std::vector<TileWork> work = work_list(sds, policy, order, grid, &nt, &g);
+    if ((int)work.size() > tileCap) return fail(BIMP_ERR_INVALID, "tile plan larger than its buffer");
     BIMP_CUDA(cudaSetDevice(device));
     BIMP_CUDA(cudaMemcpy(d_sd, sds.data(), sizeof(ScaleDev) * sds.size(), cudaMemcpyHostToDevice));
-    if (!tiles.empty())
-      BIMP_CUDA(cudaMemcpy(d_tiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice));
+    if (!work.empty())
+      BIMP_CUDA(cudaMemcpy(d_tiles, work.data(), sizeof(TileWork) * work.size(), cudaMemcpyHostToDevice));
     h_sd = sds;
-    nTiles = static_cast<int>(tiles.size());
-    tileGrid = grid > 0 ? std::min(grid, nTiles) : nTiles;
+    nTiles = nt;
+    nWork = static_cast<int>(work.size());
+    tileGrid = g;
+    tileGridReq = grid > 0 ? grid : 0;
     tilePolicy = policy;
     tileOrder = order;
     tilePipelined = kernel == 1 && pipelined_fits();
@@ -375,19 +449,30 @@ struct Engine {
       pyrMaxH.push_back(mh);
     }
     nTiles = static_cast<int>(tiles.size());
-    // One CTA per tile by default.  BIMP_TILE_GRID caps the grid so that each
-    // CTA walks several tiles (used by the tests of the persistent loop).
+    // Default tile plan: the balanced split over one persistent CTA per SM.
+    // BIMP_TILE_GRID=g uses g CTAs instead (g <= 0: one CTA per tile).
+    BIMP_CUDA(cudaSetDevice(dev));
+    const int sms = num_sms();
+    int defGrid = sms;
+    if (const char* g = std::getenv("BIMP_TILE_GRID")) defGrid = std::atoi(g);
+    std::vector<TileWork> work = tiles;
     tileGrid = nTiles;
-    if (const char* g = std::getenv("BIMP_TILE_GRID")) {
-      const int cap = std::atoi(g);
-      if (cap > 0) tileGrid = std::min(tileGrid, cap);
-    }
+    if (defGrid > 0 && !tiles.empty()) work = split_plan(tiles, sds, defGrid, &tileGrid);
+    nWork = static_cast<int>(work.size());
+    tileGridReq = std::max(0, defGrid);
     nSten = static_cast<int>(sten.size());
     nRows = static_cast<int>(rows.size());
     const size_t offSd = a.reserve(sizeof(ScaleDev) * sds.size());
     {   // the tile buffer holds the largest plan the autotuner may choose
-      std::vector<ScaleDev> tmp = sds;
-      tileCap = static_cast<int>(std::max(tiles.size(), tile_plan(tmp, 1, 0).size()));
+      tileCap = nWork;
+      const int grids[4] = {0, sms, 2 * sms, defGrid};
+      for (int policy = 0; policy < 2; ++policy)
+        for (int order = 0; order < 2; ++order)
+          for (int g : grids) {
+            std::vector<ScaleDev> tmp = sds;
+            int nt = 0, ng = 0;
+            tileCap = std::max(tileCap, static_cast<int>(work_list(tmp, policy, order, g, &nt, &ng).size()));
+          }
     }
     const size_t offTiles = a.reserve(sizeof(TileWork) * std::max<size_t>(1, (size_t)tileCap));
     const size_t offSten = a.reserve(sizeof(int2) * std::max<size_t>(1, sten.size()));
@@ -469,8 +554,8 @@ struct Engine {
     for (auto& s : bank) { s.spectrum.clear(); s.spectrum.shrink_to_fit(); }
     BIMP_CUDA(cudaMemcpy(d_sd, sds.data(), sizeof(ScaleDev) * sds.size(), cudaMemcpyHostToDevice));
     BIMP_CUDA(cudaMemcpy(base + offMaps, maps.data(), kTensorMapBytes * sds.size(), cudaMemcpyHostToDevice));
-    if (!tiles.empty())
-      BIMP_CUDA(cudaMemcpy(d_tiles, tiles.data(), sizeof(TileWork) * tiles.size(), cudaMemcpyHostToDevice));
+    if (!work.empty())
+      BIMP_CUDA(cudaMemcpy(d_tiles, work.data(), sizeof(TileWork) * work.size(), cudaMemcpyHostToDevice));
     if (!sten.empty())
       BIMP_CUDA(cudaMemcpy(d_sten, sten.data(), sizeof(int2) * sten.size(), cudaMemcpyHostToDevice));
     if (!rows.empty())
@@ -504,7 +589,7 @@ struct Engine {
       // stages 1-3 follow the previous stage's kernel with programmatic
       // dependent launch (each waits in the kernel for its predecessor)
       case 1:
-        if (nTiles > 0) launch_gabor(d_sd, d_tiles, nTiles, tileGrid, d_fault, s, tilePipelined, pdl_enabled());
+        if (nWork > 0) launch_gabor(d_sd, d_tiles, nWork, tileGrid, d_fault, s, tilePipelined, pdl_enabled());
         break;
       case 2:
         if (nSten > 0) launch_stencil(d_sd, d_sten, nSten, d_fault, s, kStencilD, pdl_enabled());
@@ -1107,7 +1192,7 @@ int bimp_batch_autotune(bimp_batch* b, void* stream, int reps, bimp_tile_plan* c
           }
           float ms = 0.f;
           cudaEventElapsedTime(&ms, e0, e1);
-          const bimp_tile_plan pl{policy, order, b->eng.tilePipelined ? 1 : 0, b->eng.tileGrid, b->eng.nTiles,
+          const bimp_tile_plan pl{policy, order, b->eng.tilePipelined ? 1 : 0, b->eng.tileGridReq, b->eng.nTiles,
                                   ms / reps};
           if (count < max_tried) tried[count] = pl;
           ++count;
@@ -1116,7 +1201,7 @@ int bimp_batch_autotune(bimp_batch* b, void* stream, int reps, bimp_tile_plan* c
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != BIMP_OK) return rc;
-  rc = b->eng.retile(best.policy, best.order, best.grid >= best.tiles ? 0 : best.grid, best.kernel);
+  rc = b->eng.retile(best.policy, best.order, best.grid, best.kernel);
   if (rc == BIMP_OK) rc = capture_batch(b);
   if (rc != BIMP_OK) return rc;
   if (chosen) *chosen = best;

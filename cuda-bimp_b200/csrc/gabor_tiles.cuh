@@ -8,7 +8,9 @@
 // 2 py and 2 py + 1 the real and imaginary parts of row py.  Thread t reads
 // only lane t mod 128, which is the lane its warp may access, so the spectrum
 // product pass of every orientation fetches its 8 values with one tcgen05.ld
-// and no Hermitian lookup.  For each of the 8 orientations the spectrum is
+// and no Hermitian lookup.  For each orientation of the work item (all 8,
+// or a run of them where the plan splits a tile between CTAs, each of which
+// then transforms the tile forward) the spectrum is
 // multiplied by that orientation's real Gabor spectrum G_o, inverse
 // transformed as one complex FFT (e + i o) and reduced to |e + i o| on the
 // valid outputs.  SAVE_Z also stores e + i o (the line/edge detector's even
@@ -334,6 +336,8 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
 
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const TileWork item = work[w];
+    const int oB = item.oBegin, oE = item.oEnd;
+    if (oB >= oE) continue;   // empty slot of a padded plan (the same item in every thread)
     const ScaleDev* sd = sds + item.entry;
     const int kX = sd->kX, V = sd->V;
     const int ty = item.tile / sd->tilesX, tx = item.tile - ty * sd->tilesX;
@@ -341,10 +345,11 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     const float* __restrict__ G0 = sd->G;
 
     __syncthreads();   // previous tile finished with every buffer
-    if (t == 0) {      // orientation 0's four chunks into slots 0..3
+    if (t == 0) {      // orientation oB's four chunks into slots 0..3
       fence_proxy_async();
-      for (int c = 0; c < 4; ++c) bulk_load(gdst0 + c * kGChunkFloats * 4, G0 + c * kGChunkFloats, kGChunkFloats * 4,
-                                            bar0 + 8 * c);
+      for (int c = 0; c < 4; ++c)
+        bulk_load(gdst0 + c * kGChunkFloats * 4, G0 + (size_t)(4 * oB + c) * kGChunkFloats, kGChunkFloats * 4,
+                  bar0 + 8 * c);
     }
     tile_forward_spectrum<FLT>(sd, R0, C0, W, Xh64, Nyq, tw, rmap, cmap, t);
     // full spectrum into TMEM: this thread writes the rows py = 8 k2 + k1,
@@ -382,14 +387,15 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     float* __restrict__ C0p = sd->C;
     float2* __restrict__ Z0p = sd->Z;
     const long long cStride = sd->cStride;
-    for (int o = 0; o < kNumOri; ++o) {
+    for (int o = oB; o < oE; ++o) {
       float* __restrict__ Cout = C0p + (size_t)o * cStride;
+      const int r = o - oB;   // position in the item: chunk 4 r + q of the item sits in ring slot (4 r + q) mod 6
       // I1: y-dim pass B' with the spectrum product Z = X * G; quarter q
-      // uses chunk 4 o + q (G rows py in [32 q, 32 q + 32))
+      // uses chunk 4 o + q of G (rows py in [32 q, 32 q + 32))
 #pragma unroll 1
       for (int q = 0; q < 4; ++q) {
         const int k2 = h + 4 * q;
-        const int slot = (4 * o + q) % kGSlots;
+        const int slot = (4 * r + q) % kGSlots;
         float2 v[8];
         tmem_load8(tlane + 16 * k2, v);
         if (!mbar_wait(bar0 + 8 * slot, (ph >> slot) & 1)) fault = true;
@@ -409,10 +415,10 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
       // consumed, and (previous orientation) no thread still reads W
       __syncthreads();
       tmem_fence_after();
-      if (t == 0 && o + 1 < kNumOri) {   // orientation o + 1's chunks land during I2..I4
+      if (t == 0 && o + 1 < oE) {   // orientation o + 1's chunks land during I2..I4
         fence_proxy_async();
         for (int j = 0; j < 4; ++j) {
-          const int c = 4 * (o + 1) + j, sl = c % kGSlots;
+          const int c = 4 * (o + 1) + j, sl = (4 * (r + 1) + j) % kGSlots;
           bulk_load(gdst0 + sl * kGChunkFloats * 4, G0 + (size_t)c * kGChunkFloats, kGChunkFloats * 4, bar0 + 8 * sl);
         }
       }
@@ -570,6 +576,8 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
 
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const TileWork item = work[w];
+    const int oB = item.oBegin, oE = item.oEnd, nO = oE - oB;
+    if (nO <= 0) continue;   // empty slot of a padded plan
     const ScaleDev* sd = sds + item.entry;
     const int kX = sd->kX, V = sd->V;
     const int ty = item.tile / sd->tilesX, tx = item.tile - ty * sd->tilesX;
@@ -592,8 +600,8 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
     __syncthreads();   // spectrum in TMEM; the forward scratch in the row buffers is dead
     tmem_fence_after();
     if (groupY) {
-      for (int o = 0; o < kNumOri; ++o) {
-        const int b = o & 1;
+      for (int o = oB; o < oE; ++o) {
+        const int b = (o - oB) & 1;
         float2* Wo = Wb + b * kWsBuf;
         const float* __restrict__ Go = sd->G + (size_t)o * kSpecFloats;
         // I1: y-dim pass B' with the spectrum product (TMEM in, TMEM y-area
@@ -623,7 +631,7 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
         tmem_fence_before();
         nbar_sync(kBarY, kWsGroup);   // the y-area holds orientation o's first y-pass
         tmem_fence_after();
-        if (o >= 2) nbar_sync(kBarEmpty0 + b, kTileThreads);   // group X is done with orientation o - 2
+        if (o - oB >= 2) nbar_sync(kBarEmpty0 + b, kTileThreads);   // group X is done with orientation o - 2
         // I2: y-dim pass A' -> natural y; the valid rows into buffer b
 #pragma unroll
         for (int it = 0; it < 4; ++it) {
@@ -656,8 +664,8 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
       }
       float* __restrict__ C0p = sd->C;
       const long long cStride = sd->cStride;
-      for (int o = 0; o < kNumOri; ++o) {
-        const int b = o & 1;
+      for (int o = oB; o < oE; ++o) {
+        const int b = (o - oB) & 1;
         float2* Wo = Wb + b * kWsBuf;
         float* __restrict__ Cout = C0p + (size_t)o * cStride;
         nbar_sync(kBarFull0 + b, kTileThreads);
@@ -703,9 +711,9 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
             }
           }
         }
-        // buffer b may be refilled by orientation o + 2; the last two
+        // buffer b may be refilled by orientation o + 2; the item's last two
         // orientations are ordered against the next tile by its barrier
-        if (o < kNumOri - 2) nbar_arrive(kBarEmpty0 + b, kTileThreads);
+        if (o - oB < nO - 2) nbar_arrive(kBarEmpty0 + b, kTileThreads);
       }
     }
   }

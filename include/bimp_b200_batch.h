@@ -41,8 +41,11 @@ int bimp_batch_image(bimp_batch* batch, int i, uint8_t** d_image, size_t* pitch)
  * the scales' tiles; `kernel` 1 runs the warp-specialised tile kernel (the
  * inverse y-passes of one orientation overlap the x-passes of the previous
  * one; needs every valid block <= 104), 0 the phased one (all warps pass by
- * pass); `grid` is the number of CTAs of the tile kernel (each walks tiles;
- * the tile count means one CTA per tile).  `ms` is the measured time of one
+ * pass); `grid` 0 launches one CTA per tile, grid > 0 at most that many
+ * persistent CTAs that share the (tile, orientation) pairs in contiguous runs
+ * of equal estimated cost (a tile cut between two CTAs is transformed
+ * forward by both; the default plan uses one CTA per SM).  `tiles` is the
+ * plan's tile count.  `ms` is the measured time of one
  * detection of the batch with the plan. */
 typedef struct {
   int policy;
@@ -54,8 +57,8 @@ typedef struct {
 } bimp_tile_plan;
 
 /* Autotuner (no counterpart in the reference): times every tile plan
- * (2 kernels x 2 policies x 2 orders x 3 grids: one CTA per tile, one and two
- * per SM)
+ * (2 kernels x 2 policies x 2 orders x 3 grids: one CTA per tile, or the
+ * split plan over one or two CTAs per SM)
  * over `reps` detections of the batch's current inputs on `stream`, keeps
  * the fastest and recaptures the graph with it.  Plans of one policy give
  * bitwise identical results; policy 1 moves tile boundaries, which changes
@@ -66,7 +69,8 @@ int bimp_batch_autotune(bimp_batch* batch, void* stream, int reps, bimp_tile_pla
                         bimp_tile_plan* tried, int max_tried, int* n_tried);
 
 /* Uses the given tile plan (e.g. one the autotuner chose earlier) and
- * recaptures the graph; grid <= 0 means one CTA per tile; kernel 1 falls back
+ * recaptures the graph; grid <= 0 means one CTA per tile, grid > 0 the split
+ * plan over at most `grid` persistent CTAs; kernel 1 falls back
  * to the phased kernel where the pipelined one does not fit. */
 int bimp_batch_set_tile_plan(bimp_batch* batch, int policy, int order, int grid, int kernel);
 

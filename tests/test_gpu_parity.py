@@ -298,15 +298,20 @@ def test_batch_tile_plans_and_autotune():
     b.close()
 
 
-def test_persistent_tile_loop_matches(monkeypatch):
-    """Each CTA of the tile kernel walks many tiles (grid capped at 7): the
-    spectrum double buffer's phases carry across tiles; results unchanged."""
+@pytest.mark.parametrize("grid", ["7", "0", "1000"])
+def test_tile_plans_bitwise_equal(monkeypatch, grid):
+    """The default plan (the tiles' orientations split over one persistent
+    CTA per SM) against: 7 CTAs, each walking many tiles and orientation runs
+    (the G ring's phases carry across items); one CTA per tile (0); and more
+    CTAs than the plan can use (1000: runs of one orientation).  Every
+    (tile, orientation) is computed the same way in all of them, so maps and
+    records are bitwise equal."""
     imgs, lam = synth.workload("vga")
     img = imgs[0]
     cs = api.CudaStuff(img.shape[1], img.shape[0], lam)
     ref = api.keypoint_matrix_to_records(api.getKeypoints(img, cs, capacity=100000))
     d_ref = [cs.dense_map(i).cpu().numpy() for i in range(len(lam))]
-    monkeypatch.setenv("BIMP_TILE_GRID", "7")
+    monkeypatch.setenv("BIMP_TILE_GRID", grid)
     cs2 = api.CudaStuff(img.shape[1], img.shape[0], lam)
     got = api.keypoint_matrix_to_records(api.getKeypoints(img, cs2, capacity=100000))
     assert np.array_equal(ref, got)
@@ -518,4 +523,26 @@ def test_pipeline_matches_detect_host(depth):
     while pl.in_flight():
         pl.pop()
     pl.close()
+    cs.close()
+
+
+def test_device_allocation_failure_is_a_status():
+    """A batch whose arena exceeds the device memory (four 32767 x 32767
+    images, about 400 GB) fails with BIMP_ERR_NOMEM and a message, allocates
+    nothing, and the library keeps working afterwards."""
+    import ctypes as C
+    from bimp_b200 import _lib as L
+    n = 4
+    ws = (C.c_int * n)(*[32767] * n)
+    hs = (C.c_int * n)(*[32767] * n)
+    lam = synth.bank(8)
+    la = (C.c_float * len(lam))(*lam)
+    h = C.c_void_p()
+    rc = L.lib().bimp_batch_create(C.byref(h), ws, hs, n, la, len(lam), None, 1024)
+    assert rc == L.BIMP_ERR_NOMEM and not h.value
+    assert b"cudaMalloc" in L.lib().bimp_last_error()
+    imgs, lam2 = synth.workload("vga")
+    cs = api.CudaStuff(640, 480, lam2)
+    kp, n_found = api.getKeypoints(imgs[0], cs, capacity=100000, return_count=True)
+    assert n_found > 0
     cs.close()
