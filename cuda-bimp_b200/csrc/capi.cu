@@ -165,16 +165,17 @@ struct Engine {
   // orientation) pairs, tile by tile in plan order, are cut into at most
   // `grid` contiguous runs of about equal cost; a run becomes one work item
   // per tile it touches (a tile cut between two CTAs is transformed forward by
-  // both).  Costs per pass, from the kernel's instruction counts per thread:
-  // an orientation 0.5 + 0.005 V (product and inverse y-passes on all 128
-  // columns, inverse x-passes and magnitudes on V rows), the forward
-  // transform 0.8.  The smallest run bound that fits in `grid` runs is found
-  // by bisection.  Item k of CTA b is placed at index k * grid + b (the kernel
-  // strides its work list by the grid); CTAs with fewer items get empty ones.
-  // *usedGrid receives the number of CTAs with work.
+  // both).  Costs, from the kernel's measured phase times (cycles between its
+  // CTA barriers, 1080p): an orientation 0.5 + 0.005 V (product and inverse
+  // y-passes on all 128 columns, inverse x-passes and magnitudes on V rows),
+  // an item's forward transform and spectrum store 1.2.  The smallest run
+  // bound that fits in `grid` runs is found by bisection.  Item k of CTA b is
+  // placed at index k * grid + b (the kernel strides its work list by the
+  // grid); CTAs with fewer items get empty ones.  *usedGrid receives the
+  // number of CTAs with work.
   static std::vector<TileWork> split_plan(const std::vector<TileWork>& tiles, const std::vector<ScaleDev>& sds,
                                           int grid, int* usedGrid) {
-    const double kFwd = 0.8;
+    const double kFwd = 1.2;
     std::vector<double> ori(tiles.size());
     double total = 0.0, worst = 0.0;
     for (size_t i = 0; i < tiles.size(); ++i) {

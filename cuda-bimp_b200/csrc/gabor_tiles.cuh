@@ -422,7 +422,8 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
           bulk_load(gdst0 + sl * kGChunkFloats * 4, G0 + (size_t)c * kGChunkFloats, kGChunkFloats * 4, bar0 + 8 * sl);
         }
       }
-      // I2: y-dim pass A' -> natural y
+      // I2: y-dim pass A' -> natural y (all 128 rows: storing only the
+      // valid rows, under a predicate per store, measured 11% slower)
 #pragma unroll
       for (int it = 0; it < 2; ++it) {
         const int j = t + it * kTileThreads;

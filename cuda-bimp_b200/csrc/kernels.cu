@@ -64,12 +64,17 @@ __device__ __forceinline__ int reflect101_near(int i, int n) {
   return i < 0 ? -i : i;
 }
 constexpr int pyr_side(int K, int m) { return m == K ? pyr_tile(K) : 2 * pyr_side(K, m + 1) + 3; }
+// Shared memory of the computed levels 1..K (square regions).
 constexpr int pyr_smem(int K) {
-  return K == 3 ? pyr_side(3, 0) * pyr_side(3, 0) + pyr_side(3, 1) * pyr_side(3, 1) +
-                      pyr_side(3, 2) * pyr_side(3, 2) + pyr_side(3, 3) * pyr_side(3, 3)
-       : K == 2 ? pyr_side(2, 0) * pyr_side(2, 0) + pyr_side(2, 1) * pyr_side(2, 1) + pyr_side(2, 2) * pyr_side(2, 2)
-                : pyr_side(1, 0) * pyr_side(1, 0) + pyr_side(1, 1) * pyr_side(1, 1);
+  return K == 3 ? pyr_side(3, 1) * pyr_side(3, 1) + pyr_side(3, 2) * pyr_side(3, 2) + pyr_side(3, 3) * pyr_side(3, 3)
+       : K == 2 ? pyr_side(2, 1) * pyr_side(2, 1) + pyr_side(2, 2) * pyr_side(2, 2)
+                : pyr_side(1, 1) * pyr_side(1, 1);
 }
+// The source region is staged as 16-byte chunks: the chunks of a region row
+// cover its S0 bytes after a lead of up to 15 bytes (the region's first
+// column rounded down to a 16-byte boundary).
+constexpr int pyr_chunks(int K) { return (pyr_side(K, 0) + 15 + 15) / 16; }
+constexpr int kPyrThreads = 256;
 
 // Largest horizontal-pass buffer of a K-level launch (rows of the level
 // above x columns of the level computed).
@@ -78,8 +83,10 @@ constexpr int pyr_hbuf(int K) {
 }
 
 template <int K>
-__global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ jobs) {
-  __shared__ uint8_t s_lvl[pyr_smem(K)];
+__global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restrict__ jobs) {
+  constexpr int S0 = pyr_side(K, 0), CPR = pyr_chunks(K), SP = 16 * CPR;
+  __shared__ __align__(16) uint8_t s_raw[S0 * SP];   // source region, row pitch SP
+  __shared__ uint8_t s_lvl[pyr_smem(K)];             // levels 1..K
   __shared__ uint16_t s_h[pyr_hbuf(K)];
   griddep_launch_dependents();
   const PyrJob& j = jobs[blockIdx.z];
@@ -95,27 +102,33 @@ __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ job
     loX[m - 1] = 2 * loX[m] - 2;
   }
   off[0] = 0;
+  off[1] = 0;
 #pragma unroll
-  for (int m = 1; m <= K; ++m) off[m] = off[m - 1] + pyr_side(K, m - 1) * pyr_side(K, m - 1);
+  for (int m = 2; m <= K; ++m) off[m] = off[m - 1] + pyr_side(K, m - 1) * pyr_side(K, m - 1);
   const int t = threadIdx.x;
-  // source region as aligned 4-byte words (rows are 16-byte aligned in the
-  // level buffers).  Bytes outside the level (negative coordinates, or
-  // between the width and the pitch) are never used: reflect-101 keeps every
-  // tap inside the level.
+  // Source region as 16-byte chunks (level rows start 16-byte aligned and
+  // their pitch is a multiple of 16, so a chunk that starts inside the pitch
+  // lies inside the row).  All of a thread's loads are issued before the
+  // first store.  Chunks outside the level leave their bytes unset; bytes
+  // outside the level are never read: reflect-101 keeps every tap inside it.
+  const int a16 = loX[0] & ~15;
+  const int lead = loX[0] - a16;
   {
-    constexpr int S0 = pyr_side(K, 0);
-    constexpr int WPR = (S0 + 3) / 4 + 1;   // words per region row
-    const int a = loX[0] & ~3;
-    for (int idx = t; idx < S0 * WPR; idx += blockDim.x) {
-      const int r = idx / WPR, w = a + 4 * (idx - r * WPR);
-      const int gy = loY[0] + r;
-      if (gy < 0 || gy >= j.sh || w < 0 || w >= j.sp) continue;
-      const uint32_t v = *reinterpret_cast<const uint32_t*>(j.src + (size_t)gy * j.sp + w);
+    constexpr int NCH = S0 * CPR, PER = (NCH + kPyrThreads - 1) / kPyrThreads;
+    uint4 v[PER];
 #pragma unroll
-      for (int bt = 0; bt < 4; ++bt) {
-        const int c = w + bt - loX[0];
-        if (c >= 0 && c < S0) s_lvl[r * S0 + c] = (uint8_t)(v >> (8 * bt));
-      }
+    for (int i = 0; i < PER; ++i) {
+      const int idx = t + kPyrThreads * i;
+      const int r = idx / CPR, w = a16 + 16 * (idx - r * CPR);
+      const int gy = loY[0] + r;
+      v[i] = make_uint4(0u, 0u, 0u, 0u);
+      if (idx < NCH && gy >= 0 && gy < j.sh && w >= 0 && w < j.sp)
+        v[i] = *reinterpret_cast<const uint4*>(j.src + (size_t)gy * j.sp + w);
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int idx = t + kPyrThreads * i;
+      if (idx < NCH) reinterpret_cast<uint4*>(s_raw)[idx] = v[i];
     }
   }
   __syncthreads();
@@ -127,7 +140,8 @@ __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ job
     const int Wo = j.dw[m - 1], Ho = j.dh[m - 1];
     const int own = T << (K - m);
     const int ownY = oy << (K - m), ownX = ox << (K - m);
-    const uint8_t* in = s_lvl + off[m - 1];
+    const int ip = m == 1 ? SP : Si;   // row pitch of the level above in shared memory
+    const uint8_t* in = m == 1 ? s_raw + lead : s_lvl + off[m - 1];
     uint8_t* outS = s_lvl + off[m];
     uint8_t* dst = j.dst[m - 1];
     const int dp = j.dp[m - 1];
@@ -136,13 +150,13 @@ __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ job
     // 2 r .. 2 r + 4.
     const bool inner = loX[m - 1] >= 0 && loY[m - 1] >= 0 && loX[m - 1] + Si <= Wi && loY[m - 1] + Si <= Hi;
     if (inner) {
-      for (int idx = t; idx < Si * So; idx += blockDim.x) {
+      for (int idx = t; idx < Si * So; idx += kPyrThreads) {
         const int r = idx / So, c = idx - r * So;
-        const uint8_t* a = in + r * Si + 2 * c;
+        const uint8_t* a = in + r * ip + 2 * c;
         s_h[idx] = (uint16_t)(a[0] + 4 * a[1] + 6 * a[2] + 4 * a[3] + a[4]);
       }
       __syncthreads();
-      for (int idx = t; idx < So * So; idx += blockDim.x) {
+      for (int idx = t; idx < So * So; idx += kPyrThreads) {
         const int r = idx / So, c = idx - r * So;
         const uint16_t* a = s_h + 2 * r * So + c;
         const int acc = a[0] + 4 * a[So] + 6 * a[2 * So] + 4 * a[3 * So] + a[4 * So];
@@ -159,11 +173,11 @@ __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ job
     }
     // horizontal pass: every region row inside the level above, every
     // output column inside this level (exact integer sums)
-    for (int idx = t; idx < Si * So; idx += blockDim.x) {
+    for (int idx = t; idx < Si * So; idx += kPyrThreads) {
       const int r = idx / So, c = idx - r * So;
       const int gy = loY[m - 1] + r, x = loX[m] + c;
       if (gy < 0 || gy >= Hi || x < 0 || x >= Wo) continue;
-      const uint8_t* row = in + r * Si;
+      const uint8_t* row = in + r * ip;
       int h = 0;
 #pragma unroll
       for (int k = 0; k < 5; ++k) h += w5[k] * row[reflect101_near(2 * x + k - 2, Wi) - loX[m - 1]];
@@ -171,7 +185,7 @@ __global__ void __launch_bounds__(256) k_pyr_down(const PyrJob* __restrict__ job
     }
     __syncthreads();
     // vertical pass, rounding to nearest with ties to even
-    for (int idx = t; idx < So * So; idx += blockDim.x) {
+    for (int idx = t; idx < So * So; idx += kPyrThreads) {
       const int r = idx / So, c = idx - r * So;
       const int y = loY[m] + r, x = loX[m] + c;
       if (y < 0 || y >= Ho || x < 0 || x >= Wo) continue;
@@ -1174,9 +1188,9 @@ void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH,
   if (njobs <= 0 || levels <= 0) return;
   const int T = 32 >> (levels - 1);
   dim3 g((maxW + T - 1) / T, (maxH + T - 1) / T, njobs);
-  if (levels == 3) k_pyr_down<3><<<g, 256, 0, s>>>(d_jobs);
-  else if (levels == 2) k_pyr_down<2><<<g, 256, 0, s>>>(d_jobs);
-  else k_pyr_down<1><<<g, 256, 0, s>>>(d_jobs);
+  if (levels == 3) k_pyr_down<3><<<g, kPyrThreads, 0, s>>>(d_jobs);
+  else if (levels == 2) k_pyr_down<2><<<g, kPyrThreads, 0, s>>>(d_jobs);
+  else k_pyr_down<1><<<g, kPyrThreads, 0, s>>>(d_jobs);
 }
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                   cudaStream_t s, bool pipelined, bool pdl) {
