@@ -165,21 +165,30 @@ struct Engine {
   // orientation) pairs, tile by tile in plan order, are cut into at most
   // `grid` contiguous runs of about equal cost; a run becomes one work item
   // per tile it touches (a tile cut between two CTAs is transformed forward by
-  // both).  Costs, from the kernel's measured phase times (cycles between its
-  // CTA barriers, 1080p): an orientation 0.5 + 0.005 V (product and inverse
-  // y-passes on all 128 columns, inverse x-passes and magnitudes on V rows),
-  // an item's forward transform and spectrum store 1.2.  The smallest run
-  // bound that fits in `grid` runs is found by bisection.  Item k of CTA b is
+  // both).  Costs come from the kernel's measured phase times (cycles between
+  // its CTA barriers at 1080p, in units of one orientation of a V = 100
+  // tile): per orientation, the product and inverse y-passes on all 128
+  // columns 0.414, each round of the first inverse x-pass (16 V items over
+  // 512 threads) 0.0565, each round of the second (8 V items) 0.18, of which
+  // the magnitudes and stores are 0.42 and scale with the share of the
+  // tile's outputs inside the map; an item's forward transform and spectrum
+  // store 1.45.  The smallest run bound that fits in `grid` runs is found by
+  // bisection.  Item k of CTA b is
   // placed at index k * grid + b (the kernel strides its work list by the
   // grid); CTAs with fewer items get empty ones.  *usedGrid receives the
   // number of CTAs with work.
   static std::vector<TileWork> split_plan(const std::vector<TileWork>& tiles, const std::vector<ScaleDev>& sds,
                                           int grid, int* usedGrid) {
-    const double kFwd = 1.2;
+    const double kFwd = 1.45;
     std::vector<double> ori(tiles.size());
     double total = 0.0, worst = 0.0;
     for (size_t i = 0; i < tiles.size(); ++i) {
-      ori[i] = 0.5 + 0.005 * sds[tiles[i].entry].V;
+      const ScaleDev& d = sds[tiles[i].entry];
+      const int ty = tiles[i].tile / d.tilesX, tx = tiles[i].tile - ty * d.tilesX;
+      const double inside = (double)std::min(d.V, d.cRows - ty * d.V) * std::min(d.V, d.cCols - tx * d.V) /
+                            ((double)d.V * d.V);
+      const int r3 = (16 * d.V + kTileThreads - 1) / kTileThreads, r4 = (8 * d.V + kTileThreads - 1) / kTileThreads;
+      ori[i] = 0.414 + 0.0565 * r3 + 0.18 * r4 * (0.58 + 0.42 * inside);
       total += kNumOri * ori[i] + kFwd;
       worst = std::max(worst, ori[i] + kFwd);
     }
