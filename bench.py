@@ -365,6 +365,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         bt = api.Batch(sizes, lam_b, kp_capacity=65536)
         bt.load(imgs)
         tune = bt.autotune(reps=3)   # tile plan: kernel variant, valid-block policy, tile order, grid
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
         for _ in range(3):
             bt.run()
         torch.cuda.synchronize()
@@ -404,10 +405,16 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "autotune": {"chosen": tune["chosen"], "plans_timed": len(tune["tried"]),
                                 "kernels_tried": sorted({t["kernel"] for t in tune["tried"]}),
                                 "valid_block_policies_tried": sorted({t["policy"] for t in tune["tried"]}),
+                                "grids_tried": sorted({t["grid"] for t in tune["tried"]}),
+                                # the plan a batch starts with: phased kernel, largest valid
+                                # block, scale-by-scale order, split over one CTA per SM
                                 "default_plan_ms": next((t["ms"] for t in tune["tried"]
                                                          if t["policy"] == 0 and t["order"] == 0
-                                                         and t["grid"] == t["tiles"] and t["kernel"] == 1),
-                                                        None)}}
+                                                         and t["grid"] == sms and t["kernel"] == 0),
+                                                        None),
+                                "tried": [[t["policy"], t["order"], t["kernel"], t["grid"], t["ms"]]
+                                          for t in tune["tried"]],
+                                "tried_fields": ["policy", "order", "kernel", "grid", "ms"]}}
         for c2 in ctxs:
             c2.close()
         bt.close()
