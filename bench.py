@@ -508,6 +508,9 @@ def run_adjoint_bench(args, rank, world, dev, stream, max_ms):
         out["fd_step_1e-4_rel_diff_image0"] = float(abs(fd - float((g0 * v).sum())) / abs(fd))
         one.close()
     adj.close()
+    if rank == 0 and world == 1 and not args.no_uhd_adjoint:
+        # the 32-frame UHD configuration (12 scales): timing and peak device memory
+        out["uhd_32_frames"] = uhd_adjoint(synth.uhd_frames(32, 1004), dev, stream)
     return out
 
 
@@ -588,31 +591,56 @@ def run_configs(args):
     torch.cuda.synchronize()
     fwd = {"ms_per_batch": round(ms, 2), "mpixel_s": round(32 * 3840 * 2160 / (ms * 1e-3) / 1e6, 1),
            "device_bytes": int(bt_bytes), "keypoints": n_kp, "graph": True}
+    out["cfg4"] = {"workload": "32 correlated 3840x2160 frames (subpixel shifts <= 2 px + N(0,2) noise), "
+                               "12 scales x 8 orientations",
+                   "forward_batched": fwd,
+                   "adjoint": uhd_adjoint(frames, dev, stream),
+                   "cpu_baseline_one_frame": cpu(synth.uhd_frames(1, 1004)[0], lam12, 1)}
+    print(json.dumps({"configs": out}), flush=True)
+
+
+def uhd_adjoint(frames, dev, stream) -> dict:
+    """Adjoint forward + backward of 32 UHD frames with the 12-scale bank:
+    times, bwd/fwd ratio and the device memory it holds at its peak."""
+    import torch
+    from bimp_b200 import api, synth
+    lam12 = synth.bank(12)
+    n = len(frames)
     x = torch.from_numpy(np.stack([f.astype(np.float32) / np.float32(255.0) for f in frames])).to(dev)
-    del frames
+    torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info()[0]
-    adj = api.Adjoint(3840, 2160, 32, lam12)
-    masks = torch.randn(32 * adj.mask_stride, generator=torch.Generator(device=dev).manual_seed(5), device=dev)
+    adj = api.Adjoint(3840, 2160, n, lam12)
+    masks = torch.randn(n * adj.mask_stride, generator=torch.Generator(device=dev).manual_seed(5), device=dev)
     adj.forward(x, masks)
     grad, _ = adj.backward()
     torch.cuda.synchronize()
     held = free0 - torch.cuda.mem_get_info()[0]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, k):
+        fn()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(k):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / k
+
     f_ms = timed(lambda: adj.forward(x, masks), 3)
     b_ms = timed(lambda: adj.backward(grad), 3)
-    out["cfg4"] = {"workload": "32 correlated 3840x2160 frames (subpixel shifts <= 2 px + N(0,2) noise), "
-                               "12 scales x 8 orientations",
-                   "forward_batched": fwd,
-                   "adjoint": {"fwd_ms": round(f_ms, 2), "bwd_ms": round(b_ms, 2),
-                               "bwd_fwd_ratio": round(b_ms / f_ms, 3),
-                               "train_step_mpixel_s": round(32 * 3840 * 2160 / ((f_ms + b_ms) * 1e-3) / 1e6, 1),
-                               "device_bytes_arena": adj.device_bytes(),
-                               "device_bytes_held": int(held),
-                               "note": "the backward recomputes each tile's spectrum and e + i o (nothing of "
-                                       "the forward's responses is stored); complex cells, their gradient and "
-                                       "the inhibition maps exist for a chunk of frames at a time"},
-                   "cpu_baseline_one_frame": cpu(synth.uhd_frames(1, 1004)[0], lam12, 1)}
+    out = {"workload": f"{n} correlated 3840x2160 float frames, 12 scales x 8 orientations, L = sum(M * D)",
+           "fwd_ms": round(f_ms, 2), "bwd_ms": round(b_ms, 2), "bwd_fwd_ratio": round(b_ms / f_ms, 3),
+           "train_step_mpixel_s": round(n * 3840 * 2160 / ((f_ms + b_ms) * 1e-3) / 1e6, 1),
+           "device_bytes_arena": adj.device_bytes(), "device_bytes_held": int(held),
+           "note": "peak device memory held by the adjoint (its arena plus the gradient output), measured "
+                   "as the drop in free device memory; the backward recomputes each tile's spectrum and "
+                   "e + i o (nothing of the forward's responses is stored); complex cells, their gradient "
+                   "and the inhibition maps exist for a chunk of frames at a time"}
     adj.close()
-    print(json.dumps({"configs": out}), flush=True)
+    del x, masks, grad
+    torch.cuda.synchronize()
+    return out
 
 
 def cs_launches(cs) -> int:
@@ -690,6 +718,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-uhd-adjoint", action="store_true",
+                    help="skip the 32-frame UHD adjoint inside the adjoint block (N=1 only)")
     ap.add_argument("--configs", action="store_true",
                     help="the other workload configurations (VGA, 32 UHD frames forward and adjoint), 1 GPU")
     ap.add_argument("--adjoint-only", action="store_true",
