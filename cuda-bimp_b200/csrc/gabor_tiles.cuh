@@ -243,26 +243,28 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
     for (int k1 = 0; k1 < 8; ++k1) W[widx(r, 8 * k2 + k1)] = v[k1];
   }
   __syncthreads();
-  // separation of the packed rows into the Hermitian half (kx = 0..64)
-  for (int j = t; j < 64 * kXhCols; j += kTileThreads) {
-    const int r = j / kXhCols, s = j - r * kXhCols;
-    const int kx = s < 64 ? (s >> 2) + 16 * (s & 3) : 64;
-    const int nk = (128 - kx) & 127;
-    const float2 Z = W[widx(r, 8 * (kx & 15) + (kx >> 4))];
-    const float2 Zn = W[widx(r, 8 * (nk & 15) + (nk >> 4))];
-    *xh_ptr(Xh64, Nyq, r, s) = make_float2(0.5f * (Z.x + Zn.x), 0.5f * (Z.y - Zn.y));
-    *xh_ptr(Xh64, Nyq, r + 64, s) = make_float2(0.5f * (Z.y + Zn.y), 0.5f * (Zn.x - Z.x));
-  }
-  __syncthreads();
-  // F3: y-dim pass A on the 65 half columns
+  // F3: y-dim pass A on the 65 half columns (kx = 0..64), reading the packed
+  // rows and separating them on the way in: packed row r (< 64) holds
+  // in[r] + i in[r + 64], so X[r][kx] = (Z[kx] + conj Z[-kx]) / 2 and
+  // X[r + 64][kx] = (Z[kx] - conj Z[-kx]) / 2i.  The packed rows (rows 0..63
+  // of W) and the half spectrum (rows 64..127 of W, and the Nyquist slot)
+  // do not overlap.
   for (int j = t; j < 8 * kXhCols; j += kTileThreads) {
     const int n1 = j / kXhCols, s = j - n1 * kXhCols;
-    float2* col = xh_ptr(Xh64, Nyq, 0, s);
-    const int st = s < 64 ? 64 : 1;
+    const int kx = s < 64 ? (s >> 2) + 16 * (s & 3) : 64;
+    const int nk = (128 - kx) & 127;
+    const int pk = 8 * (kx & 15) + (kx >> 4), pn = 8 * (nk & 15) + (nk >> 4);
     float2 v[16];
 #pragma unroll
-    for (int m = 0; m < 16; ++m) v[m] = col[(n1 + 8 * m) * st];
+    for (int m = 0; m < 8; ++m) {
+      const int r = n1 + 8 * m;
+      const float2 Z = W[widx(r, pk)], Zn = W[widx(r, pn)];
+      v[m] = make_float2(0.5f * (Z.x + Zn.x), 0.5f * (Z.y - Zn.y));
+      v[m + 8] = make_float2(0.5f * (Z.y + Zn.y), 0.5f * (Zn.x - Z.x));
+    }
     dft16<false>(v);
+    float2* col = xh_ptr(Xh64, Nyq, 0, s);
+    const int st = s < 64 ? 64 : 1;
 #pragma unroll
     for (int k2 = 0; k2 < 16; ++k2) col[(n1 + 8 * k2) * st] = k2 ? c_mul(v[k2], tw[n1 * 17 + k2]) : v[0];
   }
@@ -276,11 +278,10 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
 #pragma unroll
     for (int n1 = 0; n1 < 8; ++n1) v[n1] = col[(8 * k2 + n1) * st];
     dft8<false>(v);
+    if (j == 0) v[0].x += 0.5f * (float)(kTile * kTile);   // DC of the removed 0.5 offset
 #pragma unroll
     for (int k1 = 0; k1 < 8; ++k1) col[(8 * k2 + k1) * st] = v[k1];
   }
-  __syncthreads();
-  if (t == 0) Xh64[0].x += 0.5f * (float)(kTile * kTile);   // DC of the removed 0.5 offset
   __syncthreads();
 }
 
