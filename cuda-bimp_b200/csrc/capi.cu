@@ -172,14 +172,14 @@ struct Engine {
   // 512 threads) 0.0565, each round of the second (8 V items) 0.18, of which
   // the magnitudes and stores are 0.42 and scale with the share of the
   // tile's outputs inside the map; an item's forward transform and spectrum
-  // store 1.45.  The smallest run bound that fits in `grid` runs is found by
+  // store 1.35.  The smallest run bound that fits in `grid` runs is found by
   // bisection.  Item k of CTA b is
   // placed at index k * grid + b (the kernel strides its work list by the
   // grid); CTAs with fewer items get empty ones.  *usedGrid receives the
   // number of CTAs with work.
   static std::vector<TileWork> split_plan(const std::vector<TileWork>& tiles, const std::vector<ScaleDev>& sds,
                                           int grid, int* usedGrid) {
-    const double kFwd = 1.45;
+    const double kFwd = 1.35;
     std::vector<double> ori(tiles.size());
     double total = 0.0, worst = 0.0;
     for (size_t i = 0; i < tiles.size(); ++i) {
