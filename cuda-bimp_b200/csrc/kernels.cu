@@ -55,14 +55,6 @@ __device__ __forceinline__ int reflect101(int i, int n) {
 // from the one above, writing the part it owns.
 constexpr int pyr_tile(int K) { return 32 >> (K - 1); }
 
-// reflect101 for indices at most one period outside [0, n) (the 5-tap
-// support, n >= 2); the general form for n == 1
-__device__ __forceinline__ int reflect101_near(int i, int n) {
-  if (n == 1) return 0;
-  i = i < 0 ? -i : i;
-  i = i >= n ? 2 * n - 2 - i : i;
-  return i < 0 ? -i : i;
-}
 constexpr int pyr_side(int K, int m) { return m == K ? pyr_tile(K) : 2 * pyr_side(K, m + 1) + 3; }
 // Shared memory of the computed levels 1..K (square regions).
 constexpr int pyr_smem(int K) {
@@ -87,9 +79,10 @@ __global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restri
   constexpr int S0 = pyr_side(K, 0), CPR = pyr_chunks(K), SP = 16 * CPR;
   __shared__ __align__(16) uint8_t s_raw[S0 * SP];   // source region, row pitch SP
   __shared__ uint8_t s_lvl[pyr_smem(K)];             // levels 1..K
-  __shared__ uint16_t s_h[pyr_hbuf(K)];
+  __shared__ uint16_t s_h[pyr_hbuf(K) + 2 * pyr_side(K, 1)];   // + 2 rows read by the last row pair
   griddep_launch_dependents();
-  const PyrJob& j = jobs[blockIdx.z];
+  // the job by value: read once (the level stores below could alias it for the compiler)
+  const PyrJob j = jobs[blockIdx.z];
   constexpr int T = pyr_tile(K);
   const int oy = blockIdx.y * T, ox = blockIdx.x * T;
   if (oy >= j.dh[K - 1] || ox >= j.dw[K - 1]) return;
@@ -109,8 +102,8 @@ __global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restri
   // Source region as 16-byte chunks (level rows start 16-byte aligned and
   // their pitch is a multiple of 16, so a chunk that starts inside the pitch
   // lies inside the row).  All of a thread's loads are issued before the
-  // first store.  Chunks outside the level leave their bytes unset; bytes
-  // outside the level are never read: reflect-101 keeps every tap inside it.
+  // first store.  Chunks outside the level leave their bytes unset until the
+  // reflect-101 fill below.
   const int a16 = loX[0] & ~15;
   const int lead = loX[0] - a16;
   {
@@ -132,7 +125,6 @@ __global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restri
     }
   }
   __syncthreads();
-  const int w5[5] = {1, 4, 6, 4, 1};
 #pragma unroll
   for (int m = 1; m <= K; ++m) {
     const int Si = pyr_side(K, m - 1), So = pyr_side(K, m);
@@ -145,58 +137,59 @@ __global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restri
     uint8_t* outS = s_lvl + off[m];
     uint8_t* dst = j.dst[m - 1];
     const int dp = j.dp[m - 1];
-    // A region wholly inside the level above needs no reflection: output
-    // column c of the region takes input columns 2 c .. 2 c + 4, row r rows
-    // 2 r .. 2 r + 4.
+    // A region partly outside the level above first gets its reflect-101
+    // border: each position outside level m - 1 takes the value of its
+    // reflection inside the level where that lies in the region (the other
+    // positions feed no output inside level m).  Sources are inside the
+    // level and targets outside it, so the copies do not overlap.  After
+    // that every region runs the same passes: output column c takes input
+    // columns 2 c .. 2 c + 4, output row r rows 2 r .. 2 r + 4 (exact
+    // integer sums, the same values as reflecting each tap).
     const bool inner = loX[m - 1] >= 0 && loY[m - 1] >= 0 && loX[m - 1] + Si <= Wi && loY[m - 1] + Si <= Hi;
-    if (inner) {
-      for (int idx = t; idx < Si * So; idx += kPyrThreads) {
-        const int r = idx / So, c = idx - r * So;
-        const uint8_t* a = in + r * ip + 2 * c;
-        s_h[idx] = (uint16_t)(a[0] + 4 * a[1] + 6 * a[2] + 4 * a[3] + a[4]);
+    if (!inner) {
+      uint8_t* buf = m == 1 ? s_raw + lead : s_lvl + off[m - 1];
+      for (int idx = t; idx < Si * Si; idx += kPyrThreads) {
+        const int r = idx / Si, c = idx - r * Si;
+        const int y = loY[m - 1] + r, x = loX[m - 1] + c;
+        if (y >= 0 && y < Hi && x >= 0 && x < Wi) continue;
+        const int sr = reflect101(y, Hi) - loY[m - 1], sc = reflect101(x, Wi) - loX[m - 1];
+        if (sr >= 0 && sr < Si && sc >= 0 && sc < Si) buf[r * ip + c] = buf[sr * ip + sc];
       }
       __syncthreads();
-      for (int idx = t; idx < So * So; idx += kPyrThreads) {
-        const int r = idx / So, c = idx - r * So;
-        const uint16_t* a = s_h + 2 * r * So + c;
-        const int acc = a[0] + 4 * a[So] + 6 * a[2 * So] + 4 * a[3 * So] + a[4 * So];
+    }
+    // horizontal pass, two outputs per item: columns c, c + 1 share input
+    // columns 2 c + 2 .. 2 c + 4 (for an odd So the last item's second output
+    // is not stored; its two extra input bytes lie inside the buffers)
+    const int Sp = (So + 1) / 2;
+    for (int idx = t; idx < Si * Sp; idx += kPyrThreads) {
+      const int r = idx / Sp, c = 2 * (idx - r * Sp);
+      const uint8_t* a = in + r * ip + 2 * c;
+      const int a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], a4 = a[4], a5 = a[5], a6 = a[6];
+      s_h[r * So + c] = (uint16_t)(a0 + 4 * a1 + 6 * a2 + 4 * a3 + a4);
+      if (c + 1 < So) s_h[r * So + c + 1] = (uint16_t)(a2 + 4 * a3 + 6 * a4 + 4 * a5 + a6);
+    }
+    __syncthreads();
+    // vertical pass, two outputs per item (rows r, r + 1 share h-pass rows
+    // 2 r + 2 .. 2 r + 4), rounding to nearest with ties to even; the owned
+    // outputs inside the level go to the level buffer
+    for (int idx = t; idx < Sp * So; idx += kPyrThreads) {
+      const int rp = idx / So, c = idx - rp * So, r = 2 * rp;
+      const uint16_t* a = s_h + 2 * r * So + c;
+      const int b0 = a[0], b1 = a[So], b2 = a[2 * So], b3 = a[3 * So], b4 = a[4 * So], b5 = a[5 * So],
+                b6 = a[6 * So];
+      const int x = loX[m] + c;
+      const bool xin = x >= ownX && x < ownX + own && x < Wo;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (h == 1 && r + 1 >= So) break;
+        const int acc = h ? b2 + 4 * b3 + 6 * b4 + 4 * b5 + b6 : b0 + 4 * b1 + 6 * b2 + 4 * b3 + b4;
         const int q = acc >> 8;
         int v = (acc + 127 + (q & 1)) >> 8;
         v = v > 255 ? 255 : v;
-        outS[idx] = (uint8_t)v;
-        const int y = loY[m] + r, x = loX[m] + c;
-        if (y >= ownY && y < ownY + own && x >= ownX && x < ownX + own && y < Ho && x < Wo)
-          dst[(size_t)y * dp + x] = (uint8_t)v;
+        outS[(r + h) * So + c] = (uint8_t)v;
+        const int y = loY[m] + r + h;
+        if (xin && y >= ownY && y < ownY + own && y < Ho) dst[(size_t)y * dp + x] = (uint8_t)v;
       }
-      __syncthreads();
-      continue;
-    }
-    // horizontal pass: every region row inside the level above, every
-    // output column inside this level (exact integer sums)
-    for (int idx = t; idx < Si * So; idx += kPyrThreads) {
-      const int r = idx / So, c = idx - r * So;
-      const int gy = loY[m - 1] + r, x = loX[m] + c;
-      if (gy < 0 || gy >= Hi || x < 0 || x >= Wo) continue;
-      const uint8_t* row = in + r * ip;
-      int h = 0;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) h += w5[k] * row[reflect101_near(2 * x + k - 2, Wi) - loX[m - 1]];
-      s_h[r * So + c] = (uint16_t)h;
-    }
-    __syncthreads();
-    // vertical pass, rounding to nearest with ties to even
-    for (int idx = t; idx < So * So; idx += kPyrThreads) {
-      const int r = idx / So, c = idx - r * So;
-      const int y = loY[m] + r, x = loX[m] + c;
-      if (y < 0 || y >= Ho || x < 0 || x >= Wo) continue;
-      int acc = 0;
-#pragma unroll
-      for (int i = 0; i < 5; ++i) acc += w5[i] * (int)s_h[(reflect101_near(2 * y + i - 2, Hi) - loY[m - 1]) * So + c];
-      const int q = acc >> 8;
-      int v = (acc + 127 + (q & 1)) >> 8;
-      v = v > 255 ? 255 : v;
-      outS[idx] = (uint8_t)v;
-      if (y >= ownY && y < ownY + own && x >= ownX && x < ownX + own) dst[(size_t)y * dp + x] = (uint8_t)v;
     }
     __syncthreads();
   }
