@@ -74,6 +74,91 @@ constexpr int pyr_hbuf(int K) {
   return K == 3 ? pyr_side(3, 0) * pyr_side(3, 1) : K == 2 ? pyr_side(2, 0) * pyr_side(2, 1) : pyr_side(1, 0) * pyr_side(1, 1);
 }
 
+// Level M of a K-level launch from level M - 1: regions of side
+// pyr_side(K, M - 1) (in) and pyr_side(K, M) (out) in shared memory.  A
+// region partly outside level M - 1 first gets its reflect-101 border: each
+// position outside the level takes the value of its reflection inside it,
+// where that lies in the region (the other positions feed no output inside
+// level M).  Sources lie inside the level and targets outside it, so the
+// copies do not overlap.  Then every region runs the same two passes:
+// output column c takes input columns 2 c .. 2 c + 4, output row r rows
+// 2 r .. 2 r + 4 (exact integer sums: the same values as reflecting each
+// tap), two outputs per item.
+template <int K, int M>
+__device__ __forceinline__ void pyr_level(const PyrJob& j, const int (&loY)[K + 1], const int (&loX)[K + 1],
+                                          const int (&off)[K + 1], int oy, int ox, int lead, uint8_t* s_raw,
+                                          uint8_t* s_lvl, uint16_t* s_h, int t) {
+  constexpr int Si = pyr_side(K, M - 1), So = pyr_side(K, M), Sp = (So + 1) / 2;
+  constexpr int ip = M == 1 ? 16 * pyr_chunks(K) : Si;   // row pitch of the level above in shared memory
+  constexpr int own = pyr_tile(K) << (K - M);
+  const int Wi = M == 1 ? j.sw : j.dw[M - 2], Hi = M == 1 ? j.sh : j.dh[M - 2];
+  const int Wo = j.dw[M - 1], Ho = j.dh[M - 1];
+  const int ownY = oy << (K - M), ownX = ox << (K - M);
+  uint8_t* in = M == 1 ? s_raw + lead : s_lvl + off[M - 1];
+  uint8_t* outS = s_lvl + off[M];
+  uint8_t* dst = j.dst[M - 1];
+  const int dp = j.dp[M - 1];
+  const int ly = loY[M - 1], lx = loX[M - 1];
+  if (!(lx >= 0 && ly >= 0 && lx + Si <= Wi && ly + Si <= Hi)) {
+    // the region's rows [r0, r1) and columns [c0, c1) lie inside the level;
+    // items: every column of the rows outside, then the columns outside of
+    // the rows inside
+    const int r0 = min(Si, max(0, -ly)), r1 = max(r0, min(Si, Hi - ly));
+    const int c0 = min(Si, max(0, -lx)), c1 = max(c0, min(Si, Wi - lx));
+    const int nOutC = Si - (c1 - c0);
+    const int nA = (Si - (r1 - r0)) * Si, nB = (r1 - r0) * nOutC;
+    for (int idx = t; idx < nA + nB; idx += kPyrThreads) {
+      int r, c;
+      if (idx < nA) {
+        const int rr = idx / Si;
+        c = idx - rr * Si;
+        r = rr < r0 ? rr : r1 + (rr - r0);
+      } else {
+        const int k = idx - nA, ir = k / nOutC, cc = k - ir * nOutC;
+        r = r0 + ir;
+        c = cc < c0 ? cc : c1 + (cc - c0);
+      }
+      const int sr = reflect101(ly + r, Hi) - ly, sc = reflect101(lx + c, Wi) - lx;
+      if (sr >= 0 && sr < Si && sc >= 0 && sc < Si) in[r * ip + c] = in[sr * ip + sc];
+    }
+    __syncthreads();
+  }
+  // horizontal pass: columns c, c + 1 share input columns 2 c + 2 .. 2 c + 4
+  // (for an odd So the last item's second output is not stored; its two
+  // extra input bytes lie inside the buffers)
+  for (int idx = t; idx < Si * Sp; idx += kPyrThreads) {
+    const int r = idx / Sp, c = 2 * (idx - r * Sp);
+    const uint8_t* a = in + r * ip + 2 * c;
+    const int a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], a4 = a[4], a5 = a[5], a6 = a[6];
+    s_h[r * So + c] = (uint16_t)(a0 + 4 * a1 + 6 * a2 + 4 * a3 + a4);
+    if (c + 1 < So) s_h[r * So + c + 1] = (uint16_t)(a2 + 4 * a3 + 6 * a4 + 4 * a5 + a6);
+  }
+  __syncthreads();
+  // vertical pass: rows r, r + 1 share h-pass rows 2 r + 2 .. 2 r + 4;
+  // rounding to nearest with ties to even; the owned outputs inside the
+  // level go to the level buffer
+  for (int idx = t; idx < Sp * So; idx += kPyrThreads) {
+    const int rp = idx / So, c = idx - rp * So, r = 2 * rp;
+    const uint16_t* a = s_h + 2 * r * So + c;
+    const int b0 = a[0], b1 = a[So], b2 = a[2 * So], b3 = a[3 * So], b4 = a[4 * So], b5 = a[5 * So],
+              b6 = a[6 * So];
+    const int x = loX[M] + c;
+    const bool xin = x >= ownX && x < ownX + own && x < Wo;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && r + 1 >= So) break;
+      const int acc = h ? b2 + 4 * b3 + 6 * b4 + 4 * b5 + b6 : b0 + 4 * b1 + 6 * b2 + 4 * b3 + b4;
+      const int q = acc >> 8;
+      int v = (acc + 127 + (q & 1)) >> 8;
+      v = v > 255 ? 255 : v;
+      outS[(r + h) * So + c] = (uint8_t)v;
+      const int y = loY[M] + r + h;
+      if (xin && y >= ownY && y < ownY + own && y < Ho) dst[(size_t)y * dp + x] = (uint8_t)v;
+    }
+  }
+  __syncthreads();
+}
+
 template <int K>
 __global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restrict__ jobs) {
   constexpr int S0 = pyr_side(K, 0), CPR = pyr_chunks(K), SP = 16 * CPR;
@@ -81,7 +166,7 @@ __global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restri
   __shared__ uint8_t s_lvl[pyr_smem(K)];             // levels 1..K
   __shared__ uint16_t s_h[pyr_hbuf(K) + 2 * pyr_side(K, 1)];   // + 2 rows read by the last row pair
   griddep_launch_dependents();
-  // the job by value: read once (the level stores below could alias it for the compiler)
+  // the job by value: read once (the level stores could alias it for the compiler)
   const PyrJob j = jobs[blockIdx.z];
   constexpr int T = pyr_tile(K);
   const int oy = blockIdx.y * T, ox = blockIdx.x * T;
@@ -103,7 +188,7 @@ __global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restri
   // their pitch is a multiple of 16, so a chunk that starts inside the pitch
   // lies inside the row).  All of a thread's loads are issued before the
   // first store.  Chunks outside the level leave their bytes unset until the
-  // reflect-101 fill below.
+  // reflect-101 fill of the first level step.
   const int a16 = loX[0] & ~15;
   const int lead = loX[0] - a16;
   {
@@ -125,74 +210,9 @@ __global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restri
     }
   }
   __syncthreads();
-#pragma unroll
-  for (int m = 1; m <= K; ++m) {
-    const int Si = pyr_side(K, m - 1), So = pyr_side(K, m);
-    const int Wi = m == 1 ? j.sw : j.dw[m - 2], Hi = m == 1 ? j.sh : j.dh[m - 2];
-    const int Wo = j.dw[m - 1], Ho = j.dh[m - 1];
-    const int own = T << (K - m);
-    const int ownY = oy << (K - m), ownX = ox << (K - m);
-    const int ip = m == 1 ? SP : Si;   // row pitch of the level above in shared memory
-    const uint8_t* in = m == 1 ? s_raw + lead : s_lvl + off[m - 1];
-    uint8_t* outS = s_lvl + off[m];
-    uint8_t* dst = j.dst[m - 1];
-    const int dp = j.dp[m - 1];
-    // A region partly outside the level above first gets its reflect-101
-    // border: each position outside level m - 1 takes the value of its
-    // reflection inside the level where that lies in the region (the other
-    // positions feed no output inside level m).  Sources are inside the
-    // level and targets outside it, so the copies do not overlap.  After
-    // that every region runs the same passes: output column c takes input
-    // columns 2 c .. 2 c + 4, output row r rows 2 r .. 2 r + 4 (exact
-    // integer sums, the same values as reflecting each tap).
-    const bool inner = loX[m - 1] >= 0 && loY[m - 1] >= 0 && loX[m - 1] + Si <= Wi && loY[m - 1] + Si <= Hi;
-    if (!inner) {
-      uint8_t* buf = m == 1 ? s_raw + lead : s_lvl + off[m - 1];
-      for (int idx = t; idx < Si * Si; idx += kPyrThreads) {
-        const int r = idx / Si, c = idx - r * Si;
-        const int y = loY[m - 1] + r, x = loX[m - 1] + c;
-        if (y >= 0 && y < Hi && x >= 0 && x < Wi) continue;
-        const int sr = reflect101(y, Hi) - loY[m - 1], sc = reflect101(x, Wi) - loX[m - 1];
-        if (sr >= 0 && sr < Si && sc >= 0 && sc < Si) buf[r * ip + c] = buf[sr * ip + sc];
-      }
-      __syncthreads();
-    }
-    // horizontal pass, two outputs per item: columns c, c + 1 share input
-    // columns 2 c + 2 .. 2 c + 4 (for an odd So the last item's second output
-    // is not stored; its two extra input bytes lie inside the buffers)
-    const int Sp = (So + 1) / 2;
-    for (int idx = t; idx < Si * Sp; idx += kPyrThreads) {
-      const int r = idx / Sp, c = 2 * (idx - r * Sp);
-      const uint8_t* a = in + r * ip + 2 * c;
-      const int a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], a4 = a[4], a5 = a[5], a6 = a[6];
-      s_h[r * So + c] = (uint16_t)(a0 + 4 * a1 + 6 * a2 + 4 * a3 + a4);
-      if (c + 1 < So) s_h[r * So + c + 1] = (uint16_t)(a2 + 4 * a3 + 6 * a4 + 4 * a5 + a6);
-    }
-    __syncthreads();
-    // vertical pass, two outputs per item (rows r, r + 1 share h-pass rows
-    // 2 r + 2 .. 2 r + 4), rounding to nearest with ties to even; the owned
-    // outputs inside the level go to the level buffer
-    for (int idx = t; idx < Sp * So; idx += kPyrThreads) {
-      const int rp = idx / So, c = idx - rp * So, r = 2 * rp;
-      const uint16_t* a = s_h + 2 * r * So + c;
-      const int b0 = a[0], b1 = a[So], b2 = a[2 * So], b3 = a[3 * So], b4 = a[4 * So], b5 = a[5 * So],
-                b6 = a[6 * So];
-      const int x = loX[m] + c;
-      const bool xin = x >= ownX && x < ownX + own && x < Wo;
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (h == 1 && r + 1 >= So) break;
-        const int acc = h ? b2 + 4 * b3 + 6 * b4 + 4 * b5 + b6 : b0 + 4 * b1 + 6 * b2 + 4 * b3 + b4;
-        const int q = acc >> 8;
-        int v = (acc + 127 + (q & 1)) >> 8;
-        v = v > 255 ? 255 : v;
-        outS[(r + h) * So + c] = (uint8_t)v;
-        const int y = loY[m] + r + h;
-        if (xin && y >= ownY && y < ownY + own && y < Ho) dst[(size_t)y * dp + x] = (uint8_t)v;
-      }
-    }
-    __syncthreads();
-  }
+  pyr_level<K, 1>(j, loY, loX, off, oy, ox, lead, s_raw, s_lvl, s_h, t);
+  if constexpr (K >= 2) pyr_level<K, 2>(j, loY, loX, off, oy, ox, lead, s_raw, s_lvl, s_h, t);
+  if constexpr (K >= 3) pyr_level<K, 3>(j, loY, loX, off, oy, ox, lead, s_raw, s_lvl, s_h, t);
 }
 
 // ---------------------------------------------------------------------------
