@@ -593,8 +593,10 @@ struct Engine {
   int stage(int which, cudaStream_t s) {
     switch (which) {
       case 0:
+        // the first launch also zeroes the per-detection reset words
         for (size_t l = 0; l < pyrFirst.size(); ++l)
-          launch_pyr(d_pyr + pyrFirst[l], pyrCount[l], pyrLevels[l], pyrMaxW[l], pyrMaxH[l], s);
+          launch_pyr(d_pyr + pyrFirst[l], pyrCount[l], pyrLevels[l], pyrMaxW[l], pyrMaxH[l], s,
+                     l == 0 ? d_maxKeys : nullptr, l == 0 ? static_cast<int>(resetBytes / sizeof(unsigned int)) : 0);
         break;
       // stages 1-3 follow the previous stage's kernel with programmatic
       // dependent launch (each waits in the kernel for its predecessor)
@@ -620,8 +622,9 @@ struct Engine {
 
   // Everything after the level-0 images are in place.
   int enqueue(cudaStream_t s) {
-    // the reset first, so that the four kernels follow one another directly
-    BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, resetBytes, s));
+    // the reset of the map maxima and the fault word: done by the first
+    // pyramid launch, or (a bank without pyramid levels) by a memset
+    if (pyrFirst.empty()) BIMP_CUDA(cudaMemsetAsync(d_maxKeys, 0, resetBytes, s));
     int rc = stage(0, s);
     if (rc != BIMP_OK) return rc;
     for (int k = 1; k <= 3; ++k) {
@@ -854,6 +857,9 @@ static int ctx_run(bimp_context* c, const uint8_t* image, size_t pitch, int widt
   o.ld = ld;
   o.capacity = capacity;
   o.aos = aos;
+  // the NMS writes the keypoint total to d_count itself when the image has
+  // candidate rows (otherwise the total stays 0 and is copied below)
+  o.count = e.nNmsCtas > 0 ? d_count : nullptr;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   BIMP_CUDA(cudaStreamIsCapturing(s, &cap));
   // the destination descriptor: rewritten when it changes, and always when
@@ -874,7 +880,8 @@ static int ctx_run(bimp_context* c, const uint8_t* image, size_t pitch, int widt
     const int rc = e.enqueue(s);
     if (rc != BIMP_OK) return rc;
   }
-  if (d_count) BIMP_CUDA(cudaMemcpyAsync(d_count, e.d_totals, sizeof(int), cudaMemcpyDeviceToDevice, s));
+  if (d_count && !o.count)
+    BIMP_CUDA(cudaMemcpyAsync(d_count, e.d_totals, sizeof(int), cudaMemcpyDeviceToDevice, s));
   return BIMP_OK;
 }
 

@@ -160,12 +160,17 @@ __device__ __forceinline__ void pyr_level(const PyrJob& j, const int (&loY)[K + 
 }
 
 template <int K>
-__global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(kPyrThreads) k_pyr_down(const PyrJob* __restrict__ jobs,
+                                                           unsigned int* __restrict__ reset, int resetWords) {
   constexpr int S0 = pyr_side(K, 0), CPR = pyr_chunks(K), SP = 16 * CPR;
   __shared__ __align__(16) uint8_t s_raw[S0 * SP];   // source region, row pitch SP
   __shared__ uint8_t s_lvl[pyr_smem(K)];             // levels 1..K
   __shared__ uint16_t s_h[pyr_hbuf(K) + 2 * pyr_side(K, 1)];   // + 2 rows read by the last row pair
   griddep_launch_dependents();
+  // the detection's reset (the map maxima and the fault word), done here
+  // instead of by a memset of its own: every later kernel waits for this grid
+  if (reset && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
+    for (int i = threadIdx.x; i < resetWords; i += kPyrThreads) reset[i] = 0u;
   // the job by value: read once (the level stores could alias it for the compiler)
   const PyrJob j = jobs[blockIdx.z];
   constexpr int T = pyr_tile(K);
@@ -1004,7 +1009,11 @@ k_nms_emit(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, cons
     base += s_part[w];
     total += s_cnt[w];
   }
-  if (cta.last && t == 0) imageTotals[cta.image] = base + total;
+  if (cta.last && t == 0) {
+    imageTotals[cta.image] = base + total;
+    int* const cnt = outs[cta.image].count;
+    if (cnt) *cnt = base + total;
+  }
   if (warp < cta.nRows && cnt > 0) {
     for (int w = 0; w < warp; ++w) base += s_cnt[w];
     const ScaleDev* sd = sds + item.x;
@@ -1197,13 +1206,14 @@ static void launch_ex(void (*k)(Params...), dim3 grid, dim3 block, size_t smem, 
 __global__ void k_set_out(KpOut* __restrict__ d, KpOut v) { *d = v; }
 void launch_set_out(KpOut* d, const KpOut& v, cudaStream_t s) { k_set_out<<<1, 1, 0, s>>>(d, v); }
 
-void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s) {
+void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s,
+                unsigned int* reset, int resetWords) {
   if (njobs <= 0 || levels <= 0) return;
   const int T = 32 >> (levels - 1);
   dim3 g((maxW + T - 1) / T, (maxH + T - 1) / T, njobs);
-  if (levels == 3) k_pyr_down<3><<<g, kPyrThreads, 0, s>>>(d_jobs);
-  else if (levels == 2) k_pyr_down<2><<<g, kPyrThreads, 0, s>>>(d_jobs);
-  else k_pyr_down<1><<<g, kPyrThreads, 0, s>>>(d_jobs);
+  if (levels == 3) k_pyr_down<3><<<g, kPyrThreads, 0, s>>>(d_jobs, reset, resetWords);
+  else if (levels == 2) k_pyr_down<2><<<g, kPyrThreads, 0, s>>>(d_jobs, reset, resetWords);
+  else k_pyr_down<1><<<g, kPyrThreads, 0, s>>>(d_jobs, reset, resetWords);
 }
 void launch_gabor(const ScaleDev* d_sd, const TileWork* d_work, int nwork, int grid, unsigned int* d_fault,
                   cudaStream_t s, bool pipelined, bool pdl) {

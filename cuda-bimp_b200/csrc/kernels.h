@@ -29,15 +29,15 @@ struct PyrJobF {
   int dw, dh, dp;
 };
 
-// Keypoint destination of one image: 7 x ld float matrix, `capacity` columns.
 // Keypoint destination of one image: a 7 x ld SURF-layout float matrix
 // (rows X, Y, LAPLACIAN, OCTAVE, SIZE, ANGLE, HESSIAN), or with aos = 1 an
 // array of bimp_keypoint records (7 words each, cv::KeyPoint field order).
 struct KpOut {
-  float* kp;
-  size_t ld;
-  int capacity;
-  int aos;
+  float* kp = nullptr;
+  size_t ld = 0;
+  int capacity = 0;
+  int aos = 0;
+  int* count = nullptr;   // where the NMS also writes the image's keypoint total (or null)
 };
 
 cudaError_t configure_kernels();
@@ -49,7 +49,10 @@ size_t stencil_smem_bytes();
 // `levels` (1..3) pyrDown steps per job in one launch; maxW/maxH: largest
 // deepest-level size over the jobs
 void launch_set_out(KpOut* d, const KpOut& v, cudaStream_t s);
-void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s);
+// reset/resetWords: words the launch's first CTA zeroes before anything else
+// of the detection runs (the map maxima and the fault word), or null.
+void launch_pyr(const PyrJob* d_jobs, int njobs, int levels, int maxW, int maxH, cudaStream_t s,
+                unsigned int* reset = nullptr, int resetWords = 0);
 // d_fault: word that receives 1 if a bounded device wait expired.
 // pipelined: the warp-specialised variant (k_gabor_tiles_ws), for work whose
 // scales all have V <= pipelined_tile_max_valid(); otherwise the phased one
