@@ -168,8 +168,9 @@ struct Engine {
   // both).  Costs come from the kernel's measured phase times (cycles between
   // its CTA barriers at 1080p, in units of one orientation of a V = 100
   // tile): per orientation, the product and inverse y-passes on all 128
-  // columns 0.414, each round of the first inverse x-pass (16 V items over
-  // 512 threads) 0.0565, each round of the second (8 V items) 0.18, of which
+  // columns 0.414, each round of the first inverse x-pass (16 items per valid
+  // row inside the map over 512 threads) 0.0565, each round of the second
+  // (8 items per row) 0.18, of which
   // the magnitudes and stores are 0.42 and scale with the share of the
   // tile's outputs inside the map; an item's forward transform and spectrum
   // store 1.35.  The smallest run bound that fits in `grid` runs is found by
@@ -185,9 +186,9 @@ struct Engine {
     for (size_t i = 0; i < tiles.size(); ++i) {
       const ScaleDev& d = sds[tiles[i].entry];
       const int ty = tiles[i].tile / d.tilesX, tx = tiles[i].tile - ty * d.tilesX;
-      const double inside = (double)std::min(d.V, d.cRows - ty * d.V) * std::min(d.V, d.cCols - tx * d.V) /
-                            ((double)d.V * d.V);
-      const int r3 = (16 * d.V + kTileThreads - 1) / kTileThreads, r4 = (8 * d.V + kTileThreads - 1) / kTileThreads;
+      const int vr = std::min(d.V, d.cRows - ty * d.V);   // valid rows inside the map (the x-passes' rows)
+      const double inside = (double)vr * std::min(d.V, d.cCols - tx * d.V) / ((double)d.V * d.V);
+      const int r3 = (16 * vr + kTileThreads - 1) / kTileThreads, r4 = (8 * vr + kTileThreads - 1) / kTileThreads;
       ori[i] = 0.414 + 0.0565 * r3 + 0.18 * r4 * (0.58 + 0.42 * inside);
       total += kNumOri * ori[i] + kFwd;
       worst = std::max(worst, ori[i] + kFwd);

@@ -375,8 +375,11 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     // tiles holding window column 0 or column dataW of a map with fftW == dataW
     const bool wrapTile = sd->wrapW != 0 && (C0 == 0 || C0 + V >= cCols);
-    // window positions x in [kX, xHi) are this tile's valid outputs
+    // window positions x in [kX, xHi) are this tile's valid outputs; only
+    // its first Vr valid rows lie inside the map, and the x-passes run on
+    // those alone (a tile of the last tile row may hold only a few)
     const int xHi = min(kX + V, cCols - C0 + kX);
+    const int Vr = min(V, cRows - R0);
     // I4's thread keeps column group n1 = t mod 8 for the whole tile: bit n2
     // of xMask says whether its output x = n1 + 8 n2 is in [kX, xHi)
     unsigned int xMask = 0;
@@ -439,7 +442,7 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
       __syncthreads();   // W holds the y-transformed tile; the TMEM y-pass area is free
       tmem_fence_after();
       // I3: x-dim pass B' on the rows holding valid outputs
-      for (int j = t; j < V * 16; j += kTileThreads) {
+      for (int j = t; j < Vr * 16; j += kTileThreads) {
         const int y = kX + (j >> 4), k2 = j & 15;
         float2 v[8];
 #pragma unroll
@@ -450,7 +453,7 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
       }
       __syncthreads();
       // I4: x-dim pass A' -> natural x; complex magnitude of valid outputs
-      for (int j = t; j < V * 8; j += kTileThreads) {
+      for (int j = t; j < Vr * 8; j += kTileThreads) {
         const int y = kX + (j >> 3), n1 = j & 7;
         float2 v[16];
 #pragma unroll
@@ -657,6 +660,7 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
       const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
       const bool wrapTile = sd->wrapW != 0 && (C0 == 0 || C0 + V >= cCols);
       const int xHi = min(kX + V, cCols - C0 + kX);
+      const int Vr = min(V, cRows - R0);   // valid rows inside the map
       // I4 keeps column group n1 = tg mod 8 for the whole tile
       unsigned int xMask = 0;
 #pragma unroll
@@ -672,7 +676,7 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
         float* __restrict__ Cout = C0p + (size_t)o * cStride;
         nbar_sync(kBarFull0 + b, kTileThreads);
         // I3: x-dim pass B' on the V rows of the buffer
-        for (int j = tg; j < V * 16; j += kWsGroup) {
+        for (int j = tg; j < Vr * 16; j += kWsGroup) {
           const int y = j >> 4, k2 = j & 15;
           float2 v[8];
 #pragma unroll
@@ -683,7 +687,7 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
         }
         nbar_sync(kBarX, kWsGroup);
         // I4: x-dim pass A' -> natural x; complex magnitude of valid outputs
-        for (int j = tg; j < V * 8; j += kWsGroup) {
+        for (int j = tg; j < Vr * 8; j += kWsGroup) {
           const int y = j >> 3, n1 = j & 7;
           float2 v[16];
 #pragma unroll
