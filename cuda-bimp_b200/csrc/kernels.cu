@@ -958,6 +958,12 @@ __device__ __forceinline__ int nms_decide_piece(const ScaleDev* __restrict__ sd,
       const float cv[6] = {lc, c[k].x, c[k].y, c[k].z, c[k].w, rcv};
       const float uv[6] = {lu, u[k].x, u[k].y, u[k].z, u[k].w, ruv};
       const float dv[6] = {ld, d[k].x, d[k].y, d[k].z, d[k].w, rdv};
+      // the 8-neighbour maximum from the column maxima of the rows above and
+      // below, shared by adjacent pixels (max is exact, so the order of the
+      // comparisons does not matter)
+      float vm[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) vm[q] = fmaxf(uv[q], dv[q]);
       unsigned int b[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -965,9 +971,7 @@ __device__ __forceinline__ int nms_decide_piece(const ScaleDev* __restrict__ sd,
         const float v = cv[i + 1];
         bool keep = false;
         if (x > off && x < xEnd && v > thr) {
-          float dil = fmaxf(fmaxf(uv[i], uv[i + 1]), uv[i + 2]);
-          dil = fmaxf(dil, fmaxf(cv[i], cv[i + 2]));
-          dil = fmaxf(dil, fmaxf(fmaxf(dv[i], dv[i + 1]), dv[i + 2]));
+          const float dil = fmaxf(fmaxf(vm[i], vm[i + 1]), fmaxf(vm[i + 2], fmaxf(cv[i], cv[i + 2])));
           keep = v - dil > 0.f;
         }
         b[i] = __ballot_sync(0xffffffffu, keep);
