@@ -245,38 +245,6 @@ constexpr int kStX = 32, kStY = 32, kHalo = 8;   // kStY: the adjoint's stencil 
 constexpr int kFwY = kStencilBlockH;               // forward stencil block rows
 constexpr int kStW = kStX + 2 * kHalo, kStH = kFwY + 2 * kHalo;
 
-// Largest tap offset of an offset set along rows (axis 0) or columns (1):
-// end-stop taps at +-2 es, the tangential tap at in, the radial taps at +-ih.
-constexpr int offset_set_reach(int set, int axis) {
-  int m = 0;
-  for (int o = 0; o < kNumOri; ++o) {
-    const int e = kOffsetSets[set][axis][o], i = kOffsetSets[set][2 + axis][o], h = kOffsetSets[set][4 + axis][o];
-    const int v = 2 * (e < 0 ? -e : e), w = i < 0 ? -i : i, u = h < 0 ? -h : h;
-    m = v > m ? v : m;
-    m = w > m ? w : m;
-    m = u > m ? u : m;
-  }
-  return m;
-}
-// Staged window of a forward stencil block for offset pattern PAT (0: run-
-// time offsets): the 32 x kFwY block plus halos hx, hy on each side that
-// cover the pattern's taps; hx is a multiple of 4 floats, so that the box
-// starts on a 16-byte boundary (block columns start at multiples of 32).
-template <int PAT>
-struct StWin {
-  static constexpr int hy = PAT == 0 ? kHalo : offset_set_reach(PAT - 1, 0);
-  static constexpr int hx = PAT == 0 ? kHalo : (offset_set_reach(PAT - 1, 1) + 3) / 4 * 4;
-  static constexpr int w = kStX + 2 * hx, h = kFwY + 2 * hy;
-  static_assert(hx <= kHalo && hy <= kHalo, "a pattern's window exceeds the general one");
-};
-// Box of the window of a pattern known only at run time (host and producer).
-__host__ __device__ __forceinline__ void st_window(int pattern, int& hx, int& hy, int& w, int& h) {
-  if (pattern == 1) { hx = StWin<1>::hx; hy = StWin<1>::hy; w = StWin<1>::w; h = StWin<1>::h; }
-  else if (pattern == 2) { hx = StWin<2>::hx; hy = StWin<2>::hy; w = StWin<2>::w; h = StWin<2>::h; }
-  else { hx = StWin<0>::hx; hy = StWin<0>::hy; w = StWin<0>::w; h = StWin<0>::h; }
-}
-static_assert(kNumOffsetSets == 2, "st_window covers two offset sets");
-
 __device__ __forceinline__ unsigned int float_key(float f) {
   const unsigned int b = __float_as_uint(f);
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
@@ -325,15 +293,14 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
                                               float& Sout, float& Tout, float& Rout, unsigned int& bits) {
   float S = 0.f, D = 0.f, T = 0.f, R = 0.f;
   unsigned int b = 0;
-  constexpr int kWw = StWin<PAT>::w, kWs = StWin<PAT>::w * StWin<PAT>::h;   // window row pitch, orientation stride
-  const float* c0 = s_c + cy * kWw + cx;
+  const float* c0 = s_c + cy * kStW + cx;
 #pragma unroll
   for (int o = 0; o < kNumOri; ++o) {
     if (CHECK && !(x >= P.exlo[o] && x <= P.exhi[o] && y >= P.eylo[o] && y <= P.eyhi[o])) continue;
     const int o1 = soff<PAT>(P, 0, o), o2 = soff<PAT>(P, 1, o);
-    const float* c = c0 + o * kWs;
-    if constexpr (MODE == kStencilDS) S += fmaxf(c[-o1 * kWw + o2] - c[o1 * kWw - o2], 0.f);
-    const float d = fmaf(-0.5f, c[2 * o1 * kWw - 2 * o2], fmaf(-0.5f, c[-2 * o1 * kWw + 2 * o2], c[0]));
+    const float* c = c0 + o * (kStH * kStW);
+    if constexpr (MODE == kStencilDS) S += fmaxf(c[-o1 * kStW + o2] - c[o1 * kStW - o2], 0.f);
+    const float d = fmaf(-0.5f, c[2 * o1 * kStW - 2 * o2], fmaf(-0.5f, c[-2 * o1 * kStW + 2 * o2], c[0]));
     if constexpr (MODE == kStencilAdj) b |= (d > 0.f ? 1u : 0u) << (4 * o);
     D += fmaxf(d, 0.f);
   }
@@ -341,17 +308,17 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
   for (int o = 0; o < kNumOri; ++o) {
     if (CHECK && !(x >= P.ixlo[o] && x <= P.ixhi[o] && y >= P.iylo[o] && y <= P.iyhi[o])) continue;
     const int o1 = soff<PAT>(P, 2, o), o2 = soff<PAT>(P, 3, o);
-    const float* c = c0 + o * kWs;
-    const float* cp = c0 + ((o + kNumOri / 2) % kNumOri) * kWs;
+    const float* c = c0 + o * (kStH * kStW);
+    const float* cp = c0 + ((o + kNumOri / 2) % kNumOri) * (kStH * kStW);
     const float centre = c[0];
-    const float v = c[-o1 * kWw - o2] - centre;
+    const float v = c[-o1 * kStW - o2] - centre;
     if constexpr (MODE == kStencilAdj) b |= (v > 0.f ? 2u : 0u) << (4 * o);
     T += fmaxf(v, 0.f);
     const int h1 = soff<PAT>(P, 4, o), h2 = soff<PAT>(P, 5, o);
-    float r = centre - gain * cp[h1 * kWw + h2];
+    float r = centre - gain * cp[h1 * kStW + h2];
     if constexpr (MODE == kStencilAdj) b |= (r > 0.f ? 8u : 0u) << (4 * o);
     r = fmaxf(r, 0.f);
-    r += centre - gain * cp[-h1 * kWw - h2];
+    r += centre - gain * cp[-h1 * kStW - h2];
     if constexpr (MODE == kStencilAdj) b |= (r > 0.f ? 4u : 0u) << (4 * o);
     R += fmaxf(r, 0.f);
   }
@@ -390,8 +357,8 @@ __device__ __forceinline__ float stencil_rows(const float* __restrict__ s_c, con
 #pragma unroll
   for (int i = 0; i < kRows; ++i) {
     const int ly = ly0 + (NT / 32) * i;
-    stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + StWin<PAT>::hy, lx + StWin<PAT>::hx, gain, wT, wR, D[i],
-                                    S[i], T[i], R[i], b[i]);
+    stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i], R[i],
+                                    b[i]);
   }
   float dmax = -INFINITY;
 #pragma unroll
@@ -421,9 +388,8 @@ __device__ __forceinline__ float stencil_block(const float* __restrict__ s_c, co
 }
 
 // Persistent, warp-specialised stencil kernel: one CTA per SM walks the block
-// list.  A producer warp stages the complex-cell windows (8 orientations of a
-// 32 x 32 block plus the halo its offset pattern needs: 40 x 40, 48 x 44, or
-// 48 x 48 for run-time offsets) as one TMA tensor
+// list.  A producer warp stages the complex-cell windows (8 orientations x 48
+// rows x 48 floats: a 32 x 32 block plus an 8-pixel halo) as one TMA tensor
 // box each, with the block's parameters, into a ring of kStBufs buffers, so
 // that up to kStBufs - 1 windows are in flight while 16 consumer warps
 // compute the oldest.  Full barriers (TMA bytes) and empty barriers (one
@@ -480,10 +446,7 @@ __device__ __forceinline__ StencilPre stencil_fetch(const ScaleDev* __restrict__
     r.gain = sd->radialGain; r.wT = sd->wTan; r.wR = sd->wRad;
     r.D = sd->D; r.S = sd->S; r.T = sd->T; r.R = sd->R; r.bits = sd->bits; r.maxKey = sd->maxKey;
   }
-  if (lane == 0) {
-    r.cMap = sd->cMap;
-    r.pattern = sd->pattern;   // the window's box (the TMA is issued by lane 0)
-  }
+  if (lane == 0) r.cMap = sd->cMap;
   return r;
 }
 
@@ -508,23 +471,18 @@ __device__ __forceinline__ void stencil_put(const StencilPre& r, StencilBlk& B, 
   }
 }
 
-// One thread: the block's window as one TMA box (w x h x 8 floats at
-// x0 - hx, y0 - hy for the scale's offset pattern; the entry's tensor map
-// holds the same box) through the entry's tensor map.  x0 - hx is a
-// multiple of 4 floats (16 bytes); parts of the box outside the maps read
-// as zero.  The arrive releases the block record written before it.
-__device__ __forceinline__ void stencil_stage_tma(const void* cMap, int pattern, int x0, int y0, float* buf,
-                                                  uint32_t bar) {
-  int hx, hy, w, h;
-  st_window(pattern, hx, hy, w, h);
+// One thread: the block's window as one TMA box (48 x 48 x 8 floats at
+// x0 - 8, y0 - 8) through the entry's tensor map.  x0 - 8 is a multiple of 4
+// floats (16 bytes); parts of the box outside the maps read as zero.  The
+// arrive releases the block record written before it.
+__device__ __forceinline__ void stencil_stage_tma(const void* cMap, int x0, int y0, float* buf, uint32_t bar) {
   fence_proxy_async();   // the buffer was last read through the generic proxy
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-               "r"((uint32_t)(kNumOri * w * h * 4))
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((uint32_t)(kStBuf * 4))
                : "memory");
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
           "r"(smem_u32(buf)),
-      "l"(cMap), "r"(x0 - hx), "r"(y0 - hy), "r"(0), "r"(bar)
+      "l"(cMap), "r"(x0 - kHalo), "r"(y0 - kHalo), "r"(0), "r"(bar)
       : "memory");
 }
 
@@ -573,7 +531,7 @@ k_stencil(const ScaleDev* __restrict__ sds, const int2* __restrict__ work, int n
       }
       stencil_put(cur, blk[b], lane);
       __syncwarp();
-      if (lane == 0) stencil_stage_tma(cur.cMap, cur.pattern, cur.x0, cur.y0, s_buf + b * kStBuf, full0 + 8 * b);
+      if (lane == 0) stencil_stage_tma(cur.cMap, cur.x0, cur.y0, s_buf + b * kStBuf, full0 + 8 * b);
       __syncwarp();
       issued = k + 1;
       if (k + 1 < nk) cur = stencil_fetch(sds, work, blockIdx.x + (k + 1) * gridDim.x, lane);
@@ -1185,9 +1143,7 @@ bool encode_c_maps(const ScaleDev* sds, int n, void* maps, std::string& err) {
     const ScaleDev& d = sds[e];
     const cuuint64_t dims[3] = {(cuuint64_t)d.cPitch, (cuuint64_t)d.cRows, (cuuint64_t)kNumOri};
     const cuuint64_t strides[2] = {(cuuint64_t)d.cPitch * sizeof(float), (cuuint64_t)d.cStride * sizeof(float)};
-    int hx, hy, w, h;   // the window box of the scale's offset pattern (what the stencil's producer expects)
-    st_window(d.pattern, hx, hy, w, h);
-    const cuuint32_t box[3] = {(cuuint32_t)w, (cuuint32_t)h, (cuuint32_t)kNumOri};
+    const cuuint32_t box[3] = {(cuuint32_t)kStW, (cuuint32_t)kStH, (cuuint32_t)kNumOri};
     const cuuint32_t elem[3] = {1, 1, 1};
     const CUresult r = enc(&out[e], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, d.C, dims, strides, box, elem,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
