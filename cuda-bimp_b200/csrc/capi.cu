@@ -475,7 +475,12 @@ struct Engine {
     nRows = static_cast<int>(rows.size());
     const size_t offSd = a.reserve(sizeof(ScaleDev) * sds.size());
     {   // the tile buffer holds the largest plan the autotuner may choose
+      // (and room for other grids a caller may ask for: a split plan's
+      // padded list holds about nTiles + 3 grid entries when the tiles'
+      // costs are within a factor of two; a plan beyond the buffer is
+      // refused by retile)
       tileCap = nWork;
+      int maxTiles = 0;
       const int grids[4] = {0, sms, 2 * sms, defGrid};
       for (int policy = 0; policy < 2; ++policy)
         for (int order = 0; order < 2; ++order)
@@ -483,7 +488,9 @@ struct Engine {
             std::vector<ScaleDev> tmp = sds;
             int nt = 0, ng = 0;
             tileCap = std::max(tileCap, static_cast<int>(work_list(tmp, policy, order, g, &nt, &ng).size()));
+            maxTiles = std::max(maxTiles, nt);
           }
+      tileCap = std::max(tileCap, 2 * maxTiles + 6 * sms);
     }
     const size_t offTiles = a.reserve(sizeof(TileWork) * std::max<size_t>(1, (size_t)tileCap));
     const size_t offSten = a.reserve(sizeof(int2) * std::max<size_t>(1, sten.size()));

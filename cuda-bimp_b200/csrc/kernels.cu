@@ -833,15 +833,6 @@ k_nms_write(const ScaleDev* __restrict__ sds, const int2* __restrict__ rows, int
 // earlier CTAs (one parallel read of at most a few thousand ints), the pieces
 // their offsets within the CTA from the popcounts of their words, and writes
 // the records.  No CTA waits for another.
-// Spreads bit i of an 8-bit value to bit 4 i.
-__device__ __forceinline__ unsigned int spread4(unsigned int x) {
-  x &= 0xffu;
-  x = (x | (x << 12)) & 0x000f000fu;
-  x = (x | (x << 6)) & 0x03030303u;
-  x = (x | (x << 3)) & 0x11111111u;
-  return x;
-}
-
 // Aligned decision words of a candidate row: word c covers the pixels
 // 32 (first + c) .. 32 (first + c) + 31, first = (off + 1) / 32; pixels outside
 // the candidate range (off, xEnd) are 0.
@@ -858,8 +849,9 @@ __device__ __forceinline__ void nms_row_words(const ScaleDev* __restrict__ sd, i
 // (the row pitch is a multiple of 32 floats), two segments per round, so a
 // row costs about one memory latency per 256 pixels; the neighbours across
 // lanes come by shuffles, across segments by two scalar loads.  Two segments
-// per round keep the kernel within 64 registers, so that every CTA of a 1080p
-// detection is resident at once (four per SM).
+// per round keep the kernel within 64 registers (four CTAs per SM).  Each
+// lane's four decisions form a nibble; the words are OR-reductions of eight
+// lanes' shifted nibbles.
 constexpr int kNmsSegBatch = 2;
 // A piece is the part of a candidate row inside one 512-pixel-aligned span
 // (four segments, sixteen decision words), so that a long row is decided by
@@ -922,7 +914,8 @@ __device__ __forceinline__ int nms_decide_piece(const ScaleDev* __restrict__ sd,
       float vm[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) vm[q] = fmaxf(uv[q], dv[q]);
-      unsigned int b[4];
+      // this lane's four decisions as a nibble (bit i: pixel x4 + i)
+      unsigned int nib = 0;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int x = x4 + i;
@@ -932,21 +925,24 @@ __device__ __forceinline__ int nms_decide_piece(const ScaleDev* __restrict__ sd,
           const float dil = fmaxf(fmaxf(vm[i], vm[i + 1]), fmaxf(vm[i + 2], fmaxf(cv[i], cv[i + 2])));
           keep = v - dil > 0.f;
         }
-        b[i] = __ballot_sync(0xffffffffu, keep);
-        n += __popc(b[i]);
+        nib |= (keep ? 1u : 0u) << i;
       }
-      // word w of the segment: lanes 8 w .. 8 w + 7, bit 4 (lane - 8 w) + i
-      if (lane < 4) {
-        const int widx = 4 * (sb + k) + lane - first;
-        if (widx >= 0 && widx < nch) {
-          unsigned int word = 0;
-#pragma unroll
-          for (int i = 0; i < 4; ++i) word |= spread4(b[i] >> (8 * lane)) << i;
-          mask[widx] = word;
-        }
+      n += __popc(nib);
+      // word w of the segment (pixels 32 w .. 32 w + 31): the nibbles of
+      // lanes 8 w .. 8 w + 7, lane 8 w + l at bits 4 l, OR-ed across the 8 lanes
+      unsigned int word = nib << (4 * (lane & 7));
+      word |= __shfl_xor_sync(0xffffffffu, word, 1);
+      word |= __shfl_xor_sync(0xffffffffu, word, 2);
+      word |= __shfl_xor_sync(0xffffffffu, word, 4);
+      if ((lane & 7) == 0) {
+        const int widx = 4 * (sb + k) + (lane >> 3) - first;
+        if (widx >= 0 && widx < nch) mask[widx] = word;
       }
     }
   }
+  // the piece's keypoint count (each lane counted its own pixels)
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) n += __shfl_xor_sync(0xffffffffu, n, m);
   return n;
 }
 

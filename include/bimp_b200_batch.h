@@ -70,7 +70,8 @@ int bimp_batch_autotune(bimp_batch* batch, void* stream, int reps, bimp_tile_pla
 
 /* Uses the given tile plan (e.g. one the autotuner chose earlier) and
  * recaptures the graph; grid <= 0 means one CTA per tile, grid > 0 the split
- * plan over at most `grid` persistent CTAs; kernel 1 falls back
+ * plan over at most `grid` persistent CTAs (BIMP_ERR_INVALID if that plan's
+ * work list exceeds the buffer sized at creation); kernel 1 falls back
  * to the phased kernel where the pipelined one does not fit. */
 int bimp_batch_set_tile_plan(bimp_batch* batch, int policy, int order, int grid, int kernel);
 
