@@ -1,15 +1,19 @@
 // BIMP device kernels for sm_100a.
 //
-//   k_pyr_down      uint8 Gaussian pyramid level (cv::cuda::pyrDown semantics)
+//   k_pyr_down      uint8 Gaussian pyramid, up to three levels per launch
+//                   (cv::cuda::pyrDown semantics)
 //   k_gabor_tiles   overlap-save 128x128 tile FFT: image spectrum once per
-//                   tile, then per orientation spectrum multiply + inverse
-//                   FFT + complex magnitude; writes only the magnitude maps
+//                   work item, then per orientation spectrum multiply +
+//                   inverse FFT + complex magnitude; writes only the
+//                   magnitude maps (k_gabor_tiles_ws: warp-specialised form)
 //   k_stencil       end-stopped cells, tangential/radial inhibition and the
 //                   summed keypoint map D (and S), all 8 orientations staged
 //                   in shared memory; per-scale max(D)
-//   k_nms_count     strict 8-neighbour maxima above 0.104*max per row
-//   k_scan          exclusive scan of the row counts
-//   k_nms_write     keypoint records in (scale, y, x) order
+//   k_nms_decide    strict 8-neighbour maxima above 0.104*max: decision
+//                   words and per-group counts
+//   k_nms_emit      keypoint records in (scale, y, x) order
+//   k_nms_count, k_scan, k_nms_write: the same NMS in three launches over
+//                   whole rows (the allocation-free extraction entry point)
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
