@@ -227,6 +227,24 @@ __device__ __forceinline__ int perm128d(int k) { return 8 * (k & 15) + (k >> 4);
 // per-orientation coefficients G(+-k), dGa, dGr come pre-gathered in the
 // half layout (ScaleDev::bwA, bwB).
 constexpr int kGaborBwdSmem = kSmemW + kSmemBh + kSmemTw + kSmemMaps + 16;
+
+// Prefetch (into L2, or into this SM's L1) of the block of dL/dC that the
+// magnitude pass of one orientation reads: rows [R0, R0 + rows), columns
+// [x0, x1) of a map with row pitch `pitch` floats (rows start on 128-byte
+// lines).  One 128-byte line per thread and step; addresses stay inside the
+// map.  The loads come after three transform passes, so the lines are in
+// place by then instead of each load waiting on device memory.
+template <bool L1>
+__device__ __forceinline__ void prefetch_block(const float* base, int pitch, int R0, int rows, int x0, int x1, int t) {
+  if (rows <= 0 || x1 <= x0) return;
+  const int l0 = x0 >> 5, nl = ((x1 - 1) >> 5) - l0 + 1;   // 32 floats per line
+  for (int i = t; i < rows * nl; i += kTileThreads) {
+    const int r = i / nl, l = l0 + (i - r * nl);
+    const float* a = base + (size_t)(R0 + r) * pitch + 32 * l;
+    if constexpr (L1) asm volatile("prefetch.global.L1 [%0];" ::"l"(a));
+    else asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+  }
+}
 static_assert(kGaborBwdSmem <= 232448, "tile backward exceeds the 227 KB shared-memory limit");
 
 __global__ void __launch_bounds__(kTileThreads, 1)
@@ -294,8 +312,12 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
     const int cRows = sd->cRows, cCols = sd->cCols, cPitch = sd->cPitch;
     const long long cStride = sd->cStride;
     const int wrapW = sd->wrapW;
+    // this tile's block of every dL/dC map: rows and columns of its valid
+    // outputs inside the map
+    const int pfRows = min(V, cRows - R0), pfX1 = min(C0 + V, cCols);
     for (int o = 0; o < kNumOri; ++o) {
       const float* __restrict__ Go = sd->G + (size_t)o * kSpecFloats;
+      prefetch_block<false>(sd->gC + (size_t)o * cStride, cPitch, R0, pfRows, C0, pfX1, t);
       // I1: y-dim pass B' with the spectrum product X * G_o (TMEM in, TMEM out)
 #pragma unroll 1
       for (int q = 0; q < 4; ++q) {
@@ -314,6 +336,8 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
       tmem_fence_before();
       __syncthreads();   // the y-pass output is complete; no thread still reads W
       tmem_fence_after();
+      // (I2 and I3 use TMEM and shared memory only: L1 keeps the block)
+      prefetch_block<true>(sd->gC + (size_t)o * cStride, cPitch, R0, pfRows, C0, pfX1, t);
       // I2: y-dim pass A' -> natural y; rows outside the valid band are zero
       // (a is zero there, and the transform of a below reads every row)
 #pragma unroll
