@@ -386,9 +386,14 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
           if (x >= kX && x < kX + V && gy < cRows && gx < cCols) {
             float gc = __ldg(sd->gC + (size_t)o * cStride + (size_t)gy * cPitch + gx);
             if (wrapW && gx == 0 && gy >= 1) gc += __ldg(sd->gWrap + o * (sd->dataH + 1) + gy - 1);
-            const float m = cmag(v[n2]);
+            // |z| as the forward computes it (s * rsqrt(s)); 1/|z| is the
+            // same reciprocal square root, so a = gc z / |z| takes no division
+            const float sq = fmaf(v[n2].x, v[n2].x, v[n2].y * v[n2].y);
+            float rs;
+            asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rs) : "f"(fmaxf(sq, 1e-30f)));
+            const float m = sq * rs;
             if (m > kMagFloor) {
-              const float sc = gc / m;
+              const float sc = gc * rs;
               a = make_float2(sc * v[n2].x, sc * v[n2].y);
             }
           }
