@@ -373,19 +373,30 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
       // on the same 16 elements, in registers
       for (int j = t; j < V * 8; j += kTileThreads) {
         const int y = kX + (j >> 3), n1 = j & 7;
+        const int gy = R0 + y - kX;
+        // dL/dC of the item's valid outputs, loaded before the transform so
+        // that their latency overlaps it
+        float gcv[16];
+        {
+          const float* __restrict__ grow = sd->gC + (size_t)o * cStride + (size_t)gy * cPitch;
+#pragma unroll
+          for (int n2 = 0; n2 < 16; ++n2) {
+            const int x = n1 + 8 * n2, gx = C0 + x - kX;
+            gcv[n2] = (x >= kX && x < kX + V && gy < cRows && gx < cCols) ? __ldg(grow + gx) : 0.f;
+            if (wrapW && gx == 0 && gy >= 1 && gy < cRows) gcv[n2] += __ldg(sd->gWrap + o * (sd->dataH + 1) + gy - 1);
+          }
+        }
         float2 v[16];
 #pragma unroll
         for (int k2 = 0; k2 < 16; ++k2) v[k2] = W[widx(y, 8 * k2 + n1)];
         dft16<true>(v);
-        const int gy = R0 + y - kX;
 #pragma unroll
         for (int n2 = 0; n2 < 16; ++n2) {
           const int x = n1 + 8 * n2;
           const int gx = C0 + x - kX;
           float2 a = make_float2(0.f, 0.f);
           if (x >= kX && x < kX + V && gy < cRows && gx < cCols) {
-            float gc = __ldg(sd->gC + (size_t)o * cStride + (size_t)gy * cPitch + gx);
-            if (wrapW && gx == 0 && gy >= 1) gc += __ldg(sd->gWrap + o * (sd->dataH + 1) + gy - 1);
+            const float gc = gcv[n2];
             // |z| as the forward computes it (s * rsqrt(s)); 1/|z| is the
             // same reciprocal square root, so a = gc z / |z| takes no division
             const float sq = fmaf(v[n2].x, v[n2].x, v[n2].y * v[n2].y);
