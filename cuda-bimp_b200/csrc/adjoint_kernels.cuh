@@ -483,7 +483,7 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
           const int kx = (sl >> 2) + 16 * (sl & 3);
           const int p = perm128d(kx), np = perm128d((kTile - kx) & 127);
           const int pp = phys(p) ^ ((pr & 1) << 3);
-#pragma unroll 4
+#pragma unroll 8
           for (int r = 0; r < 16; ++r) {
             const int py = pr + 8 * r;
             entry(py, sl, p, np, py * kTile + pp);
