@@ -226,8 +226,13 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
       v[m] = make_float2(level_value<FLT>(sd, ra, c), level_value<FLT>(sd, rb, c));
     }
     dft16<false>(v);
+    // twiddles into registers before the stores (loads of the table would
+    // otherwise wait behind each store to the same shared memory)
+    float2 twr[16];
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) W[widx(r, n1 + 8 * k2)] = k2 ? c_mul(v[k2], tw[n1 * 17 + k2]) : v[0];
+    for (int k2 = 1; k2 < 16; ++k2) twr[k2] = tw[n1 * 17 + k2];
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) W[widx(r, n1 + 8 * k2)] = k2 ? c_mul(v[k2], twr[k2]) : v[0];
   }
   __syncthreads();
   // F2: x-dim pass B
@@ -265,8 +270,11 @@ __device__ __forceinline__ void tile_forward_spectrum(const ScaleDev* sd, int R0
     dft16<false>(v);
     float2* col = xh_ptr(Xh64, Nyq, 0, s);
     const int st = s < 64 ? 64 : 1;
+    float2 twr[16];
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) col[(n1 + 8 * k2) * st] = k2 ? c_mul(v[k2], tw[n1 * 17 + k2]) : v[0];
+    for (int k2 = 1; k2 < 16; ++k2) twr[k2] = tw[n1 * 17 + k2];
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) col[(n1 + 8 * k2) * st] = k2 ? c_mul(v[k2], twr[k2]) : v[0];
   }
   __syncthreads();
   // F4: y-dim pass B -> rows in permuted ky order
@@ -406,12 +414,17 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
         ph ^= 1u << slot;
         __syncwarp();   // the warp-collective TMEM stores below need a converged warp
         const float* Gq = Gbuf + slot * kGChunkFloats + 8 * h * kTile + pI1;
+        // this quarter's twiddles, read before the TMEM stores (each store
+        // is a compiler barrier for shared-memory loads)
+        float2 twr[8];
+#pragma unroll
+        for (int n1 = 1; n1 < 8; ++n1) twr[n1] = tw[n1 * 17 + k2];
 #pragma unroll
         for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], Gq[k1 * kTile]);
         dft8<true>(v);
 #pragma unroll
         for (int n1 = 0; n1 < 8; ++n1)
-          tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0]);
+          tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], twr[n1]) : v[0]);
       }
       tmem_wait_st();
       tmem_fence_before();
@@ -441,15 +454,22 @@ k_gabor_tiles(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ wor
       tmem_fence_before();
       __syncthreads();   // W holds the y-transformed tile; the TMEM y-pass area is free
       tmem_fence_after();
-      // I3: x-dim pass B' on the rows holding valid outputs
-      for (int j = t; j < Vr * 16; j += kTileThreads) {
-        const int y = kX + (j >> 4), k2 = j & 15;
-        float2 v[8];
+      // I3: x-dim pass B' on the rows holding valid outputs; a thread's k2
+      // (= t mod 16) is the same in every item, so its twiddles are loaded once
+      {
+        const int k2 = t & 15;
+        float2 twr[8];
 #pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
-        dft8<true>(v);
+        for (int n1 = 1; n1 < 8; ++n1) twr[n1] = tw[n1 * 17 + k2];
+        for (int j = t; j < Vr * 16; j += kTileThreads) {
+          const int y = kX + (j >> 4);
+          float2 v[8];
 #pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0];
+          for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
+          dft8<true>(v);
+#pragma unroll
+          for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], twr[n1]) : v[0];
+        }
       }
       __syncthreads();
       // I4: x-dim pass A' -> natural x; complex magnitude of valid outputs
@@ -623,12 +643,15 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
 #pragma unroll
           for (int k1 = 0; k1 < 8; ++k1) gn[k1] = __ldg(Go + (size_t)(8 * k2n + k1) * kTile + pI1);
           tmem_load8(tlane + 16 * k2, v);
+          float2 twr[8];
+#pragma unroll
+          for (int n1 = 1; n1 < 8; ++n1) twr[n1] = tw[n1 * 17 + k2];
 #pragma unroll
           for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], g[k1]);
           dft8<true>(v);
 #pragma unroll
           for (int n1 = 0; n1 < 8; ++n1)
-            tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0]);
+            tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], twr[n1]) : v[0]);
 #pragma unroll
           for (int k1 = 0; k1 < 8; ++k1) g[k1] = gn[k1];
         }
@@ -675,15 +698,22 @@ k_gabor_tiles_ws(const ScaleDev* __restrict__ sds, const TileWork* __restrict__ 
         float2* Wo = Wb + b * kWsBuf;
         float* __restrict__ Cout = C0p + (size_t)o * cStride;
         nbar_sync(kBarFull0 + b, kTileThreads);
-        // I3: x-dim pass B' on the V rows of the buffer
-        for (int j = tg; j < Vr * 16; j += kWsGroup) {
-          const int y = j >> 4, k2 = j & 15;
-          float2 v[8];
+        // I3: x-dim pass B' on the V rows of the buffer (a thread's k2 is
+        // fixed: its twiddles are loaded once)
+        {
+          const int k2 = tg & 15;
+          float2 twr[8];
 #pragma unroll
-          for (int k1 = 0; k1 < 8; ++k1) v[k1] = Wo[widx(y, 8 * k2 + k1)];
-          dft8<true>(v);
+          for (int n1 = 1; n1 < 8; ++n1) twr[n1] = tw[n1 * 17 + k2];
+          for (int j = tg; j < Vr * 16; j += kWsGroup) {
+            const int y = j >> 4;
+            float2 v[8];
 #pragma unroll
-          for (int n1 = 0; n1 < 8; ++n1) Wo[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0];
+            for (int k1 = 0; k1 < 8; ++k1) v[k1] = Wo[widx(y, 8 * k2 + k1)];
+            dft8<true>(v);
+#pragma unroll
+            for (int n1 = 0; n1 < 8; ++n1) Wo[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], twr[n1]) : v[0];
+          }
         }
         nbar_sync(kBarX, kWsGroup);
         // I4: x-dim pass A' -> natural x; complex magnitude of valid outputs
