@@ -325,12 +325,15 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
         float2 v[8];
         tmem_load8(tlane + 16 * k2, v);
         const float* __restrict__ Gq = Go + (size_t)(8 * k2) * kTile + pI1;
+        float2 twr[8];   // read before the TMEM stores (compiler barriers for shared loads)
+#pragma unroll
+        for (int n1 = 1; n1 < 8; ++n1) twr[n1] = tw[n1 * 17 + k2];
 #pragma unroll
         for (int k1 = 0; k1 < 8; ++k1) v[k1] = c_scale(v[k1], __ldg(Gq + k1 * kTile));
         dft8<true>(v);
 #pragma unroll
         for (int n1 = 0; n1 < 8; ++n1)
-          tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0]);
+          tmem_store1(tlane + kTmemY + 2 * (16 * n1 + k2), n1 ? c_mulc(v[n1], twr[n1]) : v[0]);
       }
       tmem_wait_st();
       tmem_fence_before();
@@ -356,15 +359,22 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
       tmem_fence_before();
       __syncthreads();
       tmem_fence_after();
-      // I3: x-dim pass B' on the valid rows
-      for (int j = t; j < V * 16; j += kTileThreads) {
-        const int y = kX + (j >> 4), k2 = j & 15;
-        float2 v[8];
+      // I3: x-dim pass B' on the valid rows (a thread's k2 is fixed: its
+      // twiddles are read once, not behind each store)
+      {
+        const int k2 = t & 15;
+        float2 twr[8];
 #pragma unroll
-        for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
-        dft8<true>(v);
+        for (int n1 = 1; n1 < 8; ++n1) twr[n1] = tw[n1 * 17 + k2];
+        for (int j = t; j < V * 16; j += kTileThreads) {
+          const int y = kX + (j >> 4);
+          float2 v[8];
 #pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], tw[n1 * 17 + k2]) : v[0];
+          for (int k1 = 0; k1 < 8; ++k1) v[k1] = W[widx(y, 8 * k2 + k1)];
+          dft8<true>(v);
+#pragma unroll
+          for (int n1 = 0; n1 < 8; ++n1) W[widx(y, 8 * k2 + n1)] = n1 ? c_mulc(v[n1], twr[n1]) : v[0];
+        }
       }
       __syncthreads();
       // I4 + the first pass of FFT(a): x-dim pass A' gives z = e + i o at the
@@ -411,8 +421,11 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
           v[n2] = a;
         }
         dft16<false>(v);
+        float2 twr[16];
 #pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2) W[widx(y, n1 + 8 * k2)] = c_mul(v[k2], tw[n1 * 17 + k2]);
+        for (int k2 = 0; k2 < 16; ++k2) twr[k2] = tw[n1 * 17 + k2];
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) W[widx(y, n1 + 8 * k2)] = c_mul(v[k2], twr[k2]);
       }
       __syncthreads();
       for (int j = t; j < V * 16; j += kTileThreads) {
@@ -433,8 +446,11 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
 #pragma unroll
         for (int m = 0; m < 16; ++m) v[m] = W[widx(n1 + 8 * m, p)];
         dft16<false>(v);
+        float2 twr[16];
 #pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2) W[widx(n1 + 8 * k2, p)] = c_mul(v[k2], tw[n1 * 17 + k2]);
+        for (int k2 = 0; k2 < 16; ++k2) twr[k2] = tw[n1 * 17 + k2];
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) W[widx(n1 + 8 * k2, p)] = c_mul(v[k2], twr[k2]);
       }
       __syncthreads();
 #pragma unroll
