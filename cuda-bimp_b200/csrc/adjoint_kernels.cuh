@@ -494,15 +494,40 @@ k_gabor_tiles_bwd(const ScaleDev* __restrict__ sds, const TileWork* __restrict__
         // slots 0..63: thread t owns slot sl = t mod 64 and the rows
         // py = t / 64 + 8 r (r = 0..15), so its column terms are fixed and
         // widx(py, p) = 128 py + (phys(p) ^ 8 (py & 1)) with py & 1 fixed
+        // Four entries at a time: all their loads first, then the updates
+        // (the entries' Bh words are distinct, but a store would otherwise
+        // hold back the next entry's shared-memory loads).
         {
           const int sl = t & 63, pr = t >> 6;
           const int kx = (sl >> 2) + 16 * (sl & 3);
           const int p = perm128d(kx), np = perm128d((kTile - kx) & 127);
           const int pp = phys(p) ^ ((pr & 1) << 3);
-#pragma unroll 8
-          for (int r = 0; r < 16; ++r) {
-            const int py = pr + 8 * r;
-            entry(py, sl, p, np, py * kTile + pp);
+#pragma unroll 1
+          for (int r0 = 0; r0 < 16; r0 += 4) {
+            float4 c4[4];
+            float2 c2[4], X[4], A1[4], A2[4], bb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int py = pr + 8 * (r0 + u);
+              const int j = py * kXhCols + sl;
+              c4[u] = __ldg(cA + j);
+              c2[u] = __ldg(cB + j);
+              X[u] = Xs[j];
+              const int ky = 16 * (py & 7) + (py >> 3);
+              A1[u] = W[py * kTile + pp];
+              A2[u] = W[widx(perm128d((kTile - ky) & 127), np)];
+              bb[u] = Bh[j];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int j = (pr + 8 * (r0 + u)) * kXhCols + sl;
+              Bh[j] = make_float2(fmaf(0.5f * c4[u].x, A1[u].x, fmaf(0.5f * c4[u].y, A2[u].x, bb[u].x)),
+                                  fmaf(0.5f * c4[u].x, A1[u].y, fmaf(-0.5f * c4[u].y, A2[u].y, bb[u].y)));
+              const float re1 = A1[u].x * X[u].x + A1[u].y * X[u].y;
+              const float re2 = A2[u].x * X[u].x - A2[u].y * X[u].y;
+              sa = fmaf(c4[u].z, re1, fmaf(c2[u].x, re2, sa));
+              sr = fmaf(c4[u].w, re1, fmaf(c2[u].y, re2, sr));
+            }
           }
         }
         // the Nyquist slot 64 (kx = 64): one row per thread of the first 128
