@@ -336,6 +336,79 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
   }
 }
 
+// Packed pairs of floats (lane 0: the upper pixel, lane 1: the pixel 16
+// rows below) for the f32x2 arithmetic of sm_100.
+typedef unsigned long long f2p;
+__device__ __forceinline__ f2p pk2(float a, float b) {
+  f2p r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(f2p v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ f2p add2(f2p a, f2p b) {
+  f2p d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2p sub2(f2p a, f2p b) {
+  f2p d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c) {
+  f2p d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f2p relu2(f2p v) {
+  float a, b;
+  upk2(v, a, b);
+  return pk2(fmaxf(a, 0.f), fmaxf(b, 0.f));
+}
+
+// D of two pixels 16 rows apart, every tap inside its bounds (an inner
+// block), compile-time offsets: the arithmetic of stencil_pixel in the same
+// order and roundings, two pixels per instruction.
+template <int PAT>
+__device__ __forceinline__ void stencil_pair_d(const float* __restrict__ s_c, int cy, int cx, float gain, float wT,
+                                               float wR, float& Da, float& Db) {
+  constexpr int dR = 16 * kStW;
+  const float* c0 = s_c + cy * kStW + cx;
+  const f2p mh = pk2(-0.5f, -0.5f), mg = pk2(-gain, -gain);
+  f2p D = pk2(0.f, 0.f), T = D, R = D;
+  f2p cen[kNumOri];
+#pragma unroll
+  for (int o = 0; o < kNumOri; ++o) {
+    const int o1 = soff<PAT>(StencilPar{}, 0, o), o2 = soff<PAT>(StencilPar{}, 1, o);
+    const float* c = c0 + o * (kStH * kStW);
+    cen[o] = pk2(c[0], c[dR]);
+    const int ka = 2 * o1 * kStW - 2 * o2, kb = -2 * o1 * kStW + 2 * o2;
+    const f2p d = fma2(mh, pk2(c[ka], c[dR + ka]), fma2(mh, pk2(c[kb], c[dR + kb]), cen[o]));
+    D = add2(D, relu2(d));
+  }
+#pragma unroll
+  for (int o = 0; o < kNumOri; ++o) {
+    const int o1 = soff<PAT>(StencilPar{}, 2, o), o2 = soff<PAT>(StencilPar{}, 3, o);
+    const float* c = c0 + o * (kStH * kStW);
+    const float* cp = c0 + ((o + kNumOri / 2) % kNumOri) * (kStH * kStW);
+    const int kt = -o1 * kStW - o2;
+    T = add2(T, relu2(sub2(pk2(c[kt], c[dR + kt]), cen[o])));
+    const int h1 = soff<PAT>(StencilPar{}, 4, o), h2 = soff<PAT>(StencilPar{}, 5, o);
+    const int k1 = h1 * kStW + h2;
+    f2p r = relu2(fma2(mg, pk2(cp[k1], cp[dR + k1]), cen[o]));
+    r = add2(r, fma2(mg, pk2(cp[-k1], cp[dR - k1]), cen[o]));
+    R = add2(R, relu2(r));
+  }
+  float d0, d1, t0, t1, r0, r1;
+  upk2(D, d0, d1);
+  upk2(T, t0, t1);
+  upk2(R, r0, r1);
+  const float inhA = wT * t0 + wR * r0;
+  const float inhB = wT * t1 + wR * r1;
+  Da = d0 + (-inhA);
+  Db = d1 + (-inhB);
+}
+
 // Output maps of one stencil block.
 struct StencilOut {
   float* D;
@@ -358,11 +431,17 @@ __device__ __forceinline__ float stencil_rows(const float* __restrict__ s_c, con
   constexpr int kRows = kFwY / (NT / 32);
   float D[kRows], S[kRows], T[kRows], R[kRows];
   unsigned int b[kRows];
+  if constexpr (!CHECK && PAT > 0 && MODE == kStencilD && NT / 32 == 16) {
 #pragma unroll
-  for (int i = 0; i < kRows; ++i) {
-    const int ly = ly0 + (NT / 32) * i;
-    stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i], R[i],
-                                    b[i]);
+    for (int i = 0; i < kRows; i += 2)
+      stencil_pair_d<PAT>(s_c, ly0 + 16 * i + kHalo, lx + kHalo, gain, wT, wR, D[i], D[i + 1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < kRows; ++i) {
+      const int ly = ly0 + (NT / 32) * i;
+      stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i],
+                                      R[i], b[i]);
+    }
   }
   float dmax = -INFINITY;
 #pragma unroll
