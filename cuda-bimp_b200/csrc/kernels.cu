@@ -291,16 +291,35 @@ __device__ __forceinline__ int soff(const StencilPar& P, int k, int o) {
 // adjoint needs: per orientation o, bit 4o double-stopped d > 0, 4o+1
 // tangential t > 0, 4o+2 radial r > 0, 4o+3 the first radial term r1 > 0
 // (all 0 where the bounds test fails).
+// Whether orientation o's taps at offsets k, k + 1 (0: end-stopping,
+// 2: inhibition) pass the reference's bounds test at (x, y) of a W x H map.
+// With compile-time offsets the bounds are immediates against W and H in
+// registers; the staged per-orientation bounds would cost four shared loads
+// per orientation and pixel in every edge block, whose pixels then ran at
+// about half the rate of the inner blocks' pixels.
+template <int PAT>
+__device__ __forceinline__ bool stencil_in(const StencilPar& P, int k, int o, int x, int y, int W, int H) {
+  if constexpr (PAT > 0) {
+    const int a1 = 2 * abs(soff<PAT>(P, k, o)), a2 = 2 * abs(soff<PAT>(P, k + 1, o));
+    return x >= a2 && x <= W - a2 && y >= a1 && y <= H - a1;
+  } else if (k == 0) {
+    return x >= P.exlo[o] && x <= P.exhi[o] && y >= P.eylo[o] && y <= P.eyhi[o];
+  } else {
+    return x >= P.ixlo[o] && x <= P.ixhi[o] && y >= P.iylo[o] && y <= P.iyhi[o];
+  }
+}
+
 template <bool CHECK, int PAT, int MODE>
 __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, const StencilPar& P, int x, int y,
                                               int cy, int cx, float gain, float wT, float wR, float& Dout,
-                                              float& Sout, float& Tout, float& Rout, unsigned int& bits) {
+                                              float& Sout, float& Tout, float& Rout, unsigned int& bits,
+                                              int W, int H) {
   float S = 0.f, D = 0.f, T = 0.f, R = 0.f;
   unsigned int b = 0;
   const float* c0 = s_c + cy * kStW + cx;
 #pragma unroll
   for (int o = 0; o < kNumOri; ++o) {
-    if (CHECK && !(x >= P.exlo[o] && x <= P.exhi[o] && y >= P.eylo[o] && y <= P.eyhi[o])) continue;
+    if (CHECK && !stencil_in<PAT>(P, 0, o, x, y, W, H)) continue;
     const int o1 = soff<PAT>(P, 0, o), o2 = soff<PAT>(P, 1, o);
     const float* c = c0 + o * (kStH * kStW);
     if constexpr (MODE == kStencilDS) S += fmaxf(c[-o1 * kStW + o2] - c[o1 * kStW - o2], 0.f);
@@ -310,7 +329,7 @@ __device__ __forceinline__ void stencil_pixel(const float* __restrict__ s_c, con
   }
 #pragma unroll
   for (int o = 0; o < kNumOri; ++o) {
-    if (CHECK && !(x >= P.ixlo[o] && x <= P.ixhi[o] && y >= P.iylo[o] && y <= P.iyhi[o])) continue;
+    if (CHECK && !stencil_in<PAT>(P, 2, o, x, y, W, H)) continue;
     const int o1 = soff<PAT>(P, 2, o), o2 = soff<PAT>(P, 3, o);
     const float* c = c0 + o * (kStH * kStW);
     const float* cp = c0 + ((o + kNumOri / 2) % kNumOri) * (kStH * kStW);
@@ -440,7 +459,7 @@ __device__ __forceinline__ float stencil_rows(const float* __restrict__ s_c, con
     for (int i = 0; i < kRows; ++i) {
       const int ly = ly0 + (NT / 32) * i;
       stencil_pixel<CHECK, PAT, MODE>(s_c, P, x, y0 + ly, ly + kHalo, lx + kHalo, gain, wT, wR, D[i], S[i], T[i],
-                                      R[i], b[i]);
+                                      R[i], b[i], W, H);
     }
   }
   float dmax = -INFINITY;
