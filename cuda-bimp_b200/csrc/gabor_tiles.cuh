@@ -185,7 +185,12 @@ __device__ __forceinline__ float level_value(const ScaleDev* sd, int r, int c) {
   if constexpr (FLT) {
     return kFloatLevelScale * sd->lvlF[(size_t)r * sd->lvlPitchF + c] - 0.5f;
   } else {
-    return (1.0f / 65536.0f) * (float)(255 * (int)sd->lvl[(size_t)r * sd->lvlPitch + c] - 32768);
+    // 12582912 + (255 u8 - 32768) as the bits of a float (1.5 * 2^23 plus an
+    // integer of magnitude below 2^15 is exact), then x / 65536 exactly:
+    // the same value as the integer converted and scaled, without the
+    // conversion unit
+    const int b = 0x4B400000 - 32768 + 255 * (int)sd->lvl[(size_t)r * sd->lvlPitch + c];
+    return fmaf(__int_as_float(b), 1.0f / 65536.0f, -192.0f);
   }
 }
 
